@@ -1,0 +1,132 @@
+/*
+ * tce.h -- C ABI of the B200 toroidal-ERI engine (libtce.so).
+ *
+ * Drop-in boundary for the integral and SCF path of ALRAKIK/William_CI.  The
+ * reference has no FFI layer: the path sits behind Fortran subroutines and
+ * module globals.  Each entry point below names the reference routine it
+ * replaces (paths relative to the reference project root).  A Fortran
+ * caller binds them with ISO_C_BINDING; a nonzero status maps to the
+ * reference's `error stop`.
+ *
+ * Conventions
+ *   - All matrices are column-major (Fortran order), double precision.
+ *   - Indices in tce_system are 0-based; shells are found exactly as the
+ *     reference finds them (consecutive Cartesian components with the same
+ *     centre and exponents, ERI_toroidal.f90:106-125).
+ *   - Calls on one handle come from a single host thread.  Device memory is
+ *     owned by the handle.  There is no CPU fallback: without a usable B200
+ *     every call returns TCE_ERR_CUDA.
+ */
+#ifndef TCE_H
+#define TCE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TCE_OK              0
+#define TCE_ERR_ARG         1   /* bad argument / inconsistent system        */
+#define TCE_ERR_UNSUPPORTED 2   /* angular momentum or layout not supported  */
+#define TCE_ERR_CUDA        3   /* CUDA error (no device, launch failure ...) */
+#define TCE_ERR_STATE       4   /* call order (e.g. stored ERIs not built)    */
+#define TCE_ERR_NOMEM       5   /* device allocation failed                   */
+
+/* Flat, C-interoperable copy of the supercell basis.  Replaces the module
+ * globals torus_init (Torus_init.f90:1-31), unitcell_module (unitcell.f90),
+ * keywords c_physicist/c_SAO/c_prim_screen (keywords.f90), nquad_point /
+ * t_val / w_val (precompute_t.f90:5-14) and the AO array of ERI_function
+ * (ERI_mod.f90:5-12), which has allocatable components and is not
+ * interoperable. */
+typedef struct {
+    int32_t ndp;              /* periodic directions 1..ndp (Tori1D/2D/3D)   */
+    int32_t ncell[3];         /* nx, ny, nz; cells numbered x fastest        */
+    int32_t nfuc;             /* functions per unit cell                     */
+    int32_t nbas;             /* functions in the supercell                  */
+    int32_t nquad;            /* t nodes: 32/40 mapped GL (fast_quad) or the
+                                 number of entries of t_nodes                */
+    double  L[3];             /* Lx, Ly, Lz; a_d = 2 pi / L_d                */
+    const double  *ctr;       /* [3*nbas] centres (x,y,z per function)       */
+    const int32_t *lxyz;      /* [3*nbas] Cartesian powers (class.f90 order) */
+    const int32_t *prim_off;  /* [nbas+1] CSR offsets into exps/coefs        */
+    const double  *exps;      /* primitive exponents                         */
+    const double  *coefs;     /* NORMALISED contraction coefficients
+                                 (normalize_AO_toroidal_*D already applied)  */
+    const double  *t_nodes;   /* [nquad] or NULL: mapped Gauss-Legendre,
+                                 t = 0.6 u/(1-u) (precompute_t.f90:906-942)  */
+    const double  *t_weights; /* [nquad] or NULL                             */
+    int32_t physicist;        /* stored layout: 0 chemist, 1 physicist       */
+    int32_t sao;              /* 1: ERI_size = nfuc, 0: ERI_size = nbas      */
+    int32_t prim_screen;      /* primitive-pair Schwarz screen (default 1)   */
+    double  schwarz_thr;      /* 1e-13 (ERI_toroidal.f90:64)                 */
+    double  prim_thr;         /* 1e-14 (clifford_tools.f90:74)               */
+} tce_system;
+
+/* Counters of the work set (translation- and 8-fold-unique quartets). */
+typedef struct {
+    int32_t nsh, nshuc, ncap, nquad;
+    int64_t n_shell_quartets;     /* unique shell quartets after screening  */
+    int64_t n_func_quartets;      /* function quartets after the Q screen   */
+    int64_t n_unit_pairs;         /* significant unit-cell shell pairs       */
+    int64_t device_bytes;         /* device memory held by the handle        */
+} tce_info;
+
+/* Build the engine for one supercell basis: t-tables, shells, Schwarz
+ * bounds, primitive-pair table and the unique-quartet work list, all on the
+ * device.  Replaces direct_init (eri_direct.f90:76-225) and the preamble of
+ * ERI_integral_toroidal (ERI_toroidal.f90:93-337). */
+int tce_create(const tce_system *sys, void **handle);
+int tce_destroy(void *handle);
+const char *tce_last_error(void *handle);   /* handle may be NULL */
+int tce_get_info(void *handle, tce_info *info);
+
+/* One shell quartet block (S1 S2|S3 S4), blk column-major (n1,n2,n3,n4).
+ * Parity hook for ERI_shell_block_toroidal (ERI_shell_block_toroidal.f90:28).
+ * mode 0: prefactor screens (Schwarz pass); 1: + primitive screen (the main
+ * loops; needs S1 in the unit cell); 2: no screens (primitive-table pass). */
+int tce_shell_block(void *handle, const int32_t sh4[4], int32_t mode, double *blk);
+
+/* Shell list: first function and component count of each shell. */
+int tce_shells(void *handle, int32_t *first, int32_t *n);
+
+/* Schwarz matrix Q(i,j) = sqrt|(ij|ij)| (nbas x nbas), as built by the
+ * driver (ERI_toroidal.f90:200-236). */
+int tce_schwarz(void *handle, double *Q);
+
+/* Stored ERIs ERI(eri_size, nbas, nbas, nbas), chemist or physicist order,
+ * eri_size = nfuc (sao) or nbas (rows i > nfuc filled by translation,
+ * symmetric_matrix.f90:62-131).  Replaces ERI_integral_toroidal
+ * (ERI_toroidal.f90:36).  The array is also kept on the device for
+ * tce_stored_jk. */
+int tce_eri_stored(void *handle, int64_t eri_size, double *eri);
+
+/* J and K from the device-resident stored ERIs (rows < ERI_size filled).
+ * Replaces hartree_exchange_potential (hartree_exchange_potential.f90:30). */
+int tce_stored_jk(void *handle, const double *P, double *J, double *K);
+
+/* J and K from a caller-provided stored ERI array (uploaded per call); same
+ * formulas as hartree_exchange_potential (hartree_exchange_potential.f90:30)
+ * with n1 = ERI_size. */
+int tce_hartree_exchange(int32_t n1, int32_t nbas, int32_t physicist, const double *P,
+                         const double *eri, double *J, double *K);
+
+/* Integral-direct J/K for one SCF iteration: rows < nfuc of J and K filled,
+ * the others zero.  Host arrays, nbas x nbas.  Replaces direct_JK
+ * (eri_direct.f90:262-374). */
+int tce_direct_jk(void *handle, const double *P, double *J, double *K);
+
+/* Same with device pointers on the caller's stream (cudaStream_t as void*):
+ * dP nbas x nbas, dJ and dK nfuc x nbas (column-major, leading dim nfuc). */
+int tce_direct_jk_device(void *handle, const double *dP, double *dJ, double *dK, void *stream);
+
+/* Elapsed device time (ms) of the last tce_direct_jk[_device] call's quartet
+ * kernel, measured with CUDA events on the launching stream. */
+int tce_last_kernel_ms(void *handle, double *ms);
+
+/* Library build identification (sm_100a, version). */
+const char *tce_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

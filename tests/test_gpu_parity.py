@@ -1,0 +1,104 @@
+"""Parity of the CUDA engine (through the C ABI) with the CPU oracle.
+
+Tolerances: 1e-10 absolute per integral (shell blocks, stored ERIs, Schwarz
+bounds); J and K, which are sums of ~1e5-1e6 integral x density products,
+within 1e-9 absolute.
+"""
+import numpy as np
+import pytest
+
+from conftest import random_density
+
+pytestmark = pytest.mark.gpu
+
+TOL_INT = 1e-10
+TOL_JK = 1e-9
+
+CASES = [
+    ("h2_ring", None),
+    ("h_chain64", (8, 1, 1)),
+    ("h2_sheet", (2, 2, 1)),
+    ("li_cube", (2, 2, 2)),
+]
+
+
+def _engines(systems, name, ncell, **kw):
+    import pyoracle
+    from william_ci_b200.engine import Engine
+    sysm = systems(name, ncell)
+    return sysm, Engine(sysm, **kw), pyoracle.Oracle(sysm, **kw)
+
+
+@pytest.mark.parametrize("name,ncell", CASES)
+def test_schwarz_and_shells(systems, name, ncell):
+    sysm, eng, orc = _engines(systems, name, ncell)
+    sh_o, nshuc, ncap = orc.shells()
+    assert eng.shells() == sh_o
+    inf = eng.info()
+    assert inf["nshuc"] == nshuc and inf["ncap"] == ncap
+    np.testing.assert_allclose(eng.schwarz(), orc.schwarz(), rtol=0, atol=TOL_INT)
+    ns, nf, npq = orc.count()
+    assert inf["n_shell_quartets"] == ns
+    assert inf["n_func_quartets"] == nf
+
+
+@pytest.mark.parametrize("name,ncell", CASES)
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_shell_blocks(systems, name, ncell, mode):
+    sysm, eng, orc = _engines(systems, name, ncell)
+    sh, nshuc, _ = orc.shells()
+    nsh = len(sh)
+    rng = np.random.default_rng(7 + mode)
+    quartets = [(0, 0, 0, 0), (0, min(1, nsh - 1), 0, min(1, nsh - 1))]
+    for _ in range(12):
+        q = [int(rng.integers(0, nshuc))] + [int(x) for x in rng.integers(0, nsh, 3)]
+        quartets.append(tuple(q))
+    for q in quartets:
+        b_gpu = eng.ERI_shell_block(*q, mode=mode)
+        b_orc = orc.shell_block(*q, mode=mode)
+        assert b_gpu.shape == b_orc.shape
+        np.testing.assert_allclose(b_gpu, b_orc, rtol=0, atol=TOL_INT, err_msg=str(q))
+
+
+@pytest.mark.parametrize("name,ncell", CASES)
+def test_direct_jk(systems, name, ncell):
+    sysm, eng, orc = _engines(systems, name, ncell)
+    P = random_density(sysm.nbas, seed=3)
+    J, K = eng.direct_JK(P)
+    Jo, Ko, _ = orc.direct_jk(P)
+    np.testing.assert_allclose(J, Jo, rtol=0, atol=TOL_JK)
+    np.testing.assert_allclose(K, Ko, rtol=0, atol=TOL_JK)
+    assert np.all(J[sysm.nfuc:] == 0) and np.all(K[sysm.nfuc:] == 0)
+
+
+@pytest.mark.parametrize("name,ncell", CASES[:3])
+@pytest.mark.parametrize("physicist", [False, True])
+def test_stored_eri_and_jk(systems, name, ncell, physicist):
+    import pyoracle
+    sysm, eng, orc = _engines(systems, name, ncell, physicist=physicist)
+    E = eng.ERI_integral_toroidal()
+    Eo, _ = orc.eri_stored()
+    assert E.shape == Eo.shape
+    np.testing.assert_allclose(E, Eo, rtol=0, atol=TOL_INT)
+    P = random_density(sysm.nbas, seed=5)
+    J, K = eng.stored_JK(P)
+    Jo, Ko = pyoracle.hartree_exchange(sysm.nfuc, P, Eo, physicist=physicist)
+    np.testing.assert_allclose(J, Jo, rtol=0, atol=TOL_JK)
+    np.testing.assert_allclose(K, Ko, rtol=0, atol=TOL_JK)
+
+
+def test_stored_nonsao_small(systems):
+    sysm, eng, orc = _engines(systems, "h_chain64", (4, 1, 1), sao=False)
+    E = eng.ERI_integral_toroidal()
+    Eo, _ = orc.eri_stored()
+    np.testing.assert_allclose(E, Eo, rtol=0, atol=TOL_INT)
+
+
+def test_direct_jk_full_chain64(systems):
+    """The 64-cell chain at full size (384 functions) against the oracle."""
+    sysm, eng, orc = _engines(systems, "h_chain64", None)
+    P = random_density(sysm.nbas, seed=11)
+    J, K = eng.direct_JK(P)
+    Jo, Ko, _ = orc.direct_jk(P)
+    np.testing.assert_allclose(J, Jo, rtol=0, atol=TOL_JK)
+    np.testing.assert_allclose(K, Ko, rtol=0, atol=TOL_JK)

@@ -1,0 +1,833 @@
+// tce_api.cu -- host side of libtce: the C ABI declared in include/tce.h.
+//
+// tce_create mirrors the set-up the reference does before its quartet loops
+// (direct_init eri_direct.f90:76-225; ERI_integral_toroidal
+// ERI_toroidal.f90:93-337): t-tables, shells, Schwarz bounds, primitive-pair
+// table, then the symmetry-unique quartet list, everything evaluated on the
+// device.  Host code here only sizes buffers, orders the work list and moves
+// data.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "tce_kernels.h"
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+
+struct Handle {
+    std::string err;
+    // system scalars
+    int ndp = 0, nq = 0, ncap = 0, nbas = 0, nfuc = 0, nsh = 0, nshuc = 0, ncell = 1;
+    int ncl[3] = {1, 1, 1};
+    double a[3] = {0, 0, 0}, L[3] = {0, 0, 0};
+    int physicist = 0, sao = 1, prim_screen = 1;
+    double thr = 1e-13, prim_thr = 1e-14;
+    // host copies
+    std::vector<double> ctr, exps, coefs, tnode, tweight;
+    std::vector<int> lxyz, poff;
+    std::vector<int> sh_first, sh_n, sh_l, sh_np, sh_eoff, sh_coff;
+    std::vector<double> sh_r, sh_exp, sh_coef, sh_cmax;
+    std::vector<UnitPair> up;
+    std::vector<double> Q, Qsh;
+    double Qmax = 0.0;
+    std::vector<int> tnmax;
+    // device
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int num_sms = 148;
+    std::vector<void *> allocs;
+    size_t bytes = 0;
+    DevSys S{};
+    PairPrim *d_pp = nullptr;
+    double *d_Qsh = nullptr;
+    int4 *d_items = nullptr;
+    long long nitems = 0;
+    int max_ncomb = 1;
+    long long n_func_q = 0, n_unit_sig = 0;
+    unsigned int *d_next = nullptr;
+    double *d_P = nullptr, *d_J = nullptr, *d_K = nullptr;
+    double *d_eri = nullptr;
+    long long eri_elems = 0;
+    int eri_size = 0;
+    double *d_blk = nullptr;
+    long long *d_blkoff = nullptr;
+    int4 *d_one = nullptr;
+    float last_ms = 0.f;
+};
+
+thread_local std::string g_err;
+
+int fail(Handle *h, int code, const std::string &msg)
+{
+    if (h) h->err = msg;
+    g_err = msg;
+    return code;
+}
+
+#define CK(h, call)                                                                          \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            return fail((h), TCE_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define CKS(h, call)                                                  \
+    do {                                                              \
+        int s_ = (call);                                              \
+        if (s_ != TCE_OK) {                                           \
+            cudaError_t e_ = cudaGetLastError();                      \
+            return fail((h), s_, std::string(#call) + " failed" +     \
+                                     (e_ != cudaSuccess ? std::string(": ") + cudaGetErrorString(e_) : "")); \
+        }                                                             \
+    } while (0)
+
+template <class T>
+int dalloc(Handle *h, T **p, size_t n)
+{
+    *p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(h, TCE_ERR_NOMEM, "device allocation of " + std::to_string(n * sizeof(T)) + " bytes failed: " +
+                                          cudaGetErrorString(e));
+    }
+    h->allocs.push_back(*p);
+    h->bytes += n * sizeof(T);
+    return TCE_OK;
+}
+
+template <class T>
+int upload(Handle *h, T **p, const std::vector<T> &v)
+{
+    int s = dalloc(h, p, v.size());
+    if (s) return s;
+    if (!v.empty()) CK(h, cudaMemcpyAsync(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, h->st));
+    return TCE_OK;
+}
+
+void dfree(Handle *h, void *p)
+{
+    if (!p) return;
+    cudaFree(p);
+    auto it = std::find(h->allocs.begin(), h->allocs.end(), p);
+    if (it != h->allocs.end()) h->allocs.erase(it);
+}
+
+// Gauss-Legendre nodes on [0,1] by Newton on P_n, mapped t = 0.6 u/(1-u)
+// (fast_quad_points, precompute_t.f90:906-942).
+void mapped_gauss_legendre(int n, std::vector<double> &t, std::vector<double> &w)
+{
+    const double scale = 0.6;
+    t.assign(n, 0.0);
+    w.assign(n, 0.0);
+    for (int i = 1; i <= n; ++i) {
+        double x = std::cos(kPi * (i - 0.25) / (n + 0.5));
+        double p0 = 1, p1 = x, dp = 1;
+        for (int it = 0; it < 100; ++it) {
+            p0 = 1.0;
+            p1 = x;
+            for (int j = 2; j <= n; ++j) {
+                double p2 = ((2.0 * j - 1.0) * x * p1 - (j - 1.0) * p0) / j;
+                p0 = p1;
+                p1 = p2;
+            }
+            dp = n * (x * p1 - p0) / (x * x - 1.0);
+            double dx = p1 / dp;
+            x -= dx;
+            if (std::fabs(dx) < 1e-15) break;
+        }
+        p0 = 1.0;
+        p1 = x;
+        for (int j = 2; j <= n; ++j) {
+            double p2 = ((2.0 * j - 1.0) * x * p1 - (j - 1.0) * p0) / j;
+            p0 = p1;
+            p1 = p2;
+        }
+        dp = n * (x * p1 - p0) / (x * x - 1.0);
+        double u = 0.5 * (1.0 - x);
+        double wu = 1.0 / ((1.0 - x * x) * dp * dp);
+        t[i - 1] = scale * u / (1.0 - u);
+        w[i - 1] = wu * scale / ((1.0 - u) * (1.0 - u));
+    }
+}
+
+int mod_pos(int a, int m) { int r = a % m; return r < 0 ? r + m : r; }
+
+// index shifted by -(cell of ref), cells x fastest (translate_to_unit_cell)
+int shift_to(const Handle *h, int idx, int refcell, int nblk)
+{
+    const int *ncl = h->ncl;
+    int tx = refcell % ncl[0], ty = (refcell / ncl[0]) % ncl[1], tz = refcell / (ncl[0] * ncl[1]);
+    int c = idx / nblk, loc = idx % nblk;
+    int cx = mod_pos(c % ncl[0] - tx, ncl[0]);
+    int cy = mod_pos((c / ncl[0]) % ncl[1] - ty, ncl[1]);
+    int cz = mod_pos(c / (ncl[0] * ncl[1]) - tz, ncl[2]);
+    return (cx + ncl[0] * (cy + ncl[1] * cz)) * nblk + loc;
+}
+
+// index shifted by +(cell ct) (shift_cell, eri_direct.f90:228-236)
+int shift_by(const Handle *h, int idx, int ct, int nblk)
+{
+    const int *ncl = h->ncl;
+    int c = idx / nblk, loc = idx % nblk;
+    int cx = mod_pos(c % ncl[0] + ct % ncl[0], ncl[0]);
+    int cy = mod_pos((c / ncl[0]) % ncl[1] + (ct / ncl[0]) % ncl[1], ncl[1]);
+    int cz = mod_pos(c / (ncl[0] * ncl[1]) + ct / (ncl[0] * ncl[1]), ncl[2]);
+    return (cx + ncl[0] * (cy + ncl[1] * cz)) * nblk + loc;
+}
+
+int ncomb_of(const Handle *h, int SI, int SJ, int SK, int SL)
+{
+    return (h->sh_l[SI] + 1) * (h->sh_l[SJ] + 1) * (h->sh_l[SK] + 1) * (h->sh_l[SL] + 1);
+}
+
+// run the quartet kernel on a host list of items in a block-output mode
+int run_blocks(Handle *h, const std::vector<int4> &items, const std::vector<int> *prim_sel, int mode, int prim_screen,
+               std::vector<double> *blocks, std::vector<long long> *offs)
+{
+    if (items.empty()) return TCE_OK;
+    std::vector<long long> off(items.size() + 1, 0);
+    int mx = 1;
+    for (size_t i = 0; i < items.size(); ++i) {
+        const int4 &q = items[i];
+        off[i + 1] = off[i] + (long long)h->sh_n[q.x] * h->sh_n[q.y] * h->sh_n[q.z] * h->sh_n[q.w];
+        mx = std::max(mx, ncomb_of(h, q.x, q.y, q.z, q.w));
+    }
+    int4 *d_it = nullptr;
+    int *d_sel = nullptr;
+    double *d_out = nullptr;
+    long long *d_off = nullptr;
+    int s;
+    if ((s = upload(h, &d_it, items))) return s;
+    if (prim_sel && (s = upload(h, &d_sel, *prim_sel))) return s;
+    if (mode != TCE_MODE_PRIMTAB) {
+        if ((s = dalloc(h, &d_out, (size_t)off.back()))) return s;
+        if ((s = upload(h, &d_off, off))) return s;
+    }
+    QuartetHostArgs a;
+    a.items = d_it;
+    a.prim_sel = d_sel;
+    a.nitems = (int)items.size();
+    a.mode = mode;
+    a.prim_screen = prim_screen;
+    a.next = h->d_next;
+    a.blk_out = d_out;
+    a.blk_off = d_off;
+    a.pp_rw = h->d_pp;
+    a.max_ncomb = mx;
+    a.num_sms = h->num_sms;
+    CKS(h, tce_launch_quartets(h->S, a, h->st));
+    if (blocks) {
+        blocks->resize(off.back());
+        CK(h, cudaMemcpyAsync(blocks->data(), d_out, off.back() * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    }
+    CK(h, cudaStreamSynchronize(h->st));
+    if (offs) *offs = off;
+    dfree(h, d_it);
+    dfree(h, d_sel);
+    dfree(h, d_out);
+    dfree(h, d_off);
+    return TCE_OK;
+}
+
+int build(Handle *h, const tce_system *sys)
+{
+    // ---------------- validate + copy ----------------
+    if (!sys) return fail(h, TCE_ERR_ARG, "sys is NULL");
+    if (sys->ndp < 1 || sys->ndp > 3) return fail(h, TCE_ERR_ARG, "ndp must be 1, 2 or 3");
+    if (sys->nbas <= 0 || sys->nfuc <= 0) return fail(h, TCE_ERR_ARG, "nbas and nfuc must be positive");
+    if (!sys->ctr || !sys->lxyz || !sys->prim_off || !sys->exps || !sys->coefs)
+        return fail(h, TCE_ERR_ARG, "NULL basis array");
+    h->ndp = sys->ndp;
+    h->nbas = sys->nbas;
+    h->nfuc = sys->nfuc;
+    for (int d = 0; d < 3; ++d) h->ncl[d] = sys->ncell[d] > 1 ? sys->ncell[d] : 1;
+    h->ncell = h->ncl[0] * h->ncl[1] * h->ncl[2];
+    if (h->nbas != h->nfuc * h->ncell)
+        return fail(h, TCE_ERR_UNSUPPORTED, "the shells must be the same in every cell (nbas != nfuc * ncell)");
+    for (int d = 0; d < 3; ++d) {
+        h->L[d] = sys->L[d];
+        h->a[d] = sys->L[d] > 0 ? 2.0 * kPi / sys->L[d] : 0.0;
+        if (d < h->ndp && !(sys->L[d] > 0)) return fail(h, TCE_ERR_ARG, "periodic length must be positive");
+    }
+    h->physicist = sys->physicist != 0;
+    h->sao = sys->sao != 0;
+    h->prim_screen = sys->prim_screen != 0;
+    h->thr = sys->schwarz_thr > 0 ? sys->schwarz_thr : 1e-13;
+    h->prim_thr = sys->prim_thr > 0 ? sys->prim_thr : 1e-14;
+    const int nbas = h->nbas;
+    h->ctr.assign(sys->ctr, sys->ctr + 3 * nbas);
+    h->lxyz.assign(sys->lxyz, sys->lxyz + 3 * nbas);
+    h->poff.assign(sys->prim_off, sys->prim_off + nbas + 1);
+    if (h->poff[0] != 0) return fail(h, TCE_ERR_ARG, "prim_off[0] must be 0");
+    for (int f = 0; f < nbas; ++f)
+        if (h->poff[f + 1] <= h->poff[f]) return fail(h, TCE_ERR_ARG, "every function needs at least one primitive");
+    int nprim = h->poff[nbas];
+    h->exps.assign(sys->exps, sys->exps + nprim);
+    h->coefs.assign(sys->coefs, sys->coefs + nprim);
+    for (int f = 0; f < nbas; ++f) {
+        int l = h->lxyz[3 * f] + h->lxyz[3 * f + 1] + h->lxyz[3 * f + 2];
+        if (h->lxyz[3 * f] < 0 || h->lxyz[3 * f + 1] < 0 || h->lxyz[3 * f + 2] < 0)
+            return fail(h, TCE_ERR_ARG, "negative Cartesian power");
+        if (l > TCE_LMAX) return fail(h, TCE_ERR_UNSUPPORTED, "angular momentum above d is not supported");
+    }
+    // nodes
+    if (sys->t_nodes) {
+        if (!sys->t_weights) return fail(h, TCE_ERR_ARG, "t_weights is NULL");
+        h->tnode.assign(sys->t_nodes, sys->t_nodes + sys->nquad);
+        h->tweight.assign(sys->t_weights, sys->t_weights + sys->nquad);
+    } else {
+        mapped_gauss_legendre(sys->nquad, h->tnode, h->tweight);
+    }
+    h->nq = sys->nquad;
+    if (h->nq != 32 && h->nq != 40 && h->nq != 64 && h->nq != 128)
+        return fail(h, TCE_ERR_UNSUPPORTED, "nquad must be 32, 40, 64 or 128");
+
+    // ---------------- shells (ERI_toroidal.f90:106-125) ----------------
+    for (int i = 0; i < nbas;) {
+        int lt = h->lxyz[3 * i] + h->lxyz[3 * i + 1] + h->lxyz[3 * i + 2];
+        int ncomp = (lt + 1) * (lt + 2) / 2;
+        bool same = (i + ncomp - 1 <= nbas - 1);
+        if (same)
+            for (int j = i + 1; j <= i + ncomp - 1 && same; ++j) {
+                int lj = h->lxyz[3 * j] + h->lxyz[3 * j + 1] + h->lxyz[3 * j + 2];
+                int npi = h->poff[i + 1] - h->poff[i], npj = h->poff[j + 1] - h->poff[j];
+                same = lj == lt && h->ctr[3 * j] == h->ctr[3 * i] && h->ctr[3 * j + 1] == h->ctr[3 * i + 1] &&
+                       h->ctr[3 * j + 2] == h->ctr[3 * i + 2] && npi == npj;
+                for (int p = 0; same && p < npi; ++p) same = h->exps[h->poff[j] + p] == h->exps[h->poff[i] + p];
+            }
+        if (!same) ncomp = 1;
+        h->sh_first.push_back(i);
+        h->sh_n.push_back(ncomp);
+        h->sh_l.push_back(lt);
+        i += ncomp;
+    }
+    h->nsh = (int)h->sh_first.size();
+    h->nshuc = 0;
+    for (int S = 0; S < h->nsh; ++S)
+        if (h->sh_first[S] < h->nfuc) ++h->nshuc;
+    bool sym_ok = (h->nsh == h->nshuc * h->ncell);
+    for (int S = 0; sym_ok && S < h->nsh - h->nshuc; ++S)
+        if (h->sh_n[S + h->nshuc] != h->sh_n[S] || h->sh_first[S + h->nshuc] != h->sh_first[S] + h->nfuc) sym_ok = false;
+    if (!sym_ok) return fail(h, TCE_ERR_UNSUPPORTED, "the shells must be the same in every cell");
+    for (int S = 0; S < h->nsh; ++S) {
+        int f = h->sh_first[S], np = h->poff[f + 1] - h->poff[f];
+        h->sh_np.push_back(np);
+        h->sh_eoff.push_back((int)h->sh_exp.size());
+        h->sh_coff.push_back((int)h->sh_coef.size());
+        for (int d = 0; d < 3; ++d) h->sh_r.push_back(h->ctr[3 * f + d]);
+        for (int p = 0; p < np; ++p) h->sh_exp.push_back(h->exps[h->poff[f] + p]);
+        for (int c = 0; c < h->sh_n[S]; ++c)
+            for (int p = 0; p < np; ++p) h->sh_coef.push_back(h->coefs[h->poff[f + c] + p]);
+        for (int p = 0; p < np; ++p) {
+            double m = 0.0;
+            for (int c = 0; c < h->sh_n[S]; ++c) m = std::max(m, std::fabs(h->coefs[h->poff[f + c] + p]));
+            h->sh_cmax.push_back(m);
+        }
+    }
+
+    // ---------------- t-table size (ERI_toroidal.f90:93-104) ----------------
+    int lmax = 0;
+    double emax = 0.0;
+    for (int f = 0; f < nbas; ++f) {
+        for (int d = 0; d < h->ndp; ++d) lmax = std::max(lmax, h->lxyz[3 * f + d]);
+        for (int p = h->poff[f]; p < h->poff[f + 1]; ++p) emax = std::max(emax, h->exps[p]);
+    }
+    double amin = h->a[0];
+    for (int d = 1; d < h->ndp; ++d) amin = std::min(amin, h->a[d]);
+    double Acap = 4.0 * emax / (amin * amin);
+    h->ncap = 20 + (int)std::ceil(9.0 * std::sqrt(Acap > 0 ? Acap : 0.0)) + 2 * lmax + 1;
+
+    // ---------------- device ----------------
+    int dev = 0;
+    CK(h, cudaGetDevice(&dev));
+    CK(h, cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, dev));
+    CK(h, cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+    CK(h, cudaEventCreate(&h->ev0));
+    CK(h, cudaEventCreate(&h->ev1));
+    int s;
+    DevSys &S = h->S;
+    S.ndp = h->ndp; S.nq = h->nq; S.ncap = h->ncap; S.nbas = nbas; S.nfuc = h->nfuc;
+    S.nsh = h->nsh; S.nshuc = h->nshuc; S.ncell = h->ncell;
+    for (int d = 0; d < 3; ++d) { S.ncl[d] = h->ncl[d]; S.a[d] = h->a[d]; S.L[d] = h->L[d]; }
+    S.fac_const = 2.0 / std::sqrt(kPi);
+    for (int d = 0; d < h->ndp; ++d) S.fac_const *= h->L[d] * h->L[d];
+    S.thr = h->thr;
+    S.prim_thr = h->prim_thr;
+    {
+        int *p;
+        double *q;
+        if ((s = upload(h, &p, h->sh_first))) return s; S.sh_first = p;
+        if ((s = upload(h, &p, h->sh_n))) return s; S.sh_n = p;
+        if ((s = upload(h, &p, h->sh_l))) return s; S.sh_l = p;
+        if ((s = upload(h, &p, h->sh_np))) return s; S.sh_np = p;
+        if ((s = upload(h, &p, h->sh_eoff))) return s; S.sh_eoff = p;
+        if ((s = upload(h, &p, h->sh_coff))) return s; S.sh_coff = p;
+        if ((s = upload(h, &q, h->sh_r))) return s; S.sh_r = q;
+        if ((s = upload(h, &q, h->sh_exp))) return s; S.sh_exp = q;
+        if ((s = upload(h, &q, h->sh_coef))) return s; S.sh_coef = q;
+        if ((s = upload(h, &q, h->sh_cmax))) return s; S.sh_cmax = q;
+        if ((s = upload(h, &p, h->lxyz))) return s; S.fn_pw = p;
+        if ((s = upload(h, &q, h->tnode))) return s; S.tnode = q;
+        if ((s = upload(h, &q, h->tweight))) return s; S.tweight = q;
+    }
+    if ((s = dalloc(h, &h->d_next, 1))) return s;
+
+    // ---------------- t-tables (setup_t_tables) ----------------
+    {
+        double *tb, *Tt;
+        int *tn;
+        if ((s = dalloc(h, &tb, (size_t)(h->ncap + 1) * h->nq * h->ndp))) return s;
+        if ((s = dalloc(h, &Tt, (size_t)(h->ncap + 1) * h->nq * h->ndp))) return s;
+        if ((s = dalloc(h, &tn, (size_t)h->nq * h->ndp))) return s;
+        CKS(h, tce_launch_t_tables(h->nq, h->ndp, h->ncap, S.tnode, h->a, tb, tn, Tt, h->st));
+        h->tnmax.resize((size_t)h->nq * h->ndp);
+        CK(h, cudaMemcpyAsync(h->tnmax.data(), tn, h->tnmax.size() * sizeof(int), cudaMemcpyDeviceToHost, h->st));
+        CK(h, cudaStreamSynchronize(h->st));
+        dfree(h, tb);
+        dfree(h, tn);
+        S.Tt = Tt;
+        for (int d = 0; d < 3; ++d)
+            for (int g = 0; g < TCE_MAXG; ++g) S.gmax[d][g] = -1;
+        for (int d = 0; d < h->ndp; ++d)
+            for (int g = 0; g < h->nq / 8; ++g) {
+                int m = 0;
+                for (int k = 8 * g; k < 8 * g + 8; ++k) m = std::max(m, h->tnmax[(size_t)d * h->nq + k]);
+                S.gmax[d][g] = m;
+            }
+    }
+
+    // ---------------- unit pairs + primitive-pair scalars ----------------
+    const int nreal = 3 - h->ndp;
+    long long npp_tot = 0, e_tot = 0;
+    std::vector<int> pp_unit;
+    for (int S1 = 0; S1 < h->nshuc; ++S1)
+        for (int S2 = 0; S2 < h->nsh; ++S2) {
+            UnitPair U{};
+            U.S1 = S1; U.S2 = S2; U.l1 = h->sh_l[S1]; U.l2 = h->sh_l[S2];
+            U.np1 = h->sh_np[S1]; U.np2 = h->sh_np[S2]; U.npp = U.np1 * U.np2;
+            U.pp_off = npp_tot;
+            U.e_off = e_tot;
+            npp_tot += U.npp;
+            e_tot += (long long)U.npp * nreal * (U.l1 + 1) * (U.l2 + 1) * TCE_ECO;
+            for (int p = 0; p < U.npp; ++p) pp_unit.push_back((int)h->up.size());
+            h->up.push_back(U);
+        }
+    int *d_ppu = nullptr;
+    UnitPair *d_up = nullptr;
+    double *d_e = nullptr;
+    if ((s = upload(h, &d_ppu, pp_unit))) return s;
+    if ((s = upload(h, &d_up, h->up))) return s;
+    if ((s = dalloc(h, &h->d_pp, (size_t)npp_tot))) return s;
+    if ((s = dalloc(h, &d_e, (size_t)e_tot))) return s;
+    S.up = d_up;
+    S.pp = h->d_pp;
+    S.ecoef = d_e;
+    CKS(h, tce_launch_pair_scalars(S, npp_tot, d_ppu, h->d_pp, d_up, d_e, h->st));
+    std::vector<PairPrim> hpp((size_t)npp_tot);
+    CK(h, cudaMemcpyAsync(hpp.data(), h->d_pp, npp_tot * sizeof(PairPrim), cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    long long v_tot = 0;
+    for (auto &U : h->up) {
+        int nmax = 0;
+        double km = 0.0;
+        for (int p = 0; p < U.npp; ++p) {
+            const PairPrim &P = hpp[U.pp_off + p];
+            for (int d = 0; d < h->ndp; ++d) nmax = std::max(nmax, P.N[d]);
+            km = std::max(km, std::fabs(P.pfac) * P.cmax12);
+        }
+        U.Nlen = nmax + 1;
+        U.ket_max = km;
+        U.vec_off = v_tot;
+        v_tot += (long long)h->ndp * (U.l1 + 1) * (U.l2 + 1) * 2 * U.Nlen * U.npp;
+    }
+    CK(h, cudaMemcpyAsync(d_up, h->up.data(), h->up.size() * sizeof(UnitPair), cudaMemcpyHostToDevice, h->st));
+    double2 *d_vec = nullptr;
+    if ((s = dalloc(h, &d_vec, (size_t)v_tot))) return s;
+    S.vec = d_vec;
+    {
+        int stride = h->ncap + 2 * TCE_LMAX + 2;
+        double *scr = nullptr;
+        if ((s = dalloc(h, &scr, (size_t)npp_tot * h->ndp * stride))) return s;
+        CKS(h, tce_launch_pair_vectors(S, npp_tot, d_ppu, h->d_pp, stride, scr, d_vec, h->st));
+        CK(h, cudaStreamSynchronize(h->st));
+        dfree(h, scr);
+    }
+
+    // ---------------- Schwarz: diagonal blocks, SI in the unit cell (ERI_toroidal.f90:200-236) ----------
+    {
+        std::vector<int4> items;
+        for (int SI = 0; SI < h->nshuc; ++SI)
+            for (int SJ = 0; SJ < h->nsh; ++SJ) items.push_back(make_int4(SI, SJ, SI, SJ));
+        std::vector<double> blocks;
+        std::vector<long long> off;
+        if ((s = run_blocks(h, items, nullptr, TCE_MODE_BLOCK, 0, &blocks, &off))) return s;
+        h->Q.assign((size_t)nbas * nbas, 0.0);
+        for (size_t it = 0; it < items.size(); ++it) {
+            int SI = items[it].x, SJ = items[it].y, ni = h->sh_n[SI], nj = h->sh_n[SJ];
+            for (int a = 0; a < ni; ++a)
+                for (int b = 0; b < nj; ++b) {
+                    double qv = std::sqrt(std::fabs(blocks[off[it] + a + ni * (b + nj * (a + ni * b))]));
+                    int i = h->sh_first[SI] + a, j = h->sh_first[SJ] + b;
+                    for (int ct = 0; ct < h->ncell; ++ct) {
+                        int ii = shift_by(h, i, ct, h->nfuc), jj = shift_by(h, j, ct, h->nfuc);
+                        h->Q[ii + (size_t)nbas * jj] = qv;
+                        h->Q[jj + (size_t)nbas * ii] = qv;
+                    }
+                }
+        }
+        h->Qsh.assign((size_t)h->nsh * h->nsh, 0.0);
+        h->Qmax = 0.0;
+        for (int SI = 0; SI < h->nsh; ++SI)
+            for (int SJ = 0; SJ < h->nsh; ++SJ) {
+                double m = 0.0;
+                for (int a = 0; a < h->sh_n[SI]; ++a)
+                    for (int b = 0; b < h->sh_n[SJ]; ++b)
+                        m = std::max(m, h->Q[(h->sh_first[SI] + a) + (size_t)nbas * (h->sh_first[SJ] + b)]);
+                h->Qsh[SI + (size_t)h->nsh * SJ] = m;
+                h->Qmax = std::max(h->Qmax, m);
+            }
+        double *dQ;
+        if ((s = upload(h, &dQ, h->Q))) return s;
+        S.Q = dQ;
+        if ((s = upload(h, &h->d_Qsh, h->Qsh))) return s;
+        for (auto &U : h->up)
+            if (h->Qsh[U.S1 + (size_t)h->nsh * U.S2] * h->Qmax >= h->thr) ++h->n_unit_sig;
+    }
+
+    // ---------------- primitive Schwarz table (ERI_toroidal.f90:296-337) ----------------
+    if (h->prim_screen) {
+        std::vector<int4> items;
+        std::vector<int> sel;
+        for (const auto &U : h->up)
+            for (int p1 = 0; p1 < U.np1; ++p1)
+                for (int p2 = 0; p2 < U.np2; ++p2) {
+                    items.push_back(make_int4(U.S1, U.S2, U.S1, U.S2));
+                    sel.push_back(p1);
+                    sel.push_back(p2);
+                }
+        if ((s = run_blocks(h, items, &sel, TCE_MODE_PRIMTAB, 0, nullptr, nullptr))) return s;
+    }
+
+    // ---------------- unique quartets (ERI_toroidal.f90:342-401) ----------------
+    {
+        unsigned long long *d_cnt = nullptr;
+        if ((s = dalloc(h, &d_cnt, 2))) return s;
+        CK(h, cudaMemsetAsync(d_cnt, 0, 2 * sizeof(unsigned long long), h->st));
+        CKS(h, tce_launch_enumerate(S, h->d_Qsh, h->Qmax, nullptr, d_cnt, 0ull, d_cnt + 1, h->st));
+        unsigned long long cnt[2];
+        CK(h, cudaMemcpyAsync(cnt, d_cnt, sizeof cnt, cudaMemcpyDeviceToHost, h->st));
+        CK(h, cudaStreamSynchronize(h->st));
+        h->nitems = (long long)cnt[0];
+        h->n_func_q = (long long)cnt[1];
+        if (h->nitems > 0x7fffffffLL) return fail(h, TCE_ERR_UNSUPPORTED, "more than 2^31 unique shell quartets");
+        int4 *d_raw = nullptr;
+        if ((s = dalloc(h, &d_raw, (size_t)h->nitems))) return s;
+        CK(h, cudaMemsetAsync(d_cnt, 0, 2 * sizeof(unsigned long long), h->st));
+        CKS(h, tce_launch_enumerate(S, h->d_Qsh, h->Qmax, d_raw, d_cnt, (unsigned long long)h->nitems, d_cnt + 1, h->st));
+        std::vector<int4> items((size_t)h->nitems);
+        CK(h, cudaMemcpyAsync(items.data(), d_raw, items.size() * sizeof(int4), cudaMemcpyDeviceToHost, h->st));
+        CK(h, cudaStreamSynchronize(h->st));
+        dfree(h, d_raw);
+        dfree(h, d_cnt);
+        // order: most expensive first (dynamic scheduling, LPT); cost ~ pairs x rows x vector length
+        std::vector<double> cost(items.size());
+        for (size_t i = 0; i < items.size(); ++i) {
+            const int4 &q = items[i];
+            int cK = q.z / h->nshuc, SK0 = q.z % h->nshuc, SLp = shift_to(h, q.w, cK, h->nshuc);
+            const UnitPair &Ub = h->up[(size_t)q.x * h->nsh + q.y];
+            const UnitPair &Uk = h->up[(size_t)SK0 * h->nsh + SLp];
+            int nc = ncomb_of(h, q.x, q.y, q.z, q.w);
+            h->max_ncomb = std::max(h->max_ncomb, nc);
+            cost[i] = (double)Ub.npp * Uk.npp * nc * h->ndp * std::min(Ub.Nlen, Uk.Nlen);
+        }
+        std::vector<size_t> ord(items.size());
+        std::iota(ord.begin(), ord.end(), 0);
+        std::stable_sort(ord.begin(), ord.end(), [&](size_t x, size_t y) { return cost[x] > cost[y]; });
+        std::vector<int4> sorted(items.size());
+        for (size_t i = 0; i < ord.size(); ++i) sorted[i] = items[ord[i]];
+        if ((s = upload(h, &h->d_items, sorted))) return s;
+    }
+    if ((s = dalloc(h, &h->d_P, (size_t)nbas * nbas))) return s;
+    if ((s = dalloc(h, &h->d_J, (size_t)h->nfuc * nbas))) return s;
+    if ((s = dalloc(h, &h->d_K, (size_t)h->nfuc * nbas))) return s;
+    if ((s = dalloc(h, &h->d_one, 1))) return s;
+    if ((s = dalloc(h, &h->d_blkoff, 2))) return s;
+    {
+        long long z[2] = {0, 0};
+        CK(h, cudaMemcpyAsync(h->d_blkoff, z, sizeof z, cudaMemcpyHostToDevice, h->st));
+    }
+    if ((s = dalloc(h, &h->d_blk, (size_t)TCE_NCOMP_MAX * TCE_NCOMP_MAX * TCE_NCOMP_MAX * TCE_NCOMP_MAX))) return s;
+    CK(h, cudaStreamSynchronize(h->st));
+    return TCE_OK;
+}
+
+int direct_jk_device(Handle *h, const double *dP, double *dJ, double *dK, cudaStream_t st)
+{
+    CK(h, cudaMemsetAsync(dJ, 0, sizeof(double) * h->nfuc * h->nbas, st));
+    CK(h, cudaMemsetAsync(dK, 0, sizeof(double) * h->nfuc * h->nbas, st));
+    if (h->nitems == 0) return TCE_OK;
+    QuartetHostArgs a;
+    a.items = h->d_items;
+    a.nitems = (int)h->nitems;
+    a.mode = TCE_MODE_JK;
+    a.prim_screen = h->prim_screen;
+    a.next = h->d_next;
+    a.P = dP;
+    a.J = dJ;
+    a.K = dK;
+    a.max_ncomb = h->max_ncomb;
+    a.num_sms = h->num_sms;
+    CK(h, cudaEventRecord(h->ev0, st));
+    CKS(h, tce_launch_quartets(h->S, a, st));
+    CK(h, cudaEventRecord(h->ev1, st));
+    return TCE_OK;
+}
+
+}  // namespace
+
+// ============================================================================
+// C ABI
+// ============================================================================
+extern "C" {
+
+const char *tce_version(void) { return "libtce 0.1 (sm_100a, FP64 toroidal ERI / J-K engine)"; }
+
+const char *tce_last_error(void *handle)
+{
+    if (handle) return static_cast<Handle *>(handle)->err.c_str();
+    return g_err.c_str();
+}
+
+int tce_create(const tce_system *sys, void **handle)
+{
+    if (!handle) return fail(nullptr, TCE_ERR_ARG, "handle is NULL");
+    *handle = nullptr;
+    Handle *h = new Handle();
+    int s = build(h, sys);
+    if (s != TCE_OK) {
+        g_err = h->err;
+        for (void *p : h->allocs) cudaFree(p);
+        if (h->st) cudaStreamDestroy(h->st);
+        if (h->ev0) cudaEventDestroy(h->ev0);
+        if (h->ev1) cudaEventDestroy(h->ev1);
+        delete h;
+        return s;
+    }
+    *handle = h;
+    return TCE_OK;
+}
+
+int tce_destroy(void *handle)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h) return TCE_OK;
+    if (h->st) cudaStreamSynchronize(h->st);
+    for (void *p : h->allocs) cudaFree(p);
+    if (h->st) cudaStreamDestroy(h->st);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    delete h;
+    return TCE_OK;
+}
+
+int tce_get_info(void *handle, tce_info *info)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !info) return fail(h, TCE_ERR_ARG, "NULL argument");
+    info->nsh = h->nsh;
+    info->nshuc = h->nshuc;
+    info->ncap = h->ncap;
+    info->nquad = h->nq;
+    info->n_shell_quartets = h->nitems;
+    info->n_func_quartets = h->n_func_q;
+    info->n_unit_pairs = h->n_unit_sig;
+    info->device_bytes = (int64_t)h->bytes;
+    return TCE_OK;
+}
+
+int tce_shells(void *handle, int32_t *first, int32_t *n)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !first || !n) return fail(h, TCE_ERR_ARG, "NULL argument");
+    for (int S = 0; S < h->nsh; ++S) {
+        first[S] = h->sh_first[S];
+        n[S] = h->sh_n[S];
+    }
+    return TCE_OK;
+}
+
+int tce_schwarz(void *handle, double *Q)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !Q) return fail(h, TCE_ERR_ARG, "NULL argument");
+    std::memcpy(Q, h->Q.data(), h->Q.size() * sizeof(double));
+    return TCE_OK;
+}
+
+int tce_shell_block(void *handle, const int32_t sh4[4], int32_t mode, double *blk)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !sh4 || !blk) return fail(h, TCE_ERR_ARG, "NULL argument");
+    for (int i = 0; i < 4; ++i)
+        if (sh4[i] < 0 || sh4[i] >= h->nsh) return fail(h, TCE_ERR_ARG, "shell index out of range");
+    if (mode < 0 || mode > 2) return fail(h, TCE_ERR_ARG, "mode must be 0, 1 or 2");
+    if (mode == 1 && !h->prim_screen) return fail(h, TCE_ERR_STATE, "mode 1 needs prim_screen");
+    // translate the quartet so that S1 lies in the unit cell (values are translation invariant)
+    int c1 = sh4[0] / h->nshuc;
+    int4 q = make_int4(shift_to(h, sh4[0], c1, h->nshuc), shift_to(h, sh4[1], c1, h->nshuc),
+                       shift_to(h, sh4[2], c1, h->nshuc), shift_to(h, sh4[3], c1, h->nshuc));
+    std::vector<int4> items{q};
+    std::vector<double> blocks;
+    int s = run_blocks(h, items, nullptr, mode == 2 ? TCE_MODE_NOSCREEN : TCE_MODE_BLOCK, mode == 1, &blocks, nullptr);
+    if (s) return s;
+    std::memcpy(blk, blocks.data(), blocks.size() * sizeof(double));
+    return TCE_OK;
+}
+
+int tce_direct_jk_device(void *handle, const double *dP, double *dJ, double *dK, void *stream)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !dP || !dJ || !dK) return fail(h, TCE_ERR_ARG, "NULL argument");
+    return direct_jk_device(h, dP, dJ, dK, static_cast<cudaStream_t>(stream));
+}
+
+int tce_direct_jk(void *handle, const double *P, double *J, double *K)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !P || !J || !K) return fail(h, TCE_ERR_ARG, "NULL argument");
+    const int n = h->nbas, nf = h->nfuc;
+    CK(h, cudaMemcpyAsync(h->d_P, P, sizeof(double) * n * n, cudaMemcpyHostToDevice, h->st));
+    int s = direct_jk_device(h, h->d_P, h->d_J, h->d_K, h->st);
+    if (s) return s;
+    std::memset(J, 0, sizeof(double) * n * n);
+    std::memset(K, 0, sizeof(double) * n * n);
+    // rows < nfuc: device leading dimension nf -> host leading dimension n
+    CK(h, cudaMemcpy2DAsync(J, sizeof(double) * n, h->d_J, sizeof(double) * nf, sizeof(double) * nf, n,
+                            cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaMemcpy2DAsync(K, sizeof(double) * n, h->d_K, sizeof(double) * nf, sizeof(double) * nf, n,
+                            cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    return TCE_OK;
+}
+
+int tce_last_kernel_ms(void *handle, double *ms)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !ms) return fail(h, TCE_ERR_ARG, "NULL argument");
+    float f = 0.f;
+    CK(h, cudaEventSynchronize(h->ev1));
+    CK(h, cudaEventElapsedTime(&f, h->ev0, h->ev1));
+    *ms = f;
+    return TCE_OK;
+}
+
+int tce_eri_stored(void *handle, int64_t eri_size, double *eri)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !eri) return fail(h, TCE_ERR_ARG, "NULL argument");
+    int esz = h->sao ? h->nfuc : h->nbas;
+    if (eri_size != esz) return fail(h, TCE_ERR_ARG, "eri_size must be nfuc (sao) or nbas");
+    const long long n = h->nbas;
+    long long elems = (long long)esz * n * n * n;
+    if (!h->d_eri || h->eri_elems != elems) {
+        if (h->d_eri) dfree(h, h->d_eri);
+        h->d_eri = nullptr;
+        int s = dalloc(h, &h->d_eri, (size_t)elems);
+        if (s) return s;
+        h->eri_elems = elems;
+    }
+    h->eri_size = esz;
+    CK(h, cudaMemsetAsync(h->d_eri, 0, sizeof(double) * elems, h->st));
+    if (h->nitems > 0) {
+        QuartetHostArgs a;
+        a.items = h->d_items;
+        a.nitems = (int)h->nitems;
+        a.mode = TCE_MODE_STORE;
+        a.prim_screen = h->prim_screen;
+        a.next = h->d_next;
+        a.eri = h->d_eri;
+        a.eri_size = esz;
+        a.physicist = h->physicist;
+        a.max_ncomb = h->max_ncomb;
+        a.num_sms = h->num_sms;
+        CKS(h, tce_launch_quartets(h->S, a, h->st));
+    }
+    if (!h->sao) CKS(h, tce_launch_sym_fill(h->nbas, h->nfuc, h->ncl, h->d_eri, h->st));
+    CK(h, cudaMemcpyAsync(eri, h->d_eri, sizeof(double) * elems, cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    return TCE_OK;
+}
+
+int tce_stored_jk(void *handle, const double *P, double *J, double *K)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !P || !J || !K) return fail(h, TCE_ERR_ARG, "NULL argument");
+    if (!h->d_eri) return fail(h, TCE_ERR_STATE, "tce_eri_stored has not been called");
+    const int n = h->nbas, n1 = h->eri_size;
+    double *dJ = nullptr, *dK = nullptr;
+    int s;
+    if ((s = dalloc(h, &dJ, (size_t)n1 * n))) return s;
+    if ((s = dalloc(h, &dK, (size_t)n1 * n))) return s;
+    CK(h, cudaMemcpyAsync(h->d_P, P, sizeof(double) * n * n, cudaMemcpyHostToDevice, h->st));
+    CK(h, cudaMemsetAsync(dJ, 0, sizeof(double) * n1 * n, h->st));
+    CK(h, cudaMemsetAsync(dK, 0, sizeof(double) * n1 * n, h->st));
+    CKS(h, tce_launch_stored_jk(n1, n, h->physicist, h->d_P, h->d_eri, dJ, dK, h->st));
+    std::memset(J, 0, sizeof(double) * n * n);
+    std::memset(K, 0, sizeof(double) * n * n);
+    CK(h, cudaMemcpy2DAsync(J, sizeof(double) * n, dJ, sizeof(double) * n1, sizeof(double) * n1, n,
+                            cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaMemcpy2DAsync(K, sizeof(double) * n, dK, sizeof(double) * n1, sizeof(double) * n1, n,
+                            cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    dfree(h, dJ);
+    dfree(h, dK);
+    return TCE_OK;
+}
+
+int tce_hartree_exchange(int32_t n1, int32_t nbas, int32_t physicist, const double *P, const double *eri, double *J,
+                         double *K)
+{
+    if (n1 <= 0 || nbas <= 0 || n1 > nbas || !P || !eri || !J || !K)
+        return fail(nullptr, TCE_ERR_ARG, "bad argument");
+    Handle tmp;
+    Handle *h = &tmp;
+    CK(h, cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+    long long elems = (long long)n1 * nbas * nbas * nbas;
+    double *dE = nullptr, *dP = nullptr, *dJ = nullptr, *dK = nullptr;
+    int s = TCE_OK;
+    auto cleanup = [&]() {
+        for (void *p : h->allocs) cudaFree(p);
+        cudaStreamDestroy(h->st);
+    };
+    if ((s = dalloc(h, &dE, (size_t)elems)) || (s = dalloc(h, &dP, (size_t)nbas * nbas)) ||
+        (s = dalloc(h, &dJ, (size_t)n1 * nbas)) || (s = dalloc(h, &dK, (size_t)n1 * nbas))) {
+        cleanup();
+        return s;
+    }
+    cudaMemcpyAsync(dE, eri, sizeof(double) * elems, cudaMemcpyHostToDevice, h->st);
+    cudaMemcpyAsync(dP, P, sizeof(double) * nbas * nbas, cudaMemcpyHostToDevice, h->st);
+    cudaMemsetAsync(dJ, 0, sizeof(double) * n1 * nbas, h->st);
+    cudaMemsetAsync(dK, 0, sizeof(double) * n1 * nbas, h->st);
+    s = tce_launch_stored_jk(n1, nbas, physicist, dP, dE, dJ, dK, h->st);
+    std::memset(J, 0, sizeof(double) * nbas * nbas);
+    std::memset(K, 0, sizeof(double) * nbas * nbas);
+    cudaMemcpy2DAsync(J, sizeof(double) * nbas, dJ, sizeof(double) * n1, sizeof(double) * n1, nbas,
+                      cudaMemcpyDeviceToHost, h->st);
+    cudaMemcpy2DAsync(K, sizeof(double) * nbas, dK, sizeof(double) * n1, sizeof(double) * n1, nbas,
+                      cudaMemcpyDeviceToHost, h->st);
+    cudaError_t e = cudaStreamSynchronize(h->st);
+    cleanup();
+    if (s != TCE_OK) return fail(nullptr, s, "stored J/K launch failed");
+    if (e != cudaSuccess) return fail(nullptr, TCE_ERR_CUDA, cudaGetErrorString(e));
+    return TCE_OK;
+}
+
+}  // extern "C"

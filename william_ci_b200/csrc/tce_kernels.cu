@@ -1,0 +1,836 @@
+// tce_kernels.cu -- sm_100a kernels of the toroidal ERI engine.
+//
+//   k_t_bessel     t-tables: e^{-C} I_n(C), C = 2 t_k^2 / a_d^2, Miller recurrence
+//                  (setup_t_tables, clifford_tools.f90:620-709)
+//   k_t_finish     truncation orders and the T table c_n I~_n(C_k)
+//   k_pair_scalars primitive-pair barycentres, prefactors, truncation orders
+//                  and real-direction Hermite coefficients
+//   k_pair_bessel  I~_n(A) per primitive pair and direction (bessel_scaled_vector_fast)
+//   k_pair_vectors Fourier pair vectors (pair_vector_cached / fourier_sin_product)
+//   k_enumerate    symmetry-unique shell quartets + Schwarz screen
+//                  (ERI_toroidal.f90:342-401, eri_direct.f90:298-326)
+//   k_quartets     the quartet kernel: ERI_shell_block_toroidal
+//                  (ERI_shell_block_toroidal.f90:28-366) for one shell quartet per
+//                  warp, fused with its consumer (J/K scatter eri_direct.f90:331-357,
+//                  stored-ERI scatter ERI_toroidal.f90:416-454, Schwarz blocks,
+//                  primitive Schwarz table)
+//   k_stored_jk    J/K from stored ERIs (hartree_exchange_potential.f90:157-200)
+//   k_sym_fill     rows i > nfuc by translation (symmetric_matrix.f90:62-131)
+#include "tce_device.cuh"
+#include "tce_kernels.h"
+
+#define PI_D 3.14159265358979323846
+
+// ============================================================================
+// t-tables
+// ============================================================================
+// one thread per (node k, direction d): Miller recurrence from n0 = ncap + 30 +
+// int(sqrt(80 C)) down, storing n <= ncap, normalised with e^{-C} I_0(C).
+__global__ void k_t_bessel(int nq, int ndp, int ncap, const double *tnode, double a0, double a1, double a2,
+                           double *tb /* [(d*nq + k)*(ncap+1) + n] */)
+{
+    int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= nq * ndp) return;
+    int d = id / nq, k = id % nq;
+    double a = d == 0 ? a0 : (d == 1 ? a1 : a2);
+    double C = 2.0 * tnode[k] * tnode[k] / (a * a);
+    double *w = tb + (size_t)id * (ncap + 1);
+    if (C < 1e-12) {
+        for (int n = 0; n <= ncap; ++n) w[n] = 0.0;
+        w[0] = 1.0;
+        return;
+    }
+    long long n0 = (long long)ncap + 30 + (long long)sqrt(80.0 * C);
+    double ip1 = 0.0, ik = 1e-300, im1;
+    if (n0 <= ncap) w[n0] = ik;
+    for (long long kk = n0; kk >= 1; --kk) {
+        im1 = ip1 + (2.0 * (double)kk / C) * ik;
+        ip1 = ik;
+        ik = im1;
+        if (kk - 1 <= ncap) w[kk - 1] = ik;
+        if (fabs(ik) > 1e250) {
+            long long lo = kk - 1, hi = n0 < ncap ? n0 : ncap;
+            for (long long m = lo; m <= hi; ++m) w[m] *= 1e-250;
+            ip1 *= 1e-250;
+            ik *= 1e-250;
+        }
+    }
+    double norm = tce_iv0_scaled(C) / w[0];
+    for (int n = 0; n <= ncap; ++n) w[n] *= norm;
+}
+
+// truncation order t_nmax (1e-16 relative, +5) and the T table
+__global__ void k_t_finish(int nq, int ndp, int ncap, const double *tb, int *tnmax, double *Tt)
+{
+    int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= nq * ndp) return;
+    int d = id / nq, k = id % nq;
+    const double *w = tb + (size_t)id * (ncap + 1);
+    int nm = ncap;
+    for (int n = 0; n <= ncap; ++n)
+        if (w[n] < 1e-16 * w[0]) { nm = (n + 5 < ncap) ? n + 5 : ncap; break; }
+    tnmax[id] = nm;
+    for (int n = 0; n <= ncap; ++n) {
+        double v = (n == 0) ? w[0] : (n <= nm ? 2.0 * w[n] : 0.0);
+        Tt[((size_t)d * (ncap + 1) + n) * nq + k] = v;
+    }
+}
+
+// ============================================================================
+// primitive pairs
+// ============================================================================
+// one thread per (unit pair u, primitive pair pp)
+__global__ void k_pair_scalars(DevSys S, long long npp_tot, const int *pp_unit, PairPrim *pp,
+                               const UnitPair *upc, double *ecoef)
+{
+    long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= npp_tot) return;
+    int u = pp_unit[id];
+    const UnitPair U = upc[u];
+    int loc = (int)(id - U.pp_off);
+    int i = loc / U.np2, j = loc % U.np2;
+    int S1 = U.S1, S2 = U.S2;
+    double e1 = S.sh_exp[S.sh_eoff[S1] + i], e2 = S.sh_exp[S.sh_eoff[S2] + j];
+    double esum = e1 + e2, mu = e1 * e2 / esum;
+    PairPrim P;
+    P.esum = esum;
+    P.cmax12 = S.sh_cmax[S.sh_eoff[S1] + i] * S.sh_cmax[S.sh_eoff[S2] + j];
+    P.ps = 0.0;
+    P.pad = 0;
+    double pf = 1.0;
+    const double *r1 = S.sh_r + 3 * S1, *r2 = S.sh_r + 3 * S2;
+    for (int d = 0; d < 3; ++d) {
+        P.A[d] = 0.0;
+        P.N[d] = 0;
+        if (d < S.ndp) {
+            double pe, cen;
+            tce_bary(e1, e2, r1[d], r2[d], S.L[d], S.a[d], pe, cen);
+            P.cen[d] = cen;
+            pf *= exp(-2.0 * (esum - pe) / (S.a[d] * S.a[d]));
+            double A = 2.0 * pe / (S.a[d] * S.a[d]);
+            int est = tce_nmax_estimate(A);
+            P.A[d] = A;
+            P.N[d] = est < S.ncap ? est : S.ncap;
+        } else {
+            double cen = (e1 * r1[d] + e2 * r2[d]) / esum;
+            P.cen[d] = cen;
+            pf *= exp(-mu * (r1[d] - r2[d]) * (r1[d] - r2[d]));
+            // Hermite E for every (ia, ib) of this pair, real direction dr
+            int dr = d - S.ndp, nreal = 3 - S.ndp;
+            for (int ia = 0; ia <= U.l1; ++ia)
+                for (int ib = 0; ib <= U.l2; ++ib) {
+                    double *E = ecoef + U.e_off +
+                                ((((long long)loc * nreal + dr) * (U.l1 + 1) + ia) * (U.l2 + 1) + ib) * TCE_ECO;
+                    tce_hermite_E(ia, ib, esum, cen - r1[d], cen - r2[d], E);
+                }
+        }
+    }
+    P.pfac = pf;
+    pp[id] = P;
+}
+
+// one thread per (pp, periodic d): I~_n(A), n = 0..Nstart, Nstart = N + l1 + l2
+// (bessel_scaled_vector_fast, clifford_tools.f90:429-461), into scratch
+__global__ void k_pair_bessel(DevSys S, long long npp_tot, const int *pp_unit, const PairPrim *pp,
+                              int stride, double *scratch)
+{
+    long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= npp_tot * S.ndp) return;
+    long long p = id / S.ndp;
+    int d = (int)(id % S.ndp);
+    int u = pp_unit[p];
+    const UnitPair U = S.up[u];
+    int N = pp[p].N[d] + U.l1 + U.l2;
+    double A = pp[p].A[d];
+    double *Iv = scratch + (size_t)id * stride;
+    if (A < 1e-10) {
+        for (int k = 0; k <= N; ++k) Iv[k] = 0.0;
+        Iv[0] = 1.0;
+        return;
+    }
+    if (N < 2) {   // not reached for the ERI truncation orders (N >= 20)
+        for (int k = 0; k <= N; ++k) Iv[k] = 0.0;
+        Iv[0] = tce_iv0_scaled(A);
+        return;
+    }
+    double inv_A2 = 2.0 / A;
+    Iv[N] = 1e-280;
+    Iv[N - 1] = Iv[N] * (double)N * inv_A2;
+    for (int k = N - 1; k >= 1; --k) {
+        Iv[k - 1] = Iv[k + 1] + (double)k * inv_A2 * Iv[k];
+        if (Iv[k - 1] > 1e250)
+            for (int m = k - 1; m <= N; ++m) Iv[m] *= 1e-250;
+    }
+    double s = tce_iv0_scaled(A) / Iv[0];
+    for (int k = 0; k <= N; ++k) Iv[k] *= s;
+}
+
+// one thread per (pp, d, ia, ib, sign): V_n = sum_k d_k I~_{|n - s k|}, n < Nlen
+// (zero beyond the pair's own N), written n-major into the unit pair's slab.
+__global__ void k_pair_vectors(DevSys S, long long npp_tot, const int *pp_unit, const PairPrim *pp, int stride,
+                               const double *scratch, double2 *vec)
+{
+    const int NV = (TCE_LMAX + 1) * (TCE_LMAX + 1) * 2;
+    long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= npp_tot * S.ndp * NV) return;
+    int v = (int)(id % NV);
+    long long rest = id / NV;
+    int d = (int)(rest % S.ndp);
+    long long p = rest / S.ndp;
+    int s = v % 2, ib = (v / 2) % (TCE_LMAX + 1), ia = v / (2 * (TCE_LMAX + 1));
+    int u = pp_unit[p];
+    const UnitPair U = S.up[u];
+    if (ia > U.l1 || ib > U.l2) return;
+    int loc = (int)(p - U.pp_off);
+    const PairPrim P = pp[p];
+    const double *Iv = scratch + (size_t)(p * S.ndp + d) * stride;
+    int N = P.N[d], M = ia + ib, sg = s == 0 ? -1 : 1;
+    double2 *out = vec + U.vec_off +
+                   ((((long long)d * (U.l1 + 1) + ia) * (U.l2 + 1) + ib) * 2 + s) * (long long)U.Nlen * U.npp;
+    double dre[4 * TCE_LMAX + 1], dim[4 * TCE_LMAX + 1];
+    if (M > 0) {
+        const double *r1 = S.sh_r + 3 * U.S1, *r2 = S.sh_r + 3 * U.S2;
+        tce_fourier_sin(ia, ib, S.a[d] * (P.cen[d] - r1[d]), S.a[d] * (P.cen[d] - r2[d]), dre, dim);
+    }
+    for (int n = 0; n < U.Nlen; ++n) {
+        double2 val = make_double2(0.0, 0.0);
+        if (n <= N) {
+            if (M == 0) val.x = Iv[n];
+            else
+                for (int kk = -M; kk <= M; ++kk) {
+                    int idx = n - sg * kk;
+                    double b = Iv[idx < 0 ? -idx : idx];
+                    val.x += dre[kk + M] * b;
+                    val.y += dim[kk + M] * b;
+                }
+        }
+        out[(long long)n * U.npp + loc] = val;
+    }
+}
+
+// ============================================================================
+// symmetry-unique shell quartets (ERI_toroidal.f90:342-401)
+// ============================================================================
+__device__ __forceinline__ bool tce_is_canonical(const DevSys &S, int q0, int q1, int q2, int q3)
+{
+    const int perm[8][4] = {{0,1,2,3},{1,0,2,3},{0,1,3,2},{1,0,3,2},{2,3,0,1},{3,2,0,1},{2,3,1,0},{3,2,1,0}};
+    int q[4] = {q0, q1, q2, q3};
+    for (int ip = 1; ip < 8; ++ip) {
+        int t[4];
+#pragma unroll
+        for (int ii = 0; ii < 4; ++ii) t[ii] = q[perm[ip][ii]];
+        int ref = t[0] / S.nshuc;
+        int r[4];
+#pragma unroll
+        for (int ii = 0; ii < 4; ++ii) r[ii] = tce_shift_to(t[ii], ref, S.nshuc, S.ncl);
+        for (int ii = 0; ii < 4; ++ii) {
+            if (r[ii] < q[ii]) return false;
+            if (r[ii] > q[ii]) break;
+        }
+    }
+    return true;
+}
+
+// one thread per (SI < nshuc, SJ, SK); loops over SL.  Appends survivors.
+__global__ void k_enumerate(DevSys S, const double *Qsh, double Qmax, int4 *items, unsigned long long *count,
+                            unsigned long long cap, unsigned long long *nfunc)
+{
+    long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long tot = (long long)S.nshuc * S.nsh * S.nsh;
+    if (id >= tot) return;
+    int SK = (int)(id % S.nsh);
+    long long r = id / S.nsh;
+    int SJ = (int)(r % S.nsh);
+    int SI = (int)(r / S.nsh);
+    if (SJ % S.nshuc < SI || SK % S.nshuc < SI) return;
+    double qij = Qsh[SI + (long long)S.nsh * SJ];
+    if (qij * Qmax < S.thr) return;
+    unsigned long long myf = 0;
+    for (int SL = 0; SL < S.nsh; ++SL) {
+        if (SL % S.nshuc < SI) continue;
+        if (qij * Qsh[SK + (long long)S.nsh * SL] < S.thr) continue;
+        if (!tce_is_canonical(S, SI, SJ, SK, SL)) continue;
+        unsigned long long slot = atomicAdd(count, 1ull);
+        if (slot < cap) items[slot] = make_int4(SI, SJ, SK, SL);
+        int fI = S.sh_first[SI], fJ = S.sh_first[SJ], fK = S.sh_first[SK], fL = S.sh_first[SL];
+        for (int a = 0; a < S.sh_n[SI]; ++a)
+            for (int b = 0; b < S.sh_n[SJ]; ++b) {
+                double qab = S.Q[(fI + a) + (long long)S.nbas * (fJ + b)];
+                for (int c = 0; c < S.sh_n[SK]; ++c)
+                    for (int e = 0; e < S.sh_n[SL]; ++e)
+                        if (qab * S.Q[(fK + c) + (long long)S.nbas * (fL + e)] >= S.thr) ++myf;
+            }
+    }
+    if (myf) atomicAdd(nfunc, myf);
+}
+
+// ============================================================================
+// the quartet kernel
+// ============================================================================
+struct QuartetArgs {
+    const int4 *items;       // shell quartets (SI in the unit cell)
+    const int *prim_sel;     // mode PRIMTAB: (p1, p2) per item, else null
+    int nitems;
+    int mode;                // TCE_MODE_*
+    int prim_screen;         // apply the primitive screen (main loops)
+    unsigned int *next;      // dynamic work counter
+    // outputs
+    double *blk_out;         // BLOCK: blocks at blk_off[item]
+    const long long *blk_off;
+    const double *P;         // JK: density (nbas x nbas)
+    double *J, *K;           // JK: nfuc x nbas
+    double *eri;             // STORE
+    int eri_size, physicist;
+    PairPrim *pp_rw;         // PRIMTAB: where ps values go
+    // smem layout (doubles per warp)
+    int bmax;                // primitive quartets per batch
+    int rowcap;              // rows per batch (>= bmax * ncomb * ndp)
+    int cstride;             // power combinations per real direction (largest class)
+    int warp_smem_doubles;
+};
+
+template <int NQ>
+__device__ __forceinline__ void row_dot(const DevSys &S, int d, const double2 *__restrict__ G, int nppb, int ib_,
+                                        const double2 *__restrict__ H, int nppk, int ik_, int nm, double phi,
+                                        double sgn, double *out)
+{
+    constexpr int NG = NQ / 8;
+    const double *__restrict__ T = S.Tt + (size_t)d * (S.ncap + 1) * NQ;
+    double c1, s1;
+    sincos(phi, &s1, &c1);
+#pragma unroll
+    for (int g0 = 0; g0 < NG; g0 += 4) {
+        constexpr int dummy = 0;
+        (void)dummy;
+        double acc[32];
+#pragma unroll
+        for (int x = 0; x < 32; ++x) acc[x] = 0.0;
+        double cn = 1.0, sn = 0.0;
+        int n = 0;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            if (g0 + s >= NG) break;
+            int nend = S.gmax[d][g0 + s];
+            nend = nend < nm ? nend : nm;
+            for (; n <= nend; ++n) {
+                if (n > 0) {
+                    if ((n & 31) == 0) {
+                        sincos((double)n * phi, &sn, &cn);
+                    } else {
+                        double tmp = cn * c1 - sn * s1;
+                        sn = sn * c1 + cn * s1;
+                        cn = tmp;
+                    }
+                }
+                double2 g = __ldg(G + (size_t)n * nppb + ib_);
+                double2 h = __ldg(H + (size_t)n * nppk + ik_);
+                double ar = g.x * h.x - g.y * h.y, ai = g.x * h.y + g.y * h.x;
+                double F = ar * cn - ai * sn;
+                const double2 *Tn = reinterpret_cast<const double2 *>(T + (size_t)n * NQ + 8 * g0);
+#pragma unroll
+                for (int g = 0; g < 4; ++g) {
+                    if (g >= s && g0 + g < NG) {
+#pragma unroll
+                        for (int kk = 0; kk < 4; ++kk) {
+                            double2 t = __ldg(Tn + 4 * g + kk);
+                            acc[8 * g + 2 * kk] = fma(F, t.x, acc[8 * g + 2 * kk]);
+                            acc[8 * g + 2 * kk + 1] = fma(F, t.y, acc[8 * g + 2 * kk + 1]);
+                        }
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int x = 0; x < 32; ++x)
+            if (8 * g0 + x < NQ) out[8 * g0 + x] = acc[x] * sgn;
+    }
+}
+
+// Context of one shell quartet, shared by the phases of the quartet kernel.
+struct QCtx {
+    int SI, SJ, SK, SL, nA, nB, nC, nD, lsA, lsB, lsC, lsD, ncomb, ncq, NN, R;
+    UnitPair Ub, Uk;
+    double Tsh[3];
+};
+
+// Phases 1+2 for a batch of nb primitive quartets (qlist/qfac), accumulating
+// into the shell-quartet block blk (warp-private shared memory).
+template <int NQ>
+__device__ void process_batch(const DevSys &S, const QCtx &Q, int nb, const int2 *qlist, const double *qfac,
+                              double *rows, double *realb, double *blk, int lane, int cstride)
+{
+    constexpr int RS = NQ + 1;
+    const int ndp = S.ndp, nreal = 3 - ndp;
+    const int lsA = Q.lsA, lsB = Q.lsB, lsC = Q.lsC, lsD = Q.lsD, ncomb = Q.ncomb, R = Q.R;
+    const int nppb = Q.Ub.npp, nppk = Q.Uk.npp;
+    // ---------------- phase 1: periodic-direction rows (lane = row) ----------------
+    const int nrows = nb * R;
+    for (int r = lane; r < nrows; r += 32) {
+        int p = r / R, rem = r - p * R;
+        int d = rem / ncomb, cmb = rem - d * ncomb;
+        int ia = cmb % (lsA + 1), t1 = cmb / (lsA + 1);
+        int ib = t1 % (lsB + 1), t2 = t1 / (lsB + 1);
+        int ic = t2 % (lsC + 1), id = t2 / (lsC + 1);
+        int2 pq = qlist[p];
+        const PairPrim &Pb = S.pp[Q.Ub.pp_off + pq.x];
+        const PairPrim &Pk = S.pp[Q.Uk.pp_off + pq.y];
+        const double2 *G = S.vec + Q.Ub.vec_off +
+                           ((((long long)d * (lsA + 1) + ia) * (lsB + 1) + ib) * 2 + 0) * (long long)Q.Ub.Nlen * nppb;
+        const double2 *H = S.vec + Q.Uk.vec_off +
+                           ((((long long)d * (lsC + 1) + ic) * (lsD + 1) + id) * 2 + 1) * (long long)Q.Uk.Nlen * nppk;
+        int nm = Pb.N[d] < Pk.N[d] ? Pb.N[d] : Pk.N[d];
+        double phi = S.a[d] * (Pb.cen[d] - (Pk.cen[d] + Q.Tsh[d]));
+        double sgn = pow(S.a[d], -(double)(ia + ib + ic + id));
+        row_dot<NQ>(S, d, G, nppb, pq.x, H, nppk, pq.y, nm, phi, sgn, rows + (size_t)r * RS);
+    }
+    __syncwarp();
+    // ---------------- phase 2: real directions + contraction (lane = node) ----------------
+    const int npA = S.sh_np[Q.SI], npB = S.sh_np[Q.SJ], npC = S.sh_np[Q.SK], npD = S.sh_np[Q.SL];
+    for (int p = 0; p < nb; ++p) {
+        int2 pq = qlist[p];
+        const PairPrim &Pb = S.pp[Q.Ub.pp_off + pq.x];
+        const PairPrim &Pk = S.pp[Q.Uk.pp_off + pq.y];
+        const double pp_ = Pb.esum, qq = Pk.esum;
+        if (nreal > 0) {
+            const double *Eb = S.ecoef + Q.Ub.e_off + (long long)pq.x * nreal * (lsA + 1) * (lsB + 1) * TCE_ECO;
+            const double *Ek = S.ecoef + Q.Uk.e_off + (long long)pq.y * nreal * (lsC + 1) * (lsD + 1) * TCE_ECO;
+            for (int k = lane; k < NQ; k += 32) {
+                double t = S.tnode[k], t2 = t * t;
+                double D2 = 1.0 / (pp_ * qq + (pp_ + qq) * t2);
+                double w = pp_ * qq * t2 * D2, rs = PI_D * sqrt(D2);
+                for (int dr = 0; dr < nreal; ++dr) {
+                    int d = ndp + dr;
+                    double Rr = Pb.cen[d] - (Pk.cen[d] + Q.Tsh[d]);
+                    double gt[4 * TCE_LMAX + 2];
+                    gt[0] = (Rr == 0.0) ? rs : rs * exp(-w * Rr * Rr);
+                    double gm1 = 0.0, g0 = gt[0];
+                    for (int n = 0; n < Q.NN; ++n) {
+                        double gp1 = 2.0 * w * Rr * g0 - 2.0 * (double)n * w * gm1;
+                        gt[n + 1] = gp1;
+                        gm1 = g0;
+                        g0 = gp1;
+                    }
+                    for (int cmb = 0; cmb < ncomb; ++cmb) {
+                        int ia = cmb % (lsA + 1), u1 = cmb / (lsA + 1);
+                        int ib = u1 % (lsB + 1), u2 = u1 / (lsB + 1);
+                        int ic = u2 % (lsC + 1), id = u2 / (lsC + 1);
+                        const double *eb = Eb + ((dr * (lsA + 1) + ia) * (lsB + 1) + ib) * TCE_ECO;
+                        const double *ek = Ek + ((dr * (lsC + 1) + ic) * (lsD + 1) + id) * TCE_ECO;
+                        double val = 0.0;
+                        for (int n = 0; n <= ia + ib; ++n) {
+                            double sb = (n & 1) ? -eb[n] : eb[n];
+                            for (int kk = 0; kk <= ic + id; ++kk) val += sb * ek[kk] * gt[n + kk];
+                        }
+                        realb[((size_t)dr * cstride + cmb) * RS + k] = val;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+        const double fac = qfac[p];
+        const double *rowp = rows + (size_t)p * R * RS;
+        const int i = pq.x / Q.Ub.np2, j = pq.x % Q.Ub.np2;
+        const int kp = pq.y / Q.Uk.np2, lp = pq.y % Q.Uk.np2;
+        for (int cq = 0; cq < Q.ncq; ++cq) {
+            int ca = cq % Q.nA, r1 = cq / Q.nA;
+            int cb = r1 % Q.nB, r2 = r1 / Q.nB;
+            int cc = r2 % Q.nC, cd = r2 / Q.nC;
+            const int *pa = S.fn_pw + 3 * (S.sh_first[Q.SI] + ca);
+            const int *pb = S.fn_pw + 3 * (S.sh_first[Q.SJ] + cb);
+            const int *pc = S.fn_pw + 3 * (S.sh_first[Q.SK] + cc);
+            const int *pd = S.fn_pw + 3 * (S.sh_first[Q.SL] + cd);
+            int cm[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) cm[d] = pa[d] + (lsA + 1) * (pb[d] + (lsB + 1) * (pc[d] + (lsC + 1) * pd[d]));
+            double v = 0.0;
+            for (int k = lane; k < NQ; k += 32) {
+                double prod = S.tweight[k];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    double x = (d < ndp) ? rowp[((size_t)d * ncomb + cm[d]) * RS + k]
+                                         : realb[((size_t)(d - ndp) * cstride + cm[d]) * RS + k];
+                    prod *= x;
+                }
+                v += prod;
+            }
+            v = tce_warp_sum(v);
+            if (lane == 0) {
+                double cf = S.sh_coef[S.sh_coff[Q.SI] + ca * npA + i] * S.sh_coef[S.sh_coff[Q.SJ] + cb * npB + j] *
+                            S.sh_coef[S.sh_coff[Q.SK] + cc * npC + kp] * S.sh_coef[S.sh_coff[Q.SL] + cd * npD + lp];
+                blk[cq] += fac * cf * v;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+template <int NQ>
+__global__ void __launch_bounds__(128) k_quartets(DevSys S, QuartetArgs A)
+{
+    extern __shared__ double smem[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    double *ws = smem + (size_t)wib * A.warp_smem_doubles;
+    constexpr int RS = NQ + 1;
+    const int ndp = S.ndp, nreal = 3 - ndp;
+    // per-warp smem: [qlist qcap][qfac qcap][rows rowcap*RS][real nreal*cstride*RS][blk 1296]
+    const int qcap = A.rowcap;
+    int2 *qlist = reinterpret_cast<int2 *>(ws);
+    double *qfac = ws + qcap;
+    double *rows = ws + 2 * qcap;
+    double *realb = rows + (size_t)A.rowcap * RS;
+    double *blk = realb + (size_t)nreal * A.cstride * RS;
+
+    while (true) {
+        int it = 0;
+        if (lane == 0) it = (int)atomicAdd(A.next, 1u);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= A.nitems) break;
+        const int4 q = A.items[it];
+        QCtx Q;
+        Q.SI = q.x; Q.SJ = q.y; Q.SK = q.z; Q.SL = q.w;
+        Q.nA = S.sh_n[Q.SI]; Q.nB = S.sh_n[Q.SJ]; Q.nC = S.sh_n[Q.SK]; Q.nD = S.sh_n[Q.SL];
+        Q.lsA = S.sh_l[Q.SI]; Q.lsB = S.sh_l[Q.SJ]; Q.lsC = S.sh_l[Q.SK]; Q.lsD = S.sh_l[Q.SL];
+        Q.ncomb = (Q.lsA + 1) * (Q.lsB + 1) * (Q.lsC + 1) * (Q.lsD + 1);
+        Q.ncq = Q.nA * Q.nB * Q.nC * Q.nD;
+        Q.NN = Q.lsA + Q.lsB + Q.lsC + Q.lsD;
+        Q.R = Q.ncomb * ndp;
+        // ket: translate (SK,SL) so that SK lies in the unit cell
+        const int cK = Q.SK / S.nshuc;
+        const int SK0 = Q.SK - cK * S.nshuc;
+        const int SLp = tce_shift_to(Q.SL, cK, S.nshuc, S.ncl);
+        Q.Ub = S.up[(long long)Q.SI * S.nsh + Q.SJ];
+        Q.Uk = S.up[(long long)SK0 * S.nsh + SLp];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) Q.Tsh[d] = S.sh_r[3 * Q.SK + d] - S.sh_r[3 * SK0 + d];
+        int B = A.rowcap / Q.R;
+        if (B < 1) B = 1;
+        if (B > qcap) B = qcap;
+
+        for (int c = lane; c < Q.ncq; c += 32) blk[c] = 0.0;
+        __syncwarp();
+
+        const int nppb = Q.Ub.npp, nppk = Q.Uk.npp;
+        const long long total = (long long)nppb * nppk;
+        int want = -1;
+        if (A.mode == TCE_MODE_PRIMTAB) want = A.prim_sel[2 * it] * Q.Ub.np2 + A.prim_sel[2 * it + 1];
+        int nb = 0;
+        for (long long base = 0; base < total; base += 32) {
+            long long idx = base + lane;
+            bool keep = idx < total;
+            int ipb = 0, ipk = 0;
+            double fac = 0.0;
+            if (keep) {
+                ipb = (int)(idx / nppk);
+                ipk = (int)(idx - (long long)ipb * nppk);
+                const PairPrim &Pb = S.pp[Q.Ub.pp_off + ipb];
+                const PairPrim &Pk = S.pp[Q.Uk.pp_off + ipk];
+                fac = S.fac_const * Pb.pfac * Pk.pfac;
+                if (A.mode == TCE_MODE_PRIMTAB) {
+                    keep = (ipb == want) && (ipk == want);
+                } else if (A.mode != TCE_MODE_NOSCREEN) {
+                    // prefactor screens (ERI_shell_block_toroidal.f90:191,216) and the
+                    // primitive Schwarz screen (:217-219)
+                    double bra = fabs(S.fac_const * Pb.pfac) * Pb.cmax12;
+                    if (bra * Q.Uk.ket_max <= 2.22e-16) keep = false;
+                    else if (fabs(fac) * Pb.cmax12 * Pk.cmax12 <= 2.22e-16) keep = false;
+                    else if (A.prim_screen && Pb.ps * Pk.ps < S.prim_thr) keep = false;
+                }
+            }
+            const unsigned msk = __ballot_sync(0xffffffffu, keep);
+            const int pos = __popc(msk & ((1u << lane) - 1u));
+            const int cnt = __popc(msk);
+            int done = 0;
+            while (done < cnt) {
+                int take = B - nb;
+                if (take > cnt - done) take = cnt - done;
+                if (keep && pos >= done && pos < done + take) {
+                    qlist[nb + pos - done] = make_int2(ipb, ipk);
+                    qfac[nb + pos - done] = fac;
+                }
+                nb += take;
+                done += take;
+                __syncwarp();
+                if (nb == B) {
+                    process_batch<NQ>(S, Q, nb, qlist, qfac, rows, realb, blk, lane, A.cstride);
+                    nb = 0;
+                    __syncwarp();
+                }
+            }
+        }
+        if (nb > 0) process_batch<NQ>(S, Q, nb, qlist, qfac, rows, realb, blk, lane, A.cstride);
+        __syncwarp();
+
+        // ---------------- phase 3: the consumer of the block ----------------
+        const int nA = Q.nA, nB = Q.nB, nC = Q.nC, nD = Q.nD;
+        if (A.mode == TCE_MODE_BLOCK || A.mode == TCE_MODE_NOSCREEN) {
+            double *o = A.blk_out + A.blk_off[it];
+            for (int c = lane; c < Q.ncq; c += 32) o[c] = blk[c];
+        } else if (A.mode == TCE_MODE_PRIMTAB) {
+            if (lane == 0) {
+                double m = 0.0;
+                for (int a = 0; a < nA; ++a)
+                    for (int b = 0; b < nB; ++b) {
+                        double v = sqrt(fabs(blk[a + nA * (b + nB * (a + nA * b))]));
+                        if (v > m) m = v;
+                    }
+                A.pp_rw[Q.Ub.pp_off + want].ps = m;
+            }
+        } else {
+            const int fI = S.sh_first[Q.SI], fJ = S.sh_first[Q.SJ], fK = S.sh_first[Q.SK], fL = S.sh_first[Q.SL];
+            const int perm[8][4] = {{0,1,2,3},{1,0,2,3},{0,1,3,2},{1,0,3,2},{2,3,0,1},{3,2,0,1},{2,3,1,0},{3,2,1,0}};
+            for (int cq = lane; cq < Q.ncq; cq += 32) {
+                int ca = cq % nA, r1 = cq / nA;
+                int cb = r1 % nB, r2 = r1 / nB;
+                int cc = r2 % nC, cd = r2 / nC;
+                int f[4] = {fI + ca, fJ + cb, fK + cc, fL + cd};
+                if (S.Q[f[0] + (long long)S.nbas * f[1]] * S.Q[f[2] + (long long)S.nbas * f[3]] < S.thr) continue;
+                const double val = blk[cq];
+                int img[8][4];
+                bool rep = true;
+                for (int ip = 0; ip < 8; ++ip) {
+                    int t[4];
+#pragma unroll
+                    for (int ii = 0; ii < 4; ++ii) t[ii] = f[perm[ip][ii]];
+                    int ref = t[0] / S.nfuc;
+#pragma unroll
+                    for (int ii = 0; ii < 4; ++ii) img[ip][ii] = tce_shift_to(t[ii], ref, S.nfuc, S.ncl);
+                    // an image inside this block that sorts before f: f is not the representative
+                    const int *g = img[ip];
+                    bool inblk = g[0] >= fI && g[0] < fI + nA && g[1] >= fJ && g[1] < fJ + nB && g[2] >= fK &&
+                                 g[2] < fK + nC && g[3] >= fL && g[3] < fL + nD;
+                    if (inblk) {
+                        for (int ii = 0; ii < 4; ++ii) {
+                            if (g[ii] < f[ii]) { rep = false; break; }
+                            if (g[ii] > f[ii]) break;
+                        }
+                    }
+                }
+                if (A.mode == TCE_MODE_STORE) {
+                    for (int ip = 0; ip < 8; ++ip) {
+                        const int *g = img[ip];
+                        long long e;
+                        if (A.physicist)
+                            e = g[0] + (long long)A.eri_size * (g[2] + (long long)S.nbas * (g[1] + (long long)S.nbas * g[3]));
+                        else
+                            e = g[0] + (long long)A.eri_size * (g[1] + (long long)S.nbas * (g[2] + (long long)S.nbas * g[3]));
+                        A.eri[e] = val;
+                    }
+                    continue;
+                }
+                if (!rep) continue;
+                for (int ip = 0; ip < 8; ++ip) {
+                    const int *g = img[ip];
+                    bool dup = false;
+                    for (int jp = 0; jp < ip && !dup; ++jp)
+                        dup = img[jp][0] == g[0] && img[jp][1] == g[1] && img[jp][2] == g[2] && img[jp][3] == g[3];
+                    if (dup) continue;
+                    atomicAdd(A.J + g[0] + (long long)S.nfuc * g[1], val * A.P[g[2] + (long long)S.nbas * g[3]]);
+                    atomicAdd(A.K + g[0] + (long long)S.nfuc * g[3], -0.5 * val * A.P[g[1] + (long long)S.nbas * g[2]]);
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// ============================================================================
+// stored J/K (hartree_exchange_potential.f90:157-200): one block per column d
+// ============================================================================
+__global__ void k_stored_jk(int n1, int nbas, int physicist, const double *__restrict__ P,
+                            const double *__restrict__ eri, double *J, double *K)
+{
+    extern __shared__ double kacc[];   // n1
+    int d = blockIdx.x;
+    for (int a = threadIdx.x; a < n1; a += blockDim.x) kacc[a] = 0.0;
+    __syncthreads();
+    long long slab = (long long)n1 * nbas;
+    for (long long i = threadIdx.x; i < slab; i += blockDim.x) {
+        int a = (int)(i % n1), b = (int)(i / n1);
+        double jl = 0.0, kl = 0.0;
+        for (int c = 0; c < nbas; ++c) {
+            double e = eri[i + slab * (c + (long long)nbas * d)];
+            if (!physicist) {
+                jl += e * P[c + (long long)nbas * d];
+                kl += e * P[b + (long long)nbas * c];
+            } else {
+                // physicist ERI(a,b,c,d) = (ac|bd): J(a,c) += E P(b,d), K(a,d) += -1/2 E P(c,b)
+                atomicAdd(J + a + (long long)n1 * c, e * P[b + (long long)nbas * d]);
+                kl += e * P[c + (long long)nbas * b];
+            }
+        }
+        if (!physicist) atomicAdd(J + a + (long long)n1 * b, jl);
+        atomicAdd(&kacc[a], kl);
+    }
+    __syncthreads();
+    for (int a = threadIdx.x; a < n1; a += blockDim.x) K[a + (long long)n1 * d] = -0.5 * kacc[a];
+}
+
+// rows i >= nfuc by translation (symmetric_matrix.f90:62-131), eri is nbas^4
+__global__ void k_sym_fill(int nf, int fpuc, int nx, int ny, int nz, double *eri)
+{
+    long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long tot = (long long)(nf - fpuc) * nf * nf * nf;
+    if (id >= tot) return;
+    int i = fpuc + (int)(id % (nf - fpuc));
+    long long r = id / (nf - fpuc);
+    int j = (int)(r % nf);
+    r /= nf;
+    int k = (int)(r % nf);
+    int l = (int)(r / nf);
+    auto cell = [&](int idx, int &cx, int &cy, int &cz) {
+        int ii = idx / fpuc;
+        cx = ii % nx;
+        ii /= nx;
+        cy = ii % ny;
+        cz = ii / ny;
+    };
+    int ix, iy, iz;
+    cell(i, ix, iy, iz);
+    auto eqv = [&](int jj) {
+        int cx, cy, cz;
+        cell(jj, cx, cy, cz);
+        int m = tce_mod(cx - ix, nx), n = tce_mod(cy - iy, ny), p = tce_mod(cz - iz, nz);
+        return (p * nx * ny + n * nx + m) * fpuc + jj % fpuc;
+    };
+    eri[i + (long long)nf * (j + (long long)nf * (k + (long long)nf * l))] =
+        eri[(i % fpuc) + (long long)nf * (eqv(j) + (long long)nf * (eqv(k) + (long long)nf * eqv(l)))];
+}
+
+// ============================================================================
+// launch wrappers (host)
+// ============================================================================
+int tce_launch_quartets(const DevSys &S, const QuartetHostArgs &h, cudaStream_t st)
+{
+    QuartetArgs A;
+    A.items = h.items;
+    A.prim_sel = h.prim_sel;
+    A.nitems = h.nitems;
+    A.mode = h.mode;
+    A.prim_screen = h.prim_screen;
+    A.next = h.next;
+    A.blk_out = h.blk_out;
+    A.blk_off = h.blk_off;
+    A.P = h.P;
+    A.J = h.J;
+    A.K = h.K;
+    A.eri = h.eri;
+    A.eri_size = h.eri_size;
+    A.physicist = h.physicist;
+    A.pp_rw = h.pp_rw;
+    // batch sizing from the largest class present (rows of 32 lanes at least)
+    int R = h.max_ncomb * S.ndp;
+    int rowcap = R > 32 ? R : 32;
+    int bmax = rowcap;
+    const int RS = S.nq + 1;
+    int nreal = 3 - S.ndp;
+    long long wdoubles = 2LL * rowcap + (long long)rowcap * RS + (long long)nreal * h.max_ncomb * RS + 1296 + 8;
+    wdoubles = (wdoubles + 31) / 32 * 32;
+    A.bmax = bmax;
+    A.rowcap = rowcap;
+    A.cstride = h.max_ncomb;
+    A.warp_smem_doubles = (int)wdoubles;
+    size_t wbytes = (size_t)wdoubles * sizeof(double);
+    int warps = 4;
+    while (warps > 1 && wbytes * warps > 220 * 1024) --warps;
+    if (wbytes > 220 * 1024) return TCE_ERR_UNSUPPORTED;
+    size_t smem = wbytes * warps;
+    cudaMemsetAsync(h.next, 0, sizeof(unsigned int), st);
+    int nsm = h.num_sms > 0 ? h.num_sms : 148;
+    cudaError_t e;
+    switch (S.nq) {
+    case 32:
+        cudaFuncSetAttribute(k_quartets<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        {
+            int per = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_quartets<32>, 32 * warps, smem);
+            if (per < 1) per = 1;
+            k_quartets<32><<<nsm * per, 32 * warps, smem, st>>>(S, A);
+        }
+        break;
+    case 40:
+        cudaFuncSetAttribute(k_quartets<40>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        {
+            int per = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_quartets<40>, 32 * warps, smem);
+            if (per < 1) per = 1;
+            k_quartets<40><<<nsm * per, 32 * warps, smem, st>>>(S, A);
+        }
+        break;
+    case 64:
+        cudaFuncSetAttribute(k_quartets<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        {
+            int per = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_quartets<64>, 32 * warps, smem);
+            if (per < 1) per = 1;
+            k_quartets<64><<<nsm * per, 32 * warps, smem, st>>>(S, A);
+        }
+        break;
+    case 128:
+        cudaFuncSetAttribute(k_quartets<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        {
+            int per = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_quartets<128>, 32 * warps, smem);
+            if (per < 1) per = 1;
+            k_quartets<128><<<nsm * per, 32 * warps, smem, st>>>(S, A);
+        }
+        break;
+    default:
+        return TCE_ERR_UNSUPPORTED;
+    }
+    e = cudaGetLastError();
+    return e == cudaSuccess ? TCE_OK : TCE_ERR_CUDA;
+}
+
+int tce_launch_t_tables(int nq, int ndp, int ncap, const double *tnode, const double *a, double *tb, int *tnmax,
+                        double *Tt, cudaStream_t st)
+{
+    int n = nq * ndp;
+    k_t_bessel<<<(n + 63) / 64, 64, 0, st>>>(nq, ndp, ncap, tnode, a[0], a[1], a[2], tb);
+    k_t_finish<<<(n + 63) / 64, 64, 0, st>>>(nq, ndp, ncap, tb, tnmax, Tt);
+    return cudaGetLastError() == cudaSuccess ? TCE_OK : TCE_ERR_CUDA;
+}
+
+int tce_launch_pair_scalars(const DevSys &S, long long npp_tot, const int *pp_unit, PairPrim *pp, UnitPair *up,
+                            double *ecoef, cudaStream_t st)
+{
+    int threads = 128;
+    long long blocks = (npp_tot + threads - 1) / threads;
+    if (npp_tot == 0) return TCE_OK;
+    k_pair_scalars<<<(unsigned)blocks, threads, 0, st>>>(S, npp_tot, pp_unit, pp, up, ecoef);
+    return cudaGetLastError() == cudaSuccess ? TCE_OK : TCE_ERR_CUDA;
+}
+
+int tce_launch_pair_vectors(const DevSys &S, long long npp_tot, const int *pp_unit, const PairPrim *pp, int stride,
+                            double *scratch, double2 *vec, cudaStream_t st)
+{
+    if (npp_tot == 0) return TCE_OK;
+    long long n1 = npp_tot * S.ndp;
+    k_pair_bessel<<<(unsigned)((n1 + 127) / 128), 128, 0, st>>>(S, npp_tot, pp_unit, pp, stride, scratch);
+    const int NV = (TCE_LMAX + 1) * (TCE_LMAX + 1) * 2;
+    long long n2 = npp_tot * S.ndp * NV;
+    k_pair_vectors<<<(unsigned)((n2 + 127) / 128), 128, 0, st>>>(S, npp_tot, pp_unit, pp, stride, scratch, vec);
+    return cudaGetLastError() == cudaSuccess ? TCE_OK : TCE_ERR_CUDA;
+}
+
+int tce_launch_enumerate(const DevSys &S, const double *Qsh, double Qmax, int4 *items, unsigned long long *count,
+                         unsigned long long cap, unsigned long long *nfunc, cudaStream_t st)
+{
+    long long tot = (long long)S.nshuc * S.nsh * S.nsh;
+    k_enumerate<<<(unsigned)((tot + 127) / 128), 128, 0, st>>>(S, Qsh, Qmax, items, count, cap, nfunc);
+    return cudaGetLastError() == cudaSuccess ? TCE_OK : TCE_ERR_CUDA;
+}
+
+int tce_launch_stored_jk(int n1, int nbas, int physicist, const double *P, const double *eri, double *J, double *K,
+                         cudaStream_t st)
+{
+    k_stored_jk<<<nbas, 256, sizeof(double) * n1, st>>>(n1, nbas, physicist, P, eri, J, K);
+    return cudaGetLastError() == cudaSuccess ? TCE_OK : TCE_ERR_CUDA;
+}
+
+int tce_launch_sym_fill(int nf, int fpuc, const int *ncl, double *eri, cudaStream_t st)
+{
+    long long tot = (long long)(nf - fpuc) * nf * nf * nf;
+    if (tot <= 0) return TCE_OK;
+    k_sym_fill<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(nf, fpuc, ncl[0], ncl[1], ncl[2], eri);
+    return cudaGetLastError() == cudaSuccess ? TCE_OK : TCE_ERR_CUDA;
+}

@@ -1,0 +1,43 @@
+// tce_kernels.h -- host-side launch interface of the engine's kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include "tce_device.cuh"
+#include "../../include/tce.h"
+
+// consumers of a shell-quartet block (k_quartets)
+#define TCE_MODE_BLOCK    0   // prefactor screens, block written out (Schwarz pass)
+#define TCE_MODE_NOSCREEN 1   // no screens, block written out (ps_noscreen)
+#define TCE_MODE_PRIMTAB  2   // single primitive pair, no screens -> PairPrim::ps
+#define TCE_MODE_JK       3   // fused J/K scatter (direct_JK)
+#define TCE_MODE_STORE    4   // stored-ERI scatter (ERI_integral_toroidal)
+
+struct QuartetHostArgs {
+    const int4 *items = nullptr;
+    const int *prim_sel = nullptr;
+    int nitems = 0;
+    int mode = TCE_MODE_BLOCK;
+    int prim_screen = 0;
+    unsigned int *next = nullptr;
+    double *blk_out = nullptr;
+    const long long *blk_off = nullptr;
+    const double *P = nullptr;
+    double *J = nullptr, *K = nullptr;
+    double *eri = nullptr;
+    int eri_size = 0, physicist = 0;
+    PairPrim *pp_rw = nullptr;
+    int max_ncomb = 1;   // largest (lA+1)(lB+1)(lC+1)(lD+1) among the items
+    int num_sms = 148;
+};
+
+int tce_launch_quartets(const DevSys &S, const QuartetHostArgs &h, cudaStream_t st);
+int tce_launch_t_tables(int nq, int ndp, int ncap, const double *tnode, const double *a, double *tb, int *tnmax,
+                        double *Tt, cudaStream_t st);
+int tce_launch_pair_scalars(const DevSys &S, long long npp_tot, const int *pp_unit, PairPrim *pp, UnitPair *up,
+                            double *ecoef, cudaStream_t st);
+int tce_launch_pair_vectors(const DevSys &S, long long npp_tot, const int *pp_unit, const PairPrim *pp, int stride,
+                            double *scratch, double2 *vec, cudaStream_t st);
+int tce_launch_enumerate(const DevSys &S, const double *Qsh, double Qmax, int4 *items, unsigned long long *count,
+                         unsigned long long cap, unsigned long long *nfunc, cudaStream_t st);
+int tce_launch_stored_jk(int n1, int nbas, int physicist, const double *P, const double *eri, double *J, double *K,
+                         cudaStream_t st);
+int tce_launch_sym_fill(int nf, int fpuc, const int *ncl, double *eri, cudaStream_t st);

@@ -1,0 +1,229 @@
+"""Python host mirror of the reference's integral/SCF-path interface, over the
+C ABI of libtce.so (include/tce.h).
+
+Names follow the Fortran routines they replace:
+
+    Engine(system)                  direct_init (eri_direct.f90:76) + ERI driver preamble
+    Engine.ERI_shell_block(...)     ERI_shell_block_toroidal (ERI_shell_block_toroidal.f90:28)
+    Engine.ERI_integral_toroidal()  ERI_integral_toroidal (ERI_toroidal.f90:36)
+    Engine.direct_JK(P)             direct_JK (eri_direct.f90:262)
+    Engine.stored_JK(P)             hartree_exchange_potential on the device-resident ERIs
+    hartree_exchange_potential(...) hartree_exchange_potential (hartree_exchange_potential.f90:30)
+
+Errors: the reference stops (`error stop`); here a nonzero status raises
+TCEError with the library's message.  There is no CPU fallback: without the
+library or a usable GPU every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Tuple
+
+import numpy as np
+
+from .system import AOSystem
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtce.so")
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+
+TCE_OK, TCE_ERR_ARG, TCE_ERR_UNSUPPORTED, TCE_ERR_CUDA, TCE_ERR_STATE, TCE_ERR_NOMEM = range(6)
+
+# every symbol include/tce.h declares
+EXPORTS = ["tce_create", "tce_destroy", "tce_last_error", "tce_get_info", "tce_shell_block", "tce_shells",
+           "tce_schwarz", "tce_eri_stored", "tce_stored_jk", "tce_hartree_exchange", "tce_direct_jk",
+           "tce_direct_jk_device", "tce_last_kernel_ms", "tce_version"]
+
+
+class TCEError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__("libtce error %d: %s" % (code, msg))
+        self.code = code
+
+
+class TceSystem(C.Structure):
+    _fields_ = [("ndp", C.c_int32), ("ncell", C.c_int32 * 3), ("nfuc", C.c_int32), ("nbas", C.c_int32),
+                ("nquad", C.c_int32), ("L", C.c_double * 3), ("ctr", _dp), ("lxyz", _ip),
+                ("prim_off", _ip), ("exps", _dp), ("coefs", _dp), ("t_nodes", _dp), ("t_weights", _dp),
+                ("physicist", C.c_int32), ("sao", C.c_int32), ("prim_screen", C.c_int32),
+                ("schwarz_thr", C.c_double), ("prim_thr", C.c_double)]
+
+
+class TceInfo(C.Structure):
+    _fields_ = [("nsh", C.c_int32), ("nshuc", C.c_int32), ("ncap", C.c_int32), ("nquad", C.c_int32),
+                ("n_shell_quartets", C.c_int64), ("n_func_quartets", C.c_int64),
+                ("n_unit_pairs", C.c_int64), ("device_bytes", C.c_int64)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libtce.so (built in-tree).  Raises if it is missing: no fallback."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise TCEError(TCE_ERR_CUDA, "libtce.so is not built (run william_ci_b200.build.build())")
+        L = C.CDLL(LIB_PATH)
+        L.tce_create.argtypes = [C.POINTER(TceSystem), C.POINTER(C.c_void_p)]
+        L.tce_destroy.argtypes = [C.c_void_p]
+        L.tce_last_error.restype = C.c_char_p
+        L.tce_last_error.argtypes = [C.c_void_p]
+        L.tce_get_info.argtypes = [C.c_void_p, C.POINTER(TceInfo)]
+        L.tce_shell_block.argtypes = [C.c_void_p, _ip, C.c_int32, _dp]
+        L.tce_shells.argtypes = [C.c_void_p, _ip, _ip]
+        L.tce_schwarz.argtypes = [C.c_void_p, _dp]
+        L.tce_eri_stored.argtypes = [C.c_void_p, C.c_int64, _dp]
+        L.tce_stored_jk.argtypes = [C.c_void_p, _dp, _dp, _dp]
+        L.tce_hartree_exchange.argtypes = [C.c_int32, C.c_int32, C.c_int32, _dp, _dp, _dp, _dp]
+        L.tce_direct_jk.argtypes = [C.c_void_p, _dp, _dp, _dp]
+        L.tce_direct_jk_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.tce_last_kernel_ms.argtypes = [C.c_void_p, _dp]
+        L.tce_version.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def _check(code: int, h=None):
+    if code != TCE_OK:
+        msg = lib().tce_last_error(h)
+        raise TCEError(code, msg.decode() if msg else "")
+
+
+def _d(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+def _i(a: np.ndarray):
+    return a.ctypes.data_as(_ip)
+
+
+class Engine:
+    """Device engine for one supercell basis (normalised coefficients)."""
+
+    def __init__(self, system: AOSystem, nquad: int = 32, t_nodes=None, t_weights=None, physicist=False,
+                 sao=True, prim_screen=True, schwarz_thr=1e-13, prim_thr=1e-14):
+        self.sys = system
+        self.physicist = bool(physicist)
+        self.sao = bool(sao)
+        self._keep = [np.ascontiguousarray(system.ctr, dtype=np.float64).ravel(),
+                      np.ascontiguousarray(system.lxyz, dtype=np.int32).ravel(),
+                      np.ascontiguousarray(system.prim_off, dtype=np.int32),
+                      np.ascontiguousarray(system.exps, dtype=np.float64),
+                      np.ascontiguousarray(system.coefs, dtype=np.float64)]
+        s = TceSystem()
+        s.ndp = system.ndp
+        for d in range(3):
+            s.ncell[d] = system.ncell[d]
+            s.L[d] = system.L[d]
+        s.nfuc = system.nfuc
+        s.nbas = system.nbas
+        s.nquad = nquad
+        s.ctr, s.lxyz, s.prim_off, s.exps, s.coefs = (_d(self._keep[0]), _i(self._keep[1]), _i(self._keep[2]),
+                                                      _d(self._keep[3]), _d(self._keep[4]))
+        if t_nodes is not None:
+            tn = np.ascontiguousarray(t_nodes, dtype=np.float64)
+            tw = np.ascontiguousarray(t_weights, dtype=np.float64)
+            self._keep += [tn, tw]
+            s.nquad = len(tn)
+            s.t_nodes, s.t_weights = _d(tn), _d(tw)
+        s.physicist, s.sao, s.prim_screen = int(physicist), int(sao), int(prim_screen)
+        s.schwarz_thr, s.prim_thr = schwarz_thr, prim_thr
+        self._s = s
+        h = C.c_void_p()
+        code = lib().tce_create(C.byref(s), C.byref(h))
+        if code != TCE_OK:
+            msg = lib().tce_last_error(None)
+            raise TCEError(code, msg.decode() if msg else "")
+        self.h = h
+        self.nbas = system.nbas
+        self.nfuc = system.nfuc
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().tce_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---------------- introspection ----------------
+    def info(self) -> dict:
+        inf = TceInfo()
+        _check(lib().tce_get_info(self.h, C.byref(inf)), self.h)
+        return {f: getattr(inf, f) for f, _ in TceInfo._fields_}
+
+    def shells(self):
+        n = self.info()["nsh"]
+        first = np.zeros(n, dtype=np.int32)
+        cnt = np.zeros(n, dtype=np.int32)
+        _check(lib().tce_shells(self.h, _i(first), _i(cnt)), self.h)
+        return list(zip(first.tolist(), cnt.tolist()))
+
+    def schwarz(self) -> np.ndarray:
+        Q = np.zeros(self.nbas * self.nbas)
+        _check(lib().tce_schwarz(self.h, _d(Q)), self.h)
+        return Q.reshape(self.nbas, self.nbas, order="F")
+
+    # ---------------- the path ----------------
+    def ERI_shell_block(self, S1, S2, S3, S4, mode=1) -> np.ndarray:
+        sh = self.shells()
+        n = [sh[S][1] for S in (S1, S2, S3, S4)]
+        blk = np.zeros(int(np.prod(n)))
+        q = np.array([S1, S2, S3, S4], dtype=np.int32)
+        _check(lib().tce_shell_block(self.h, _i(q), int(mode), _d(blk)), self.h)
+        return blk.reshape(n, order="F")
+
+    def ERI_integral_toroidal(self) -> np.ndarray:
+        n = self.nbas
+        esz = self.nfuc if self.sao else n
+        eri = np.zeros(esz * n * n * n)
+        _check(lib().tce_eri_stored(self.h, esz, _d(eri)), self.h)
+        return eri.reshape((esz, n, n, n), order="F")
+
+    def direct_JK(self, P: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
+        n = self.nbas
+        Pf = np.asfortranarray(P, dtype=np.float64).ravel(order="F").copy()
+        J = np.zeros(n * n)
+        K = np.zeros(n * n)
+        _check(lib().tce_direct_jk(self.h, _d(Pf), _d(J), _d(K)), self.h)
+        return J.reshape(n, n, order="F"), K.reshape(n, n, order="F")
+
+    def direct_JK_device(self, dP_ptr: int, dJ_ptr: int, dK_ptr: int, stream_ptr: int = 0):
+        _check(lib().tce_direct_jk_device(self.h, C.c_void_p(dP_ptr), C.c_void_p(dJ_ptr), C.c_void_p(dK_ptr),
+                                          C.c_void_p(stream_ptr)), self.h)
+
+    def last_kernel_ms(self) -> float:
+        v = C.c_double()
+        _check(lib().tce_last_kernel_ms(self.h, C.byref(v)), self.h)
+        return v.value
+
+    def stored_JK(self, P: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
+        n = self.nbas
+        Pf = np.asfortranarray(P, dtype=np.float64).ravel(order="F").copy()
+        J = np.zeros(n * n)
+        K = np.zeros(n * n)
+        _check(lib().tce_stored_jk(self.h, _d(Pf), _d(J), _d(K)), self.h)
+        return J.reshape(n, n, order="F"), K.reshape(n, n, order="F")
+
+
+def hartree_exchange_potential(n1: int, P: np.ndarray, ERI: np.ndarray, physicist: bool = False):
+    n = P.shape[0]
+    Pf = np.asfortranarray(P, dtype=np.float64).ravel(order="F").copy()
+    E = np.asfortranarray(ERI, dtype=np.float64).ravel(order="F").copy()
+    J = np.zeros(n * n)
+    K = np.zeros(n * n)
+    _check(lib().tce_hartree_exchange(int(n1), int(n), int(physicist), _d(Pf), _d(E), _d(J), _d(K)))
+    return J.reshape(n, n, order="F"), K.reshape(n, n, order="F")
