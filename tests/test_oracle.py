@@ -1,0 +1,309 @@
+"""Pins of the CPU oracle (CPU only).
+
+The reference cannot be built here (no Fortran compiler) and ships no test
+vectors, so the oracle is pinned by
+  * independent implementations of its mathematics (scipy's Bessel functions,
+    Gauss-Legendre exactness, a Boys-function GTO ERI for the L -> infinity
+    limit, a brute-force real-space quadrature of the periodic direction);
+  * the reference's own data (its 64/128-node t tables, read from its source
+    into tests/golden/quad_tables.json by tests/golden/make_quad_tables.py);
+  * the reference's runtime self-checks restated as properties: <phi|phi> = 1
+    (normalize_1D.f90:62-63), 8-fold ERI symmetry (debug.f90:39-52),
+    direct J/K == stored J/K (eri_direct.f90:16-20), fast vs full quadrature
+    <= 1e-10 (fast_quad_self_check.f90:50,189).
+"""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+import pyoracle as po
+from conftest import make_system, random_density
+from william_ci_b200 import system as S
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+# ---------------------------------------------------------------------------
+# special functions
+# ---------------------------------------------------------------------------
+def test_iv_scaled_matches_scipy():
+    from scipy.special import ive
+    worst = 0.0
+    for v in [0, 1, 2, 3, 5, 8, 13, 16, 20, 40, 60, 120, 170, 300]:
+        for x in [1e-6, 1e-3, 0.1, 0.7, 1.0, 3.0, 12.0, 19.0, 25.0, 31.0, 40.0, 70.0, 100.0, 280.0,
+                  900.0, 1500.0, 2e4, 1e6]:
+            b = ive(v, x)
+            if b < 1e-290:
+                continue
+            a = po.iv_scaled(v, x)
+            worst = max(worst, abs(a - b) / b)
+    assert worst < 5e-13, worst
+
+
+def test_debye_polynomials_closed_forms():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("gen", os.path.join(os.path.dirname(po.__file__), "gen_debye.py"))
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    u = gen.debye(4)
+    from fractions import Fraction as F
+    assert u[1] == [0, F(3, 24), 0, F(-5, 24)]
+    assert u[2][2:] == [F(81, 1152), 0, F(-462, 1152), 0, F(385, 1152)]
+    assert u[3][3] == F(30375, 414720) and u[3][9] == F(-425425, 414720)
+    # u_4 (A&S 9.3.9): (4465125 t^4 - ... + 185910725 t^12) / 39813120
+    assert u[4][4] == F(4465125, 39813120) and u[4][12] == F(185910725, 39813120)
+
+
+def test_bessel_vectors_agree():
+    from scipy.special import ive
+    for A in [1e-3, 0.5, 3.0, 40.0, 800.0, 2.6e4]:
+        N = po.nmax_estimate(A)
+        ref = ive(np.arange(N + 1), A)
+        for fast in (False, True):
+            v = po.bessel_vector(N, A, fast=fast)
+            err = np.max(np.abs(v - ref)) / ref[0]
+            assert err < 1e-13, (A, fast, err)
+
+
+def test_pair_vector_sum_rule():
+    # V_n of an s pair is I~_n(A); for p pairs the n = 0 term is the mean of
+    # sin(u+phA) times the Bessel weight, so V(x) = sum_n V_n e^{inx} must
+    # reproduce sin(x+phA) e^{A(cos x - 1)} on a grid.
+    A, phA = 7.5, 0.37
+    N = po.nmax_estimate(A)
+    for sgn in (-1, 1):
+        V = po.pair_vector(N, A, 1, 0, phA, 0.0, sgn)
+        x = np.linspace(0, 2 * np.pi, 50, endpoint=False)
+        n = np.arange(1, N + 1)
+        # full series with V_{-n}: for a real function f(x) = sum_n c_n e^{i n x}, c_{-n} = conj(c_n)
+        # bra convention (sgn=-1): V_n = c_{-n}; ket (sgn=+1): V_n = c_n
+        c_pos = V[1:] if sgn == 1 else np.conj(V[1:])
+        f = V[0].real + 2 * np.real(np.exp(1j * np.outer(x, n)) @ c_pos)
+        ref = np.sin(x + phA) * np.exp(A * (np.cos(x) - 1.0))
+        assert np.max(np.abs(f - ref)) < 1e-13
+
+
+# ---------------------------------------------------------------------------
+# quadrature
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("n", [32, 40])
+def test_fast_quad_is_gauss_legendre(n):
+    t, w = po.fast_quad(n)
+    u = t / (0.6 + t)                # invert t = 0.6 u/(1-u)
+    wu = w * (1 - u) ** 2 / 0.6
+    for k in range(2 * n):
+        assert abs(np.sum(wu * u ** k) - 1.0 / (k + 1)) < 1e-14 * (k + 1)
+    assert np.all(np.diff(t) > 0)
+
+
+def test_reference_tables_fixture():
+    tab = json.load(open(os.path.join(GOLDEN, "quad_tables.json")))
+    for n in (64, 128):
+        t = np.array(tab[str(n)]["t_val"])
+        w = np.array(tab[str(n)]["w_val"])
+        assert len(t) == n and len(w) == n and np.all(np.diff(t) > 0)
+        x, wx = np.polynomial.legendre.leggauss(n)
+        u = 0.5 * (x + 1)
+        t2, w2 = u / (1 - u), 0.5 * wx / (1 - u) ** 2
+        rel = np.max(np.abs(t2 - t) / t)
+        if n == 128:   # the 128 table is the mapped rule t = u/(1-u)
+            assert rel < 1e-12
+        else:          # the 64 table deviates from it at the 1e-5 level (documented)
+            assert 1e-6 < rel < 1e-3
+
+
+# ---------------------------------------------------------------------------
+# system building + normalisation
+# ---------------------------------------------------------------------------
+def test_parsers_round_trip():
+    for name in ("h2_ring", "h_chain64", "h2_sheet", "li_cube"):
+        cell, basis = S.workload(name)
+        c2 = S.parse_unitcell(S.format_unitcell(cell))
+        b2 = S.parse_basis(S.format_basis(basis))
+        s1, s2 = S.build_system(cell, basis), S.build_system(c2, b2)
+        assert s1.nbas == s2.nbas and s1.nfuc == s2.nfuc and s1.labels == s2.labels
+        np.testing.assert_allclose(s1.ctr, s2.ctr, atol=1e-14)
+        np.testing.assert_array_equal(s1.prim_off, s2.prim_off)
+        np.testing.assert_allclose(s1.coefs, s2.coefs, rtol=1e-15)
+
+
+def test_workload_sizes():
+    expect = {"h2_ring": (2, 1), "h_chain64": (384, 6), "h2_sheet": (1408, 22), "li_cube": (576, 9),
+              "h_chain128": (768, 6)}
+    for name, (nbas, nfuc) in expect.items():
+        s = S.build_system(*S.workload(name))
+        assert (s.nbas, s.nfuc) == (nbas, nfuc), name
+
+
+@pytest.mark.parametrize("name", ["h2_ring", "h_chain64", "h2_sheet", "li_cube"])
+def test_normalisation(name):
+    s = S.build_system(*S.workload(name))
+    s.ncell  # noqa
+    one = S.build_system(*S.workload(name))
+    dev = po.normalize(one)
+    assert dev < 1e-12
+
+
+# ---------------------------------------------------------------------------
+# the reference's self-checks as properties
+# ---------------------------------------------------------------------------
+def test_eri_8fold_symmetry_and_translation():
+    s = make_system("h_chain64", (4, 1, 1))
+    o = po.Oracle(s, sao=False)
+    E, _ = o.eri_stored()
+    n = s.nbas
+    assert np.max(np.abs(E - E.transpose(1, 0, 2, 3))) < 1e-12
+    assert np.max(np.abs(E - E.transpose(0, 1, 3, 2))) < 1e-12
+    assert np.max(np.abs(E - E.transpose(2, 3, 0, 1))) < 1e-12
+    # translation by one cell
+    nf = s.nfuc
+    sh = np.roll(np.arange(n), nf)
+    Et = E[np.ix_(sh, sh, sh, sh)]
+    assert np.max(np.abs(E - Et)) < 1e-12
+
+
+@pytest.mark.parametrize("name,ncell", [("h2_ring", None), ("h_chain64", (6, 1, 1)), ("h2_sheet", (2, 1, 1)),
+                                        ("li_cube", (2, 1, 1))])
+def test_direct_equals_stored(name, ncell):
+    s = make_system(name, ncell)
+    o = po.Oracle(s)
+    E, _ = o.eri_stored()
+    P = random_density(s.nbas, seed=2)
+    J1, K1 = po.hartree_exchange(s.nfuc, P, E)
+    J2, K2, _ = o.direct_jk(P)
+    assert np.max(np.abs(J1 - J2)) < 1e-12
+    assert np.max(np.abs(K1 - K2)) < 1e-12
+
+
+@pytest.mark.parametrize("name,ncell", [("h2_ring", None), ("h_chain64", (8, 1, 1)), ("h2_sheet", (2, 2, 1)),
+                                        ("li_cube", (2, 2, 2))])
+def test_fast_vs_full_quadrature(name, ncell):
+    """fast_quad_self_check: the mapped 32/40-node rule against the 128-node table."""
+    tab = json.load(open(os.path.join(GOLDEN, "quad_tables.json")))
+    s = make_system(name, ncell)
+    o_full = po.Oracle(s, t_nodes=tab["128"]["t_val"], t_weights=tab["128"]["w_val"])
+    sh, nshuc, _ = o_full.shells()
+    rng = np.random.default_rng(5)
+    qs = [(0, 0, 0, 0)] + [tuple([int(rng.integers(0, nshuc))] + [int(x) for x in rng.integers(0, len(sh), 3)])
+                           for _ in range(10)]
+    for nq, tol in ((40, 1e-10), (32, 1e-9)):
+        o = po.Oracle(s, nquad=nq)
+        dev = max(np.max(np.abs(o.shell_block(*q, mode=0) - o_full.shell_block(*q, mode=0))) for q in qs)
+        assert dev < tol, (nq, dev)
+
+
+# ---------------------------------------------------------------------------
+# independent mathematics
+# ---------------------------------------------------------------------------
+def _boys0(T):
+    from scipy.special import erf
+    return 1.0 if T < 1e-14 else 0.5 * math.sqrt(math.pi / T) * erf(math.sqrt(T))
+
+
+def _gto_eri_s(exps_coefs, centres):
+    (ea, ca), (eb, cb), (ec, cc), (ed, cd) = exps_coefs
+    A, B, C, D = (np.asarray(x) for x in centres)
+    tot = 0.0
+    for a, xa in zip(ea, ca):
+        for b, xb in zip(eb, cb):
+            p = a + b
+            P = (a * A + b * B) / p
+            kab = math.exp(-a * b / p * np.dot(A - B, A - B))
+            for c, xc in zip(ec, cc):
+                for d, xd in zip(ed, cd):
+                    q = c + d
+                    Q = (c * C + d * D) / q
+                    kcd = math.exp(-c * d / q * np.dot(C - D, C - D))
+                    T = p * q / (p + q) * np.dot(P - Q, P - Q)
+                    tot += xa * xb * xc * xd * 2 * math.pi ** 2.5 / (p * q * math.sqrt(p + q)) * kab * kcd * _boys0(T)
+    return tot
+
+
+def test_gto_limit():
+    """L -> infinity: Clifford ERIs tend to Cartesian GTO ERIs, error ~ 1/L^2."""
+    errs = []
+    for L in (300.0, 1200.0):
+        cell = S.Cell("Tori1D", (1, 1, 1), L, (L, 0.0, 0.0), [("H", (0.0, 0.0, 0.0)), ("H", (1.4, 0.3, 0.0))])
+        s = S.build_system(cell, {1: [S.STO3G_H]})
+        po.normalize(s)
+        o = po.Oracle(s, nquad=40, prim_screen=False)
+        e, c = [], []
+        for f in range(2):
+            o0, o1 = s.prim_off[f], s.prim_off[f + 1]
+            e.append(s.exps[o0:o1])
+            c.append(s.coefs[o0:o1])
+        # the same contraction normalised with the real-GTO metric (the coefficients
+        # already carry the primitive normalisation)
+        cg = []
+        for f in range(2):
+            x = c[f]
+            nrm = sum(xi * xj * (math.pi / (ai + aj)) ** 1.5 for xi, ai in zip(x, e[f]) for xj, aj in zip(x, e[f]))
+            cg.append(x / math.sqrt(nrm))
+        worst = 0.0
+        for q in [(0, 0, 0, 0), (0, 1, 0, 1), (0, 0, 1, 1), (0, 1, 1, 1), (0, 0, 0, 1)]:
+            v = o.shell_block(*q, mode=2).item()
+            ref = _gto_eri_s([(e[i], cg[i]) for i in q], [s.ctr[i] for i in q])
+            worst = max(worst, abs(v - ref))
+        errs.append(worst)
+    assert errs[1] < 2e-5, errs
+    assert 8.0 < errs[0] / errs[1] < 32.0, errs      # second-order convergence in 1/L
+
+
+def test_bruteforce_periodic_direction():
+    """(ss|ss) on the 2-cell ring (antipodal centres) by real-space quadrature.
+
+    1/r12 = 2/sqrt(pi) int_0^inf exp(-t^2 r12^2) dt with the chord distance
+    |x|_E^2 = 2(1 - cos a x)/a^2 in the periodic direction.  The x integrals
+    are done on a grid (periodic trapezoid + Gauss-Legendre in x2 - x1 around
+    the kernel peak), y and z analytically, t by adaptive quadrature.  This
+    uses no Bessel function, pair vector or t-table of the oracle.
+    """
+    from scipy.integrate import quad
+    s = make_system("h2_ring")
+    o = po.Oracle(s, nquad=40, prim_screen=False)
+    L = s.L[0]
+    a = 2 * math.pi / L
+    M = 256
+    x1 = np.arange(M) * (L / M)
+    gx, gw = np.polynomial.legendre.leggauss(96)
+
+    def gfun(f, x):
+        o0, o1 = s.prim_off[f], s.prim_off[f + 1]
+        ex = s.exps[o0:o1][:, None]
+        return ex, s.coefs[o0:o1][:, None], np.exp(-2 * ex / a ** 2 * (1 - np.cos(a * (x[None, :] - s.ctr[f][0]))))
+
+    def eri(fa, fb, fc, fd):
+        ea, ca, ga = gfun(fa, x1)
+        eb, cb, gb = gfun(fb, x1)
+
+        def X_and_yz(t):
+            h = min(L / 2, 9.0 / max(t, 1e-12))
+            dx = h * gx
+            x2 = (x1[:, None] + dx[None, :]).ravel()
+            ec, cc, gc = gfun(fc, x2)
+            ed, cd, gd = gfun(fd, x2)
+            K = np.exp(-t * t * 2 * (1 - np.cos(a * dx)) / a ** 2)
+            tot = 0.0
+            for i in range(ea.shape[0]):
+                for j in range(eb.shape[0]):
+                    rho1 = ca[i, 0] * cb[j, 0] * ga[i] * gb[j]             # (M,)
+                    p = ea[i, 0] + eb[j, 0]
+                    for k in range(ec.shape[0]):
+                        for l in range(ed.shape[0]):
+                            rho2 = (cc[k, 0] * cd[l, 0] * gc[k] * gd[l]).reshape(M, -1)
+                            q = ec[k, 0] + ed[l, 0]
+                            X = (L / M) * h * np.sum(rho1[:, None] * rho2 * (K * gw)[None, :])
+                            yz = (math.pi / math.sqrt(p * q + (p + q) * t * t)) ** 2
+                            tot += X * yz
+            return tot
+
+        val, err = quad(X_and_yz, 0, np.inf, epsabs=1e-13, epsrel=1e-12, limit=400)
+        return 2 / math.sqrt(math.pi) * val
+
+    for q in [(0, 0, 0, 0), (0, 1, 0, 1), (0, 0, 1, 1)]:
+        ref = eri(*q)
+        v = o.shell_block(*q, mode=2).item()
+        assert abs(v - ref) < 1e-9, (q, v, ref)
