@@ -1,0 +1,307 @@
+#!/usr/bin/env python
+"""Benchmark: toroidal ERI quartets/s of one integral-direct J/K build.
+
+Workload (BASELINE config "Tori1D RHF H chain", the quoted one): 64 cells,
+spacing 1.8 bohr, torus length 115.2 bohr, per H 3 contracted s (4 primitives,
+exponents log-uniform in [0.1,20], seeded) + 1 p (0.727); 384 functions;
+synthetic inputs (seeded), normalised as the Fortran caller would.
+
+A step is one direct_JK pass (eri_direct.f90:262): every symmetry-unique shell
+quartet evaluated and contracted with the density into J and K.  Unit of the
+metric: function quartets (ij|kl) of the translation- and 8-fold-unique set
+after the Schwarz screen, counted the same way for the CPU baseline.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Under torchrun (N > 1) each rank evaluates a cost-balanced shard of the
+quartets and the partial J/K are summed with one NCCL all-reduce per step.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "toroidal ERI quartets/s at ≤1e-10 err, learned-grid vs plain; RHF SCF iter time"
+WORKLOAD = "h_chain64"
+SYSTEM_FIXTURE = os.path.join(ROOT, "tests", "golden", "systems", WORKLOAD + ".npz")
+PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "k_quartets_h_chain64_traffic.json")
+L2_FLUSH_BYTES = 512 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def density(n, seed=2026):
+    rng = np.random.default_rng(seed)
+    P = rng.standard_normal((n, n)) * 0.1
+    return np.asfortranarray(P + P.T)
+
+
+def config(sysm, extra=None):
+    c = {"workload": "Tori1D H chain, 64 cells, d=1.8, L=115.2 bohr, 3s(4 prim)+1p per H, nbas=%d, one direct J/K pass"
+                     % sysm.nbas,
+         "nbas": sysm.nbas, "nfuc": sysm.nfuc, "quadrature": "32-node mapped Gauss-Legendre (fast_quad)",
+         "l2": "flushed between timed steps (512 MiB write)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle port (C restatement of the reference, OpenMP)
+# ---------------------------------------------------------------------------
+def cpu_baseline(sysm, stride, reps=1):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    o = pyoracle.Oracle(sysm)
+    items = o.items()
+    sample = items[::stride]
+    P = density(sysm.nbas)
+    best = None
+    nf = 0
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        _, _, nf = o.direct_jk_items(sample, P)
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": nf / best, "unit": "quartets/s", "cores": cores, "kind": "port",
+            "sample": "direct_JK over every %d-th of the %d unique shell quartets (%d function quartets, %.2f s); "
+                      "C restatement of the reference (no Fortran compiler here or on the GPU box)"
+                      % (stride, len(items), nf, best)}
+
+
+def reference_arm(args, sysm):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    o = pyoracle.Oracle(sysm)
+    items = o.items()
+    stride = 8
+    sample = items[::stride]
+    P = density(sysm.nbas)
+    for _ in range(args.warmup):
+        o.direct_jk_items(sample[:max(1, len(sample) // 8)], P)
+    tot, nf_tot = 0.0, 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        _, _, nf = o.direct_jk_items(sample, P)
+        tot += time.perf_counter() - t0
+        nf_tot += nf
+    v = nf_tot / tot
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    line = {"metric": METRIC, "value": v, "unit": "quartets/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "impl": "reference",
+            "config": config(sysm, {"sample": "every %d-th unique shell quartet per step" % stride}),
+            "cpu_baseline": {"value": v, "unit": "quartets/s", "cores": cores, "kind": "port",
+                             "sample": "direct_JK over every %d-th of %d unique shell quartets per step; C restatement "
+                                       "of the reference's OpenMP path (the Fortran reference cannot be compiled: no "
+                                       "Fortran compiler)" % (stride, len(items))},
+            "e2e": {"value": v, "unit": "quartets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip() == "Active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                pass
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    from william_ci_b200.system import AOSystem
+    sysm = AOSystem.load(SYSTEM_FIXTURE)
+    if args.impl == "reference":
+        reference_arm(args, sysm)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from william_ci_b200.engine import Engine, fp64_peak_tflops
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    eng = Engine(sysm)
+    if world > 1:
+        eng.set_shard(rank, world)
+    info = eng.info()
+    n, nf = sysm.nbas, sysm.nfuc
+    Ph = density(n)
+    dP = torch.from_numpy(Ph.ravel(order="F").copy()).to(dev)
+    dJ = torch.zeros(nf * n, dtype=torch.float64, device=dev)
+    dK = torch.zeros(nf * n, dtype=torch.float64, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        eng.direct_JK_device(dP.data_ptr(), dJ.data_ptr(), dK.data_ptr(), stream.cuda_stream)
+        if world > 1:
+            dist.all_reduce(dJ)
+            dist.all_reduce(dK)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    kern_ms = []
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for i in range(args.steps):
+        flush.fill_(float(i))                     # evict L2 between timed steps (not timed)
+        ev[i][0].record(stream)
+        step()
+        ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        kern_ms.append(eng.last_kernel_ms())
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    tot_ms = sum(a.elapsed_time(b) for a, b in ev)
+    t = torch.tensor([tot_ms, float(np.mean(kern_ms))], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    tot_ms, kmax = float(t[0]), float(t[1])
+    ms_step = tot_ms / args.steps
+    nq_total = info["n_func_quartets"]
+    value = nq_total / (ms_step * 1e-3)
+
+    # ---- end to end through the public API: pinned host P in, J/K out, every step
+    Pp = torch.from_numpy(Ph.ravel(order="F").copy()).pin_memory()
+    Jp = torch.zeros(n * n, dtype=torch.float64).pin_memory()
+    Kp = torch.zeros(n * n, dtype=torch.float64).pin_memory()
+    e2e_steps = max(3, args.steps // 2)
+    if world == 1:
+        eng.direct_JK_ptrs(Pp.data_ptr(), Jp.data_ptr(), Kp.data_ptr())     # warm
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            eng.direct_JK_ptrs(Pp.data_ptr(), Jp.data_ptr(), Kp.data_ptr())
+        e2e_s = (time.perf_counter() - t0) / e2e_steps
+    else:
+        dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            dP.copy_(Pp, non_blocking=True)
+            step()
+            Jp[: nf * n].copy_(dJ, non_blocking=True)
+            Kp[: nf * n].copy_(dK, non_blocking=True)
+            torch.cuda.synchronize()
+        e2e_s = (time.perf_counter() - t0) / e2e_steps
+        te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e_s = float(te[0])
+    e2e = {"value": nq_total / e2e_s, "unit": "quartets/s", "h2d_bytes_per_step": 8 * n * n,
+           "d2h_bytes_per_step": 2 * 8 * nf * n, "ms_per_step": 1e3 * e2e_s,
+           "api": "tce_direct_jk (host buffers, pinned)" if world == 1 else
+                  "tce_direct_jk_device + NCCL all-reduce + pinned copies"}
+
+    if rank != 0:
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    peak = fp64_peak_tflops()
+    achieved = info["jk_flops"] / (kmax * 1e-3) / 1e12 if world == 1 else None
+    traffic = None
+    if os.path.exists(PROFILE_TRAFFIC):
+        try:
+            traffic = json.load(open(PROFILE_TRAFFIC)).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+    roofline = {"bound": "fp64", "kernel": "k_quartets<32> (fused quartet evaluation + J/K scatter)",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": (achieved / peak) if (achieved and peak) else None, "traffic": traffic,
+                "peak_source": "measured FP64 FMA throughput of this GPU (tce_fp64_peak probe); MEASURED_PEAKS.json "
+                               "holds no FP64 figure",
+                "algorithmic_flops_per_launch": info["jk_flops"], "kernel_ms": kmax}
+    line = {"metric": METRIC, "value": value, "unit": "quartets/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded exponents/coefficients)",
+            "config": config(sysm, {"parallelism": "quartet shards x%d + NCCL all-reduce of J/K" % world
+                                    if world > 1 else "single GPU",
+                                    "shell_quartets": info["n_shell_quartets"],
+                                    "function_quartets": nq_total, "primitive_quartets": info["n_prim_quartets"]}),
+            "e2e": e2e, "roofline": roofline, "clocks": clk, "gpu_launches": args.steps}
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(sysm, stride=1)
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

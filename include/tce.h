@@ -69,6 +69,13 @@ typedef struct {
     int64_t n_func_quartets;      /* function quartets after the Q screen   */
     int64_t n_unit_pairs;         /* significant unit-cell shell pairs       */
     int64_t device_bytes;         /* device memory held by the handle        */
+    int64_t n_prim_quartets;      /* primitive quartets evaluated per J/K pass
+                                     (after the prefactor and primitive screens) */
+    double  jk_flops;             /* algorithmic FP64 operations of one J/K pass,
+                                     counted from the reference's operation counts
+                                     (see the work-count kernel)               */
+    int32_t shard_rank, shard_nranks;  /* current shard (0, 1 when unsharded) */
+    int64_t shard_shell_quartets; /* shell quartets this shard evaluates       */
 } tce_info;
 
 /* Build the engine for one supercell basis: t-tables, shells, Schwarz
@@ -122,6 +129,23 @@ int tce_direct_jk_device(void *handle, const double *dP, double *dJ, double *dK,
 /* Elapsed device time (ms) of the last tce_direct_jk[_device] call's quartet
  * kernel, measured with CUDA events on the launching stream. */
 int tce_last_kernel_ms(void *handle, double *ms);
+
+/* Multi-GPU: restrict tce_direct_jk[_device] on this handle to shard `rank`
+ * of `nranks` (cost-balanced partition of the unique shell quartets, the same
+ * partition on every rank).  The partial J/K of the ranks sum to the full J/K;
+ * the caller reduces them (one all-reduce of 2 nfuc nbas doubles per SCF
+ * iteration).  The OpenMP task unit of the reference is the bra shell pair
+ * (eri_direct.f90:298-317); here it is the shell quartet. */
+int tce_set_shard(void *handle, int32_t rank, int32_t nranks);
+
+/* Host-only planner used by tce_set_shard: greedy longest-first assignment
+ * of n work items with the given costs to nranks owners (owner[i] in
+ * [0,nranks)).  Items are taken in the order given. */
+int tce_shard_plan(const double *cost, int64_t n, int32_t nranks, int32_t *owner);
+
+/* Measured FP64 FMA throughput of the current device (TFLOP/s), from a
+ * probe kernel of independent FMA chains on every SM. */
+int tce_fp64_peak(double *tflops);
 
 /* Library build identification (sm_100a, version). */
 const char *tce_version(void);

@@ -73,6 +73,10 @@ def lib():
         L.orc_hartree_exchange.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp]
         L.orc_sym_fill_eri.argtypes = [C.c_int, C.c_int, _ip, _dp]
         L.orc_count.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        L.orc_items.restype = C.c_int64
+        L.orc_items.argtypes = [C.c_void_p, _ip, C.c_int64]
+        L.orc_direct_jk_items.restype = C.c_int64
+        L.orc_direct_jk_items.argtypes = [C.c_void_p, _ip, C.c_int64, _dp, _dp, _dp]
         L.orc_overlap_pair.restype = C.c_double
         L.orc_overlap_pair.argtypes = [C.c_int, _dp, _ip, _ip, _dp, _dp, C.c_int, _dp, _dp, C.c_int, _dp, _dp]
         L.orc_normalize.restype = C.c_double
@@ -250,6 +254,22 @@ class Oracle:
         K = np.zeros(n * n)
         nq = lib().orc_direct_jk(self.h, dptr(Pf), dptr(J), dptr(K))
         return J.reshape(n, n, order="F"), K.reshape(n, n, order="F"), nq
+
+    def items(self) -> np.ndarray:
+        n = lib().orc_items(self.h, None, 0)
+        out = np.zeros((max(n, 1), 4), dtype=np.int32)
+        lib().orc_items(self.h, iptr(out), n)
+        return out[:n]
+
+    def direct_jk_items(self, items, P, J=None, K=None):
+        """Accumulate the J/K contributions of the given quartets; returns (J, K, nfunc)."""
+        n = self.sys.nbas
+        it = np.ascontiguousarray(items, dtype=np.int32)
+        Pf = np.asfortranarray(P, dtype=np.float64).ravel(order="F").copy()
+        Jf = np.zeros(n * n) if J is None else np.asfortranarray(J).ravel(order="F").copy()
+        Kf = np.zeros(n * n) if K is None else np.asfortranarray(K).ravel(order="F").copy()
+        nf = lib().orc_direct_jk_items(self.h, iptr(it), len(it), dptr(Pf), dptr(Jf), dptr(Kf))
+        return Jf.reshape(n, n, order="F"), Kf.reshape(n, n, order="F"), nf
 
     def count(self):
         a, b, c = C.c_int64(), C.c_int64(), C.c_int64()

@@ -1327,3 +1327,92 @@ void orc_count(orc_ctx *c, int64_t *n_shell_q, int64_t *n_func_q, int64_t *n_pri
         }
     *n_shell_q = ns; *n_func_q = nf; *n_prim_q = npq;
 }
+
+/* ---- the unique shell quartets of the direct/stored drivers (ERI_toroidal.f90:342-401),
+ *      in driver order; returns the count (items written while < cap) ---- */
+int64_t orc_items(orc_ctx *c, int32_t *out4, int64_t cap)
+{
+    const double thr = c->s.schwarz_thr;
+    int nsh = c->nsh, nshuc = c->nshuc;
+    int64_t n = 0;
+    if (!c->sym_ok) return -1;
+    for (int SI = 0; SI < nshuc; ++SI)
+        for (int SJ = 0; SJ < nsh; ++SJ) {
+            if (SJ % nshuc < SI) continue;
+            if (c->Qsh[SI + (size_t)nsh * SJ] * c->Qmax < thr) continue;
+            for (int SK = 0; SK < nsh; ++SK) {
+                if (SK % nshuc < SI) continue;
+                for (int SL = 0; SL < nsh; ++SL) {
+                    if (SL % nshuc < SI) continue;
+                    if (c->Qsh[SI + (size_t)nsh * SJ] * c->Qsh[SK + (size_t)nsh * SL] < thr) continue;
+                    int q4[4] = {SI, SJ, SK, SL};
+                    if (!is_canonical(c, q4)) continue;
+                    if (n < cap) { out4[4 * n] = SI; out4[4 * n + 1] = SJ; out4[4 * n + 2] = SK; out4[4 * n + 3] = SL; }
+                    ++n;
+                }
+            }
+        }
+    return n;
+}
+
+/* ---- direct_JK restricted to an explicit list of unique shell quartets
+ *      (same contraction and once-per-element rule as orc_direct_jk);
+ *      J/K are accumulated (not zeroed); returns the function quartets done ---- */
+int64_t orc_direct_jk_items(orc_ctx *c, const int32_t *items4, int64_t nitems, const double *P, double *J, double *K)
+{
+    const double thr = c->s.schwarz_thr;
+    int nbas = c->nbas, nfuc = c->nfuc, nsh = c->nsh;
+    int mx = 0;
+    for (int S = 0; S < nsh; ++S) if (c->sh_n[S] > mx) mx = c->sh_n[S];
+    int hs = 1;
+    while (hs < 4 * 8 * mx * mx * mx * mx) hs *= 2;
+    int64_t nf = 0;
+    #pragma omp parallel reduction(+ : nf)
+    {
+        double *Jl = calloc((size_t)nfuc * nbas, sizeof(double)), *Kl = calloc((size_t)nfuc * nbas, sizeof(double));
+        int64_t *hkey = malloc(sizeof(int64_t) * hs);
+        int *used = malloc(sizeof(int) * 8 * mx * mx * mx * mx);
+        for (int h = 0; h < hs; ++h) hkey[h] = -1;
+        #pragma omp for schedule(dynamic, 1)
+        for (int64_t it = 0; it < nitems; ++it) {
+            int SI = items4[4 * it], SJ = items4[4 * it + 1], SK = items4[4 * it + 2], SL = items4[4 * it + 3];
+            int n1 = c->sh_n[SI], n2 = c->sh_n[SJ], n3 = c->sh_n[SK], n4 = c->sh_n[SL];
+            double *blk = malloc(sizeof(double) * n1 * n2 * n3 * n4);
+            orc_shell_block(c, SI, SJ, SK, SL, c->ps_qp ? 1 : 0, blk);
+            int ns = 0;
+            for (int d = 0; d < n4; ++d)
+                for (int cc = 0; cc < n3; ++cc)
+                    for (int b = 0; b < n2; ++b)
+                        for (int a = 0; a < n1; ++a) {
+                            int f[4] = {c->sh_first[SI] + a, c->sh_first[SJ] + b, c->sh_first[SK] + cc, c->sh_first[SL] + d};
+                            if (c->Q[f[0] + (size_t)nbas * f[1]] * c->Q[f[2] + (size_t)nbas * f[3]] < thr) continue;
+                            ++nf;
+                            double val = blk[a + n1 * (b + n2 * (cc + n3 * d))];
+                            for (int ip = 0; ip < 8; ++ip) {
+                                int pp[4];
+                                for (int ii = 0; ii < 4; ++ii) pp[ii] = f[iperm8[ip][ii]];
+                                translate_to_unit_cell(pp, nfuc, c->ncl);
+                                int64_t key = (int64_t)pp[0] + (int64_t)nfuc * ((int64_t)pp[1] + (int64_t)nbas * ((int64_t)pp[2] + (int64_t)nbas * pp[3]));
+                                int h = (int)((key + (key >> 11) + (key >> 23) + (key >> 37)) & (hs - 1));
+                                while (hkey[h] != -1 && hkey[h] != key) h = (h + 1) & (hs - 1);
+                                if (hkey[h] == key) continue;
+                                hkey[h] = key; used[ns++] = h;
+                                Jl[pp[0] + (size_t)nfuc * pp[1]] += val * P[pp[2] + (size_t)nbas * pp[3]];
+                                Kl[pp[0] + (size_t)nfuc * pp[3]] -= 0.5 * val * P[pp[1] + (size_t)nbas * pp[2]];
+                            }
+                        }
+            for (int x = 0; x < ns; ++x) hkey[used[x]] = -1;
+            free(blk);
+        }
+        #pragma omp critical
+        {
+            for (int b = 0; b < nbas; ++b)
+                for (int a = 0; a < nfuc; ++a) {
+                    J[a + (size_t)nbas * b] += Jl[a + (size_t)nfuc * b];
+                    K[a + (size_t)nbas * b] += Kl[a + (size_t)nfuc * b];
+                }
+        }
+        free(Jl); free(Kl); free(hkey); free(used);
+    }
+    return nf;
+}

@@ -94,6 +94,12 @@ void orc_hartree_exchange(int n1, int nbas, int physicist, const double *P,
 /* Rows i > nfuc by translation, in place (non-SAO). */
 void orc_sym_fill_eri(int nbas, int nfuc, const int32_t ncell[3], double *eri);
 
+/* Unique shell quartets in driver order (out4: 4 ints per quartet). */
+int64_t orc_items(orc_ctx *c, int32_t *out4, int64_t cap);
+/* direct_JK over an explicit quartet list; J/K accumulated; returns the
+ * function quartets evaluated. */
+int64_t orc_direct_jk_items(orc_ctx *c, const int32_t *items4, int64_t nitems, const double *P, double *J, double *K);
+
 /* Counting helpers for the bench: unique shell quartets, function quartets
  * (after the function-level Schwarz screen) and primitive quartets evaluated. */
 void orc_count(orc_ctx *c, int64_t *n_shell_q, int64_t *n_func_q, int64_t *n_prim_q);

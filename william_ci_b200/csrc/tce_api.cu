@@ -49,7 +49,14 @@ struct Handle {
     int4 *d_items = nullptr;
     long long nitems = 0;
     int max_ncomb = 1;
-    long long n_func_q = 0, n_unit_sig = 0;
+    long long n_func_q = 0, n_unit_sig = 0, n_prim_q = 0;
+    double jk_flops = 0.0;
+    std::vector<int4> items_host;       // sorted, most expensive first
+    std::vector<double> cost_host;
+    int shard_rank = 0, shard_nranks = 1;
+    int4 *d_items_shard = nullptr;
+    long long nitems_shard = 0;
+    int *d_tnmax = nullptr;
     unsigned int *d_next = nullptr;
     double *d_P = nullptr, *d_J = nullptr, *d_K = nullptr;
     double *d_eri = nullptr;
@@ -392,7 +399,7 @@ int build(Handle *h, const tce_system *sys)
         CK(h, cudaMemcpyAsync(h->tnmax.data(), tn, h->tnmax.size() * sizeof(int), cudaMemcpyDeviceToHost, h->st));
         CK(h, cudaStreamSynchronize(h->st));
         dfree(h, tb);
-        dfree(h, tn);
+        h->d_tnmax = tn;
         S.Tt = Tt;
         for (int d = 0; d < 3; ++d)
             for (int g = 0; g < TCE_MAXG; ++g) S.gmax[d][g] = -1;
@@ -552,8 +559,30 @@ int build(Handle *h, const tce_system *sys)
         std::iota(ord.begin(), ord.end(), 0);
         std::stable_sort(ord.begin(), ord.end(), [&](size_t x, size_t y) { return cost[x] > cost[y]; });
         std::vector<int4> sorted(items.size());
-        for (size_t i = 0; i < ord.size(); ++i) sorted[i] = items[ord[i]];
+        h->cost_host.resize(items.size());
+        for (size_t i = 0; i < ord.size(); ++i) {
+            sorted[i] = items[ord[i]];
+            h->cost_host[i] = cost[ord[i]];
+        }
         if ((s = upload(h, &h->d_items, sorted))) return s;
+        h->items_host = std::move(sorted);
+        h->d_items_shard = h->d_items;
+        h->nitems_shard = h->nitems;
+        // algorithmic work of one J/K pass
+        unsigned long long *d_np = nullptr;
+        double *d_fl = nullptr;
+        if ((s = dalloc(h, &d_np, 1))) return s;
+        if ((s = dalloc(h, &d_fl, 1))) return s;
+        CK(h, cudaMemsetAsync(d_np, 0, sizeof(unsigned long long), h->st));
+        CK(h, cudaMemsetAsync(d_fl, 0, sizeof(double), h->st));
+        CKS(h, tce_launch_count_work(S, h->d_items, (int)h->nitems, h->prim_screen, h->d_tnmax, d_np, d_fl, h->st));
+        unsigned long long np_ = 0;
+        CK(h, cudaMemcpyAsync(&np_, d_np, sizeof np_, cudaMemcpyDeviceToHost, h->st));
+        CK(h, cudaMemcpyAsync(&h->jk_flops, d_fl, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+        CK(h, cudaStreamSynchronize(h->st));
+        h->n_prim_q = (long long)np_;
+        dfree(h, d_np);
+        dfree(h, d_fl);
     }
     if ((s = dalloc(h, &h->d_P, (size_t)nbas * nbas))) return s;
     if ((s = dalloc(h, &h->d_J, (size_t)h->nfuc * nbas))) return s;
@@ -573,10 +602,10 @@ int direct_jk_device(Handle *h, const double *dP, double *dJ, double *dK, cudaSt
 {
     CK(h, cudaMemsetAsync(dJ, 0, sizeof(double) * h->nfuc * h->nbas, st));
     CK(h, cudaMemsetAsync(dK, 0, sizeof(double) * h->nfuc * h->nbas, st));
-    if (h->nitems == 0) return TCE_OK;
+    if (h->nitems_shard == 0) return TCE_OK;
     QuartetHostArgs a;
-    a.items = h->d_items;
-    a.nitems = (int)h->nitems;
+    a.items = h->d_items_shard;
+    a.nitems = (int)h->nitems_shard;
     a.mode = TCE_MODE_JK;
     a.prim_screen = h->prim_screen;
     a.next = h->d_next;
@@ -650,6 +679,86 @@ int tce_get_info(void *handle, tce_info *info)
     info->n_func_quartets = h->n_func_q;
     info->n_unit_pairs = h->n_unit_sig;
     info->device_bytes = (int64_t)h->bytes;
+    info->n_prim_quartets = h->n_prim_q;
+    info->jk_flops = h->jk_flops;
+    info->shard_rank = h->shard_rank;
+    info->shard_nranks = h->shard_nranks;
+    info->shard_shell_quartets = h->nitems_shard;
+    return TCE_OK;
+}
+
+int tce_shard_plan(const double *cost, int64_t n, int32_t nranks, int32_t *owner)
+{
+    if (nranks < 1 || n < 0 || (n > 0 && (!cost || !owner))) return fail(nullptr, TCE_ERR_ARG, "bad argument");
+    std::vector<double> load(nranks, 0.0);
+    for (int64_t i = 0; i < n; ++i) {
+        int best = 0;
+        for (int r = 1; r < nranks; ++r)
+            if (load[r] < load[best]) best = r;
+        owner[i] = best;
+        load[best] += cost[i] > 0 ? cost[i] : 0.0;
+    }
+    return TCE_OK;
+}
+
+int tce_set_shard(void *handle, int32_t rank, int32_t nranks)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || nranks < 1 || rank < 0 || rank >= nranks) return fail(h, TCE_ERR_ARG, "bad shard");
+    if (h->d_items_shard && h->d_items_shard != h->d_items) dfree(h, h->d_items_shard);
+    h->shard_rank = rank;
+    h->shard_nranks = nranks;
+    if (nranks == 1) {
+        h->d_items_shard = h->d_items;
+        h->nitems_shard = h->nitems;
+        return TCE_OK;
+    }
+    std::vector<int32_t> owner(h->items_host.size());
+    int s = tce_shard_plan(h->cost_host.data(), (int64_t)owner.size(), nranks, owner.data());
+    if (s) return fail(h, s, "shard plan failed");
+    std::vector<int4> mine;
+    for (size_t i = 0; i < owner.size(); ++i)
+        if (owner[i] == rank) mine.push_back(h->items_host[i]);
+    h->nitems_shard = (long long)mine.size();
+    h->d_items_shard = nullptr;
+    if ((s = upload(h, &h->d_items_shard, mine))) return s;
+    CK(h, cudaStreamSynchronize(h->st));
+    return TCE_OK;
+}
+
+int tce_fp64_peak(double *tflops)
+{
+    if (!tflops) return fail(nullptr, TCE_ERR_ARG, "NULL argument");
+    Handle tmp;
+    Handle *h = &tmp;
+    int dev = 0, nsm = 148;
+    CK(h, cudaGetDevice(&dev));
+    CK(h, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    cudaStream_t st;
+    CK(h, cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    double *sink = nullptr;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    if (cudaMalloc(&sink, sizeof(double)) != cudaSuccess) return fail(nullptr, TCE_ERR_NOMEM, "probe alloc");
+    long long fl = 0;
+    double best = 0.0;
+    for (int rep = 0; rep < 6; ++rep) {
+        cudaEventRecord(e0, st);
+        tce_launch_fp64_probe(nsm, 20000, sink, st, &fl);
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0 && ms > 0) best = std::max(best, fl / (ms * 1e-3) / 1e12);
+    }
+    cudaError_t e = cudaStreamSynchronize(st);
+    cudaFree(sink);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(st);
+    if (e != cudaSuccess) return fail(nullptr, TCE_ERR_CUDA, cudaGetErrorString(e));
+    *tflops = best;
     return TCE_OK;
 }
 

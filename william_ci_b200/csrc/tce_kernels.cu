@@ -634,6 +634,113 @@ __global__ void __launch_bounds__(128) k_quartets(DevSys S, QuartetArgs A)
 }
 
 // ============================================================================
+// algorithmic work of one J/K pass, counted from the reference algorithm's
+// operation counts per executed primitive quartet (ERI_shell_block_toroidal.f90):
+//   periodic d : 6(nm+1) phase recurrence + ncomb*8(nm+1) F_n build
+//                + ncomb * sum_k 2(min(nm, t_nmax(k))+1) node dots
+//   real d     : nq(8 + 2 NN) Hermite nodes + sum_cmb [3 (ia+ib+1)(ic+id+1) + 2 nq (NN_c+1)]
+//   + ncomb*nq weight fold + nA nB nC nD (3 nq + 5) component contraction
+// one warp per shell quartet, lanes over primitive quartets; same screens as k_quartets.
+// ============================================================================
+__global__ void k_count_work(DevSys S, const int4 *items, int nitems, int prim_screen, const int *tnmax,
+                             unsigned long long *nprim, double *flops)
+{
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    unsigned long long myp = 0;
+    double myf = 0.0;
+    for (int it = warp; it < nitems; it += nw) {
+        int4 q = items[it];
+        int lsA = S.sh_l[q.x], lsB = S.sh_l[q.y], lsC = S.sh_l[q.z], lsD = S.sh_l[q.w];
+        int ncomb = (lsA + 1) * (lsB + 1) * (lsC + 1) * (lsD + 1);
+        int NN = lsA + lsB + lsC + lsD;
+        int ncq = S.sh_n[q.x] * S.sh_n[q.y] * S.sh_n[q.z] * S.sh_n[q.w];
+        int cK = q.z / S.nshuc, SK0 = q.z - cK * S.nshuc, SLp = tce_shift_to(q.w, cK, S.nshuc, S.ncl);
+        const UnitPair Ub = S.up[(long long)q.x * S.nsh + q.y];
+        const UnitPair Uk = S.up[(long long)SK0 * S.nsh + SLp];
+        // quartet-independent part of the real-direction count
+        double realc = 0.0;
+        for (int cmb = 0; cmb < ncomb; ++cmb) {
+            int ia = cmb % (lsA + 1), t1 = cmb / (lsA + 1);
+            int ib = t1 % (lsB + 1), t2 = t1 / (lsB + 1);
+            int ic = t2 % (lsC + 1), id = t2 / (lsC + 1);
+            realc += 3.0 * (ia + ib + 1) * (ic + id + 1) + 2.0 * S.nq * (ia + ib + ic + id + 1);
+        }
+        long long total = (long long)Ub.npp * Uk.npp;
+        for (long long idx = lane; idx < total; idx += 32) {
+            int ipb = (int)(idx / Uk.npp), ipk = (int)(idx % Uk.npp);
+            const PairPrim &Pb = S.pp[Ub.pp_off + ipb];
+            const PairPrim &Pk = S.pp[Uk.pp_off + ipk];
+            double fac = S.fac_const * Pb.pfac * Pk.pfac;
+            double bra = fabs(S.fac_const * Pb.pfac) * Pb.cmax12;
+            if (bra * Uk.ket_max <= 2.22e-16) continue;
+            if (fabs(fac) * Pb.cmax12 * Pk.cmax12 <= 2.22e-16) continue;
+            if (prim_screen && Pb.ps * Pk.ps < S.prim_thr) continue;
+            ++myp;
+            double f = 0.0;
+            for (int d = 0; d < S.ndp; ++d) {
+                int nm = Pb.N[d] < Pk.N[d] ? Pb.N[d] : Pk.N[d];
+                double dots = 0.0;
+                for (int k = 0; k < S.nq; ++k) {
+                    int tn = tnmax[d * S.nq + k];
+                    dots += 2.0 * ((nm < tn ? nm : tn) + 1);
+                }
+                f += 6.0 * (nm + 1) + ncomb * 8.0 * (nm + 1) + ncomb * dots;
+            }
+            for (int d = S.ndp; d < 3; ++d) f += S.nq * (8.0 + 2.0 * NN) + realc;
+            f += (double)ncomb * S.nq + (double)ncq * (3.0 * S.nq + 5.0);
+            myf += f;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        myp += __shfl_xor_sync(0xffffffffu, myp, o);
+        myf += __shfl_xor_sync(0xffffffffu, myf, o);
+    }
+    if (lane == 0) {
+        atomicAdd(nprim, myp);
+        atomicAdd(flops, myf);
+    }
+}
+
+int tce_launch_count_work(const DevSys &S, const int4 *items, int nitems, int prim_screen, const int *tnmax,
+                          unsigned long long *nprim, double *flops, cudaStream_t st)
+{
+    if (nitems == 0) return TCE_OK;
+    k_count_work<<<148 * 8, 128, 0, st>>>(S, items, nitems, prim_screen, tnmax, nprim, flops);
+    return cudaGetLastError() == cudaSuccess ? TCE_OK : TCE_ERR_CUDA;
+}
+
+// ============================================================================
+// FP64 FMA throughput probe (roofline denominator for the FP64-bound kernels):
+// 8 independent FMA chains per thread, grid = 8 blocks of 256 threads per SM.
+// ============================================================================
+__global__ void k_fp64_probe(int iters, double seed, double *sink)
+{
+    double a[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) a[c] = seed + 1e-3 * (threadIdx.x + c);
+    const double m = 0.999999999, b = 1e-9;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) a[c] = fma(a[c], m, b);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) s += a[c];
+    if (s == 12345.678) sink[0] = s;   // keeps the chains live
+}
+
+int tce_launch_fp64_probe(int nsm, int iters, double *sink, cudaStream_t st, long long *flops)
+{
+    int blocks = nsm * 8, threads = 256;
+    k_fp64_probe<<<blocks, threads, 0, st>>>(iters, 1.0, sink);
+    *flops = 2LL * 8 * iters * (long long)blocks * threads;
+    return cudaGetLastError() == cudaSuccess ? TCE_OK : TCE_ERR_CUDA;
+}
+
+// ============================================================================
 // stored J/K (hartree_exchange_potential.f90:157-200): one block per column d
 // ============================================================================
 __global__ void k_stored_jk(int n1, int nbas, int physicist, const double *__restrict__ P,

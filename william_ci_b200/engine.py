@@ -35,7 +35,8 @@ TCE_OK, TCE_ERR_ARG, TCE_ERR_UNSUPPORTED, TCE_ERR_CUDA, TCE_ERR_STATE, TCE_ERR_N
 # every symbol include/tce.h declares
 EXPORTS = ["tce_create", "tce_destroy", "tce_last_error", "tce_get_info", "tce_shell_block", "tce_shells",
            "tce_schwarz", "tce_eri_stored", "tce_stored_jk", "tce_hartree_exchange", "tce_direct_jk",
-           "tce_direct_jk_device", "tce_last_kernel_ms", "tce_version"]
+           "tce_direct_jk_device", "tce_last_kernel_ms", "tce_set_shard", "tce_shard_plan", "tce_fp64_peak",
+           "tce_version"]
 
 
 class TCEError(RuntimeError):
@@ -55,7 +56,9 @@ class TceSystem(C.Structure):
 class TceInfo(C.Structure):
     _fields_ = [("nsh", C.c_int32), ("nshuc", C.c_int32), ("ncap", C.c_int32), ("nquad", C.c_int32),
                 ("n_shell_quartets", C.c_int64), ("n_func_quartets", C.c_int64),
-                ("n_unit_pairs", C.c_int64), ("device_bytes", C.c_int64)]
+                ("n_unit_pairs", C.c_int64), ("device_bytes", C.c_int64), ("n_prim_quartets", C.c_int64),
+                ("jk_flops", C.c_double), ("shard_rank", C.c_int32), ("shard_nranks", C.c_int32),
+                ("shard_shell_quartets", C.c_int64)]
 
 
 _lib = None
@@ -82,6 +85,9 @@ def lib():
         L.tce_direct_jk.argtypes = [C.c_void_p, _dp, _dp, _dp]
         L.tce_direct_jk_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.tce_last_kernel_ms.argtypes = [C.c_void_p, _dp]
+        L.tce_set_shard.argtypes = [C.c_void_p, C.c_int32, C.c_int32]
+        L.tce_shard_plan.argtypes = [_dp, C.c_int64, C.c_int32, _ip]
+        L.tce_fp64_peak.argtypes = [_dp]
         L.tce_version.restype = C.c_char_p
         _lib = L
     return _lib
@@ -201,6 +207,10 @@ class Engine:
         _check(lib().tce_direct_jk(self.h, _d(Pf), _d(J), _d(K)), self.h)
         return J.reshape(n, n, order="F"), K.reshape(n, n, order="F")
 
+    def direct_JK_ptrs(self, P_ptr: int, J_ptr: int, K_ptr: int):
+        """tce_direct_jk on caller-owned host buffers (e.g. pinned), nbas x nbas column-major."""
+        _check(lib().tce_direct_jk(self.h, C.cast(P_ptr, _dp), C.cast(J_ptr, _dp), C.cast(K_ptr, _dp)), self.h)
+
     def direct_JK_device(self, dP_ptr: int, dJ_ptr: int, dK_ptr: int, stream_ptr: int = 0):
         _check(lib().tce_direct_jk_device(self.h, C.c_void_p(dP_ptr), C.c_void_p(dJ_ptr), C.c_void_p(dK_ptr),
                                           C.c_void_p(stream_ptr)), self.h)
@@ -209,6 +219,9 @@ class Engine:
         v = C.c_double()
         _check(lib().tce_last_kernel_ms(self.h, C.byref(v)), self.h)
         return v.value
+
+    def set_shard(self, rank: int, nranks: int):
+        _check(lib().tce_set_shard(self.h, int(rank), int(nranks)), self.h)
 
     def stored_JK(self, P: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
         n = self.nbas
@@ -227,3 +240,18 @@ def hartree_exchange_potential(n1: int, P: np.ndarray, ERI: np.ndarray, physicis
     K = np.zeros(n * n)
     _check(lib().tce_hartree_exchange(int(n1), int(n), int(physicist), _d(Pf), _d(E), _d(J), _d(K)))
     return J.reshape(n, n, order="F"), K.reshape(n, n, order="F")
+
+
+def shard_plan(cost: np.ndarray, nranks: int) -> np.ndarray:
+    """Cost-balanced owner of each work item (host-only, no GPU needed)."""
+    c = np.ascontiguousarray(cost, dtype=np.float64)
+    owner = np.zeros(len(c), dtype=np.int32)
+    _check(lib().tce_shard_plan(_d(c), len(c), int(nranks), _i(owner)))
+    return owner
+
+
+def fp64_peak_tflops() -> float:
+    """Measured FP64 FMA throughput of the current device (probe kernel)."""
+    v = C.c_double()
+    _check(lib().tce_fp64_peak(C.byref(v)))
+    return v.value
