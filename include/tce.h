@@ -93,6 +93,19 @@ int tce_get_info(void *handle, tce_info *info);
  * loops; needs S1 in the unit cell); 2: no screens (primitive-table pass). */
 int tce_shell_block(void *handle, const int32_t sh4[4], int32_t mode, double *blk);
 
+/* Same block as tce_shell_block, for callers that cannot have the library
+ * allocate device memory during the call: a host program whose device
+ * memory is reserved up front by its own pool allocator, where a cudaMalloc
+ * inside the library would fail or fragment the pool.  No counterpart in the
+ * reference.  The call allocates nothing: its scratch (work counter, work
+ * item, block) is one file-scope device array of 12 KiB that every GPU using
+ * the library holds until exit.  The first call on a device resolves the
+ * array's device address; make that first call before any stream capture.
+ * Blocks of more than 6^4 integrals are rejected (TCE_ERR_UNSUPPORTED).  All
+ * calls share the array: calls that overlap on the GPU race, so do not issue
+ * them concurrently from several threads or handles. */
+int tce_shell_block_noalloc(void *handle, const int32_t sh4[4], int32_t mode, double *blk);
+
 /* Shell list: first function and component count of each shell. */
 int tce_shells(void *handle, int32_t *first, int32_t *n);
 

@@ -7,7 +7,9 @@
 // device.  Host code here only sizes buffers, orders the work list and moves
 // data.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <numeric>
@@ -798,6 +800,89 @@ int tce_shell_block(void *handle, const int32_t sh4[4], int32_t mode, double *bl
     int s = run_blocks(h, items, nullptr, mode == 2 ? TCE_MODE_NOSCREEN : TCE_MODE_BLOCK, mode == 1, &blocks, nullptr);
     if (s) return s;
     std::memcpy(blk, blocks.data(), blocks.size() * sizeof(double));
+    return TCE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free shell-quartet block.  The scratch the quartet kernel needs
+// for one block (its work counter, the work item, the block offsets and the
+// block itself, at most 6^4 doubles for d shells) lives in this file-scope
+// device array instead of buffers allocated per call, so the call makes no
+// cudaMalloc/cudaFree.  Every GPU that loads the library holds the array
+// (12 KiB) until the process exits.
+// ---------------------------------------------------------------------------
+#define TCE_STATIC_SCRATCH_BYTES (12 * 1024)
+#define TCE_STATIC_MAX_BLOCK (TCE_NCOMP_MAX * TCE_NCOMP_MAX * TCE_NCOMP_MAX * TCE_NCOMP_MAX)
+static __device__ __align__(256) unsigned char g_tce_static_scratch[TCE_STATIC_SCRATCH_BYTES];
+// layout inside the array (byte offsets)
+#define TCE_STATIC_OFF_NEXT 0      // unsigned int work counter
+#define TCE_STATIC_OFF_ITEM 256    // int4 work item
+#define TCE_STATIC_OFF_BOFF 512    // long long block offsets [2]
+#define TCE_STATIC_OFF_BLK 1024    // double block[TCE_STATIC_MAX_BLOCK]
+static_assert(TCE_STATIC_OFF_BLK + TCE_STATIC_MAX_BLOCK * sizeof(double) <= TCE_STATIC_SCRATCH_BYTES,
+              "static scratch too small for a (dd|dd) block");
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mu;
+unsigned char *g_static_ptr[kMaxDevices] = {nullptr};
+
+// Device address of the array on the current device, resolved once per device
+// (the symbol name is only a host-side stand-in for the device storage).
+int static_scratch(Handle *h, unsigned char **out)
+{
+    int dev = 0;
+    CK(h, cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return fail(h, TCE_ERR_UNSUPPORTED, "device index beyond 64");
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_ptr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_tce_static_scratch);
+        if (e != cudaSuccess)
+            return fail(h, TCE_ERR_CUDA, std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
+        g_static_ptr[dev] = static_cast<unsigned char *>(p);
+    }
+    *out = g_static_ptr[dev];
+    return TCE_OK;
+}
+}  // namespace
+
+int tce_shell_block_noalloc(void *handle, const int32_t sh4[4], int32_t mode, double *blk)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !sh4 || !blk) return fail(h, TCE_ERR_ARG, "NULL argument");
+    for (int i = 0; i < 4; ++i)
+        if (sh4[i] < 0 || sh4[i] >= h->nsh) return fail(h, TCE_ERR_ARG, "shell index out of range");
+    if (mode < 0 || mode > 2) return fail(h, TCE_ERR_ARG, "mode must be 0, 1 or 2");
+    if (mode == 1 && !h->prim_screen) return fail(h, TCE_ERR_STATE, "mode 1 needs prim_screen");
+    long long nblk = (long long)h->sh_n[sh4[0]] * h->sh_n[sh4[1]] * h->sh_n[sh4[2]] * h->sh_n[sh4[3]];
+    if (nblk > TCE_STATIC_MAX_BLOCK)
+        return fail(h, TCE_ERR_UNSUPPORTED, "block of " + std::to_string(nblk) + " integrals exceeds the static scratch (" +
+                                                 std::to_string(TCE_STATIC_MAX_BLOCK) + ")");
+    unsigned char *base = nullptr;
+    int s = static_scratch(h, &base);
+    if (s) return s;
+    int c1 = sh4[0] / h->nshuc;
+    int4 q = make_int4(shift_to(h, sh4[0], c1, h->nshuc), shift_to(h, sh4[1], c1, h->nshuc),
+                       shift_to(h, sh4[2], c1, h->nshuc), shift_to(h, sh4[3], c1, h->nshuc));
+    long long off[2] = {0, nblk};
+    // the work counter must start at zero; the item and offsets are rewritten every call
+    CK(h, cudaMemsetAsync(base + TCE_STATIC_OFF_NEXT, 0, sizeof(unsigned int), h->st));
+    CK(h, cudaMemcpyAsync(base + TCE_STATIC_OFF_ITEM, &q, sizeof q, cudaMemcpyHostToDevice, h->st));
+    CK(h, cudaMemcpyAsync(base + TCE_STATIC_OFF_BOFF, off, sizeof off, cudaMemcpyHostToDevice, h->st));
+    QuartetHostArgs a;
+    a.items = reinterpret_cast<const int4 *>(base + TCE_STATIC_OFF_ITEM);
+    a.nitems = 1;
+    a.mode = mode == 2 ? TCE_MODE_NOSCREEN : TCE_MODE_BLOCK;
+    a.prim_screen = mode == 1;
+    a.next = reinterpret_cast<unsigned int *>(base + TCE_STATIC_OFF_NEXT);
+    a.blk_out = reinterpret_cast<double *>(base + TCE_STATIC_OFF_BLK);
+    a.blk_off = reinterpret_cast<const long long *>(base + TCE_STATIC_OFF_BOFF);
+    a.max_ncomb = ncomb_of(h, q.x, q.y, q.z, q.w);
+    a.num_sms = h->num_sms;
+    CKS(h, tce_launch_quartets(h->S, a, h->st));
+    CK(h, cudaMemcpyAsync(blk, base + TCE_STATIC_OFF_BLK, sizeof(double) * nblk, cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
     return TCE_OK;
 }
 

@@ -36,7 +36,7 @@ TCE_OK, TCE_ERR_ARG, TCE_ERR_UNSUPPORTED, TCE_ERR_CUDA, TCE_ERR_STATE, TCE_ERR_N
 EXPORTS = ["tce_create", "tce_destroy", "tce_last_error", "tce_get_info", "tce_shell_block", "tce_shells",
            "tce_schwarz", "tce_eri_stored", "tce_stored_jk", "tce_hartree_exchange", "tce_direct_jk",
            "tce_direct_jk_device", "tce_last_kernel_ms", "tce_set_shard", "tce_shard_plan", "tce_fp64_peak",
-           "tce_version"]
+           "tce_shell_block_noalloc", "tce_version"]
 
 
 class TCEError(RuntimeError):
@@ -77,6 +77,7 @@ def lib():
         L.tce_last_error.argtypes = [C.c_void_p]
         L.tce_get_info.argtypes = [C.c_void_p, C.POINTER(TceInfo)]
         L.tce_shell_block.argtypes = [C.c_void_p, _ip, C.c_int32, _dp]
+        L.tce_shell_block_noalloc.argtypes = [C.c_void_p, _ip, C.c_int32, _dp]
         L.tce_shells.argtypes = [C.c_void_p, _ip, _ip]
         L.tce_schwarz.argtypes = [C.c_void_p, _dp]
         L.tce_eri_stored.argtypes = [C.c_void_p, C.c_int64, _dp]
@@ -190,6 +191,15 @@ class Engine:
         blk = np.zeros(int(np.prod(n)))
         q = np.array([S1, S2, S3, S4], dtype=np.int32)
         _check(lib().tce_shell_block(self.h, _i(q), int(mode), _d(blk)), self.h)
+        return blk.reshape(n, order="F")
+
+    def ERI_shell_block_noalloc(self, S1, S2, S3, S4, mode=1) -> np.ndarray:
+        """tce_shell_block_noalloc: the same block, scratch in the library's static device array."""
+        sh = self.shells()
+        n = [sh[S][1] for S in (S1, S2, S3, S4)]
+        blk = np.zeros(int(np.prod(n)))
+        q = np.array([S1, S2, S3, S4], dtype=np.int32)
+        _check(lib().tce_shell_block_noalloc(self.h, _i(q), int(mode), _d(blk)), self.h)
         return blk.reshape(n, order="F")
 
     def ERI_integral_toroidal(self) -> np.ndarray:
