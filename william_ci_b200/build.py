@@ -13,7 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtce.so")
-SOURCES = ["tce_api.cu", "tce_kernels.cu"]
+SOURCES = ["tce_api.cu", "tce_kernels.cu", "tce_kernels_s.cu"]
+OBJDIR = os.path.join(HERE, "_build")
 HEADERS = ["tce_device.cuh", "tce_kernels.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -25,30 +26,49 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
-def _stale() -> bool:
-    if not os.path.exists(LIB):
-        return True
-    t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(ROOT, "include", "tce.h")]
-    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+def _mtime(path):
+    return os.path.getmtime(path) if os.path.exists(path) else -1.0
 
 
-def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
-    if not force and not _stale():
-        return LIB
-    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-           "-I", os.path.join(ROOT, "include"), "-o", LIB + ".tmp"]
+def _headers():
+    return [os.path.join(CSRC, f) for f in HEADERS] + [os.path.join(ROOT, "include", "tce.h")]
+
+
+def _compile(src: str, obj: str, verbose: bool, ptxas_info: bool) -> None:
+    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-c",
+           "-I", os.path.join(ROOT, "include"), "-o", obj + ".tmp", src]
     if ptxas_info:
-        cmd += ["-Xptxas", "-v"]
-    cmd += [os.path.join(CSRC, f) for f in SOURCES]
+        cmd[1:1] = ["-Xptxas", "-v"]
     if verbose:
         print(" ".join(cmd))
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
-    if verbose or ptxas_info:
+        raise RuntimeError("nvcc failed on %s:\n%s%s" % (src, r.stdout, r.stderr))
+    if ptxas_info:
         sys.stdout.write(r.stdout + r.stderr)
-    os.replace(LIB + ".tmp", LIB)
+    os.replace(obj + ".tmp", obj)
+
+
+def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
+    """Compile each source to an object (only when it or a header changed), then link."""
+    os.makedirs(OBJDIR, exist_ok=True)
+    hdr_t = max(_mtime(h) for h in _headers())
+    objs, relink = [], force or not os.path.exists(LIB)
+    for f in SOURCES:
+        src = os.path.join(CSRC, f)
+        obj = os.path.join(OBJDIR, f.replace(".cu", ".o"))
+        objs.append(obj)
+        if force or _mtime(obj) < max(_mtime(src), hdr_t):
+            _compile(src, obj, verbose, ptxas_info)
+            relink = True
+        elif _mtime(obj) > _mtime(LIB):
+            relink = True
+    if relink:
+        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB + ".tmp", *objs]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("link failed:\n" + r.stdout + r.stderr)
+        os.replace(LIB + ".tmp", LIB)
     return LIB
 
 

@@ -56,7 +56,11 @@ struct Handle {
     std::vector<int4> items_host;       // sorted, most expensive first
     std::vector<double> cost_host;
     int shard_rank = 0, shard_nranks = 1;
-    int4 *d_items_shard = nullptr;
+    // the J/K work of this shard, one list per kernel: kind 0 generic
+    // (k_quartets), 1 all-s (k_quartets_s), 2 one-periodic-direction s/p class
+    // `cls` (k_quartets_r1)
+    struct WorkList { int kind, cls; int4 *d = nullptr; long long n = 0; };
+    std::vector<WorkList> lists;
     long long nitems_shard = 0;
     int *d_tnmax = nullptr;
     unsigned int *d_next = nullptr;
@@ -190,6 +194,52 @@ int shift_by(const Handle *h, int idx, int ct, int nblk)
     int cy = mod_pos((c / ncl[0]) % ncl[1] + (ct / ncl[0]) % ncl[1], ncl[1]);
     int cz = mod_pos(c / (ncl[0] * ncl[1]) + ct / (ncl[0] * ncl[1]), ncl[2]);
     return (cx + ncl[0] * (cy + ncl[1] * cz)) * nblk + loc;
+}
+
+// which kernel evaluates a quartet in J/K mode: key = kind * 16 + cls
+int route(const Handle *h, const int4 &q)
+{
+    const int l[4] = {h->sh_l[q.x], h->sh_l[q.y], h->sh_l[q.z], h->sh_l[q.w]};
+    int cls = 0;
+    bool sp = true;
+    for (int i = 0; i < 4; ++i) {
+        if (l[i] > 1) sp = false;
+        else cls |= l[i] << i;
+    }
+    if (sp) {
+        for (int i = 0; i < 4; ++i) {   // r1 needs the reference component order px, py, pz
+            int S = (&q.x)[i];
+            if (l[i] == 1)
+                for (int c = 0; c < 3; ++c)
+                    for (int d = 0; d < 3; ++d)
+                        if (h->lxyz[3 * (h->sh_first[S] + c) + d] != (c == d ? 1 : 0)) sp = false;
+        }
+    }
+    if (cls == 0 && sp && (h->nq == 32 || h->nq == 40)) return 1 * 16;
+    if (sp && tce_r1_supported(h->ndp, h->nq, cls)) return 2 * 16 + cls;
+    return 0;
+}
+
+// split a list of quartets (most expensive first) into per-kernel device lists
+int make_lists(Handle *h, const std::vector<int4> &items)
+{
+    for (auto &w : h->lists) dfree(h, w.d);
+    h->lists.clear();
+    std::vector<std::vector<int4>> by(3 * 16);
+    for (const int4 &q : items) by[route(h, q)].push_back(q);
+    h->nitems_shard = 0;
+    for (int key = 0; key < 3 * 16; ++key) {
+        if (by[key].empty()) continue;
+        Handle::WorkList w;
+        w.kind = key / 16;
+        w.cls = key % 16;
+        w.n = (long long)by[key].size();
+        int s = upload(h, &w.d, by[key]);
+        if (s) return s;
+        h->nitems_shard += w.n;
+        h->lists.push_back(w);
+    }
+    return TCE_OK;
 }
 
 int ncomb_of(const Handle *h, int SI, int SJ, int SK, int SL)
@@ -568,8 +618,7 @@ int build(Handle *h, const tce_system *sys)
         }
         if ((s = upload(h, &h->d_items, sorted))) return s;
         h->items_host = std::move(sorted);
-        h->d_items_shard = h->d_items;
-        h->nitems_shard = h->nitems;
+        if ((s = make_lists(h, h->items_host))) return s;
         // algorithmic work of one J/K pass
         unsigned long long *d_np = nullptr;
         double *d_fl = nullptr;
@@ -604,20 +653,36 @@ int direct_jk_device(Handle *h, const double *dP, double *dJ, double *dK, cudaSt
 {
     CK(h, cudaMemsetAsync(dJ, 0, sizeof(double) * h->nfuc * h->nbas, st));
     CK(h, cudaMemsetAsync(dK, 0, sizeof(double) * h->nfuc * h->nbas, st));
-    if (h->nitems_shard == 0) return TCE_OK;
-    QuartetHostArgs a;
-    a.items = h->d_items_shard;
-    a.nitems = (int)h->nitems_shard;
-    a.mode = TCE_MODE_JK;
-    a.prim_screen = h->prim_screen;
-    a.next = h->d_next;
-    a.P = dP;
-    a.J = dJ;
-    a.K = dK;
-    a.max_ncomb = h->max_ncomb;
-    a.num_sms = h->num_sms;
     CK(h, cudaEventRecord(h->ev0, st));
-    CKS(h, tce_launch_quartets(h->S, a, st));
+    for (const auto &w : h->lists) {
+        if (w.n == 0) continue;
+        if (w.kind == 0) {   // every other class: generic kernel
+            QuartetHostArgs a;
+            a.items = w.d;
+            a.nitems = (int)w.n;
+            a.mode = TCE_MODE_JK;
+            a.prim_screen = h->prim_screen;
+            a.next = h->d_next;
+            a.P = dP;
+            a.J = dJ;
+            a.K = dK;
+            a.max_ncomb = h->max_ncomb;
+            a.num_sms = h->num_sms;
+            CKS(h, tce_launch_quartets(h->S, a, st));
+        } else {             // register-resident kernels of the dominant classes
+            SArgsHost b;
+            b.items = w.d;
+            b.nitems = (int)w.n;
+            b.prim_screen = h->prim_screen;
+            b.next = h->d_next;
+            b.P = dP;
+            b.J = dJ;
+            b.K = dK;
+            b.num_sms = h->num_sms;
+            if (w.kind == 1) CKS(h, tce_launch_quartets_s(h->S, b, st));
+            else CKS(h, tce_launch_quartets_r1(h->S, w.cls, b, st));
+        }
+    }
     CK(h, cudaEventRecord(h->ev1, st));
     return TCE_OK;
 }
@@ -707,23 +772,15 @@ int tce_set_shard(void *handle, int32_t rank, int32_t nranks)
 {
     Handle *h = static_cast<Handle *>(handle);
     if (!h || nranks < 1 || rank < 0 || rank >= nranks) return fail(h, TCE_ERR_ARG, "bad shard");
-    if (h->d_items_shard && h->d_items_shard != h->d_items) dfree(h, h->d_items_shard);
-    h->shard_rank = rank;
-    h->shard_nranks = nranks;
-    if (nranks == 1) {
-        h->d_items_shard = h->d_items;
-        h->nitems_shard = h->nitems;
-        return TCE_OK;
-    }
     std::vector<int32_t> owner(h->items_host.size());
     int s = tce_shard_plan(h->cost_host.data(), (int64_t)owner.size(), nranks, owner.data());
     if (s) return fail(h, s, "shard plan failed");
     std::vector<int4> mine;
     for (size_t i = 0; i < owner.size(); ++i)
         if (owner[i] == rank) mine.push_back(h->items_host[i]);
-    h->nitems_shard = (long long)mine.size();
-    h->d_items_shard = nullptr;
-    if ((s = upload(h, &h->d_items_shard, mine))) return s;
+    if ((s = make_lists(h, mine))) return s;
+    h->shard_rank = rank;
+    h->shard_nranks = nranks;
     CK(h, cudaStreamSynchronize(h->st));
     return TCE_OK;
 }

@@ -210,3 +210,44 @@ __device__ __forceinline__ int tce_shift_to(int idx, int refcell, int nblk, cons
     int cz = tce_mod(c / (ncl[0] * ncl[1]) - tz, ncl[2]);
     return (cx + ncl[0] * (cy + ncl[1] * cz)) * nblk + loc;
 }
+
+// J/K contributions of one function quartet f = (i,j|k,l) of the block of
+// shell quartet (fI..|..), every stored element (p1 in the unit cell) once:
+// J(p1,p2) += E P(p3,p4), K(p1,p4) += -1/2 E P(p2,p3) (eri_direct.f90:331-357).
+// The element set of f is its 8 permutations translated to the unit cell; f
+// contributes only if it is the smallest member of that set inside the block,
+// and each distinct element once (the reference dedupes with a hash).
+__device__ __forceinline__ void tce_scatter_jk(const DevSys &S, const double *__restrict__ P, double *J, double *K,
+                                               const int f[4], double val, int fI, int nA, int fJ, int nB, int fK,
+                                               int nC, int fL, int nD)
+{
+    const int perm[8][4] = {{0,1,2,3},{1,0,2,3},{0,1,3,2},{1,0,3,2},{2,3,0,1},{3,2,0,1},{2,3,1,0},{3,2,1,0}};
+    int img[8][4];
+    for (int ip = 0; ip < 8; ++ip) {
+        int t[4];
+#pragma unroll
+        for (int ii = 0; ii < 4; ++ii) t[ii] = f[perm[ip][ii]];
+        int ref = t[0] / S.nfuc;
+#pragma unroll
+        for (int ii = 0; ii < 4; ++ii) img[ip][ii] = tce_shift_to(t[ii], ref, S.nfuc, S.ncl);
+        const int *g = img[ip];
+        bool inblk = g[0] >= fI && g[0] < fI + nA && g[1] >= fJ && g[1] < fJ + nB && g[2] >= fK && g[2] < fK + nC &&
+                     g[3] >= fL && g[3] < fL + nD;
+        if (inblk) {
+            for (int ii = 0; ii < 4; ++ii) {
+                if (g[ii] < f[ii]) return;
+                if (g[ii] > f[ii]) break;
+            }
+        }
+    }
+    for (int ip = 0; ip < 8; ++ip) {
+        const int *g = img[ip];
+        bool dup = false;
+        for (int jp = 0; jp < ip && !dup; ++jp)
+            dup = img[jp][0] == g[0] && img[jp][1] == g[1] && img[jp][2] == g[2] && img[jp][3] == g[3];
+        if (dup) continue;
+        atomicAdd(J + g[0] + (long long)S.nfuc * g[1], val * P[g[2] + (long long)S.nbas * g[3]]);
+        atomicAdd(K + g[0] + (long long)S.nfuc * g[3], -0.5 * val * P[g[1] + (long long)S.nbas * g[2]]);
+    }
+}
+

@@ -577,7 +577,6 @@ __global__ void __launch_bounds__(128) k_quartets(DevSys S, QuartetArgs A)
             }
         } else {
             const int fI = S.sh_first[Q.SI], fJ = S.sh_first[Q.SJ], fK = S.sh_first[Q.SK], fL = S.sh_first[Q.SL];
-            const int perm[8][4] = {{0,1,2,3},{1,0,2,3},{0,1,3,2},{1,0,3,2},{2,3,0,1},{3,2,0,1},{2,3,1,0},{3,2,1,0}};
             for (int cq = lane; cq < Q.ncq; cq += 32) {
                 int ca = cq % nA, r1 = cq / nA;
                 int cb = r1 % nB, r2 = r1 / nB;
@@ -585,29 +584,15 @@ __global__ void __launch_bounds__(128) k_quartets(DevSys S, QuartetArgs A)
                 int f[4] = {fI + ca, fJ + cb, fK + cc, fL + cd};
                 if (S.Q[f[0] + (long long)S.nbas * f[1]] * S.Q[f[2] + (long long)S.nbas * f[3]] < S.thr) continue;
                 const double val = blk[cq];
-                int img[8][4];
-                bool rep = true;
-                for (int ip = 0; ip < 8; ++ip) {
-                    int t[4];
-#pragma unroll
-                    for (int ii = 0; ii < 4; ++ii) t[ii] = f[perm[ip][ii]];
-                    int ref = t[0] / S.nfuc;
-#pragma unroll
-                    for (int ii = 0; ii < 4; ++ii) img[ip][ii] = tce_shift_to(t[ii], ref, S.nfuc, S.ncl);
-                    // an image inside this block that sorts before f: f is not the representative
-                    const int *g = img[ip];
-                    bool inblk = g[0] >= fI && g[0] < fI + nA && g[1] >= fJ && g[1] < fJ + nB && g[2] >= fK &&
-                                 g[2] < fK + nC && g[3] >= fL && g[3] < fL + nD;
-                    if (inblk) {
-                        for (int ii = 0; ii < 4; ++ii) {
-                            if (g[ii] < f[ii]) { rep = false; break; }
-                            if (g[ii] > f[ii]) break;
-                        }
-                    }
-                }
                 if (A.mode == TCE_MODE_STORE) {
+                    const int perm[8][4] = {{0,1,2,3},{1,0,2,3},{0,1,3,2},{1,0,3,2},{2,3,0,1},{3,2,0,1},{2,3,1,0},{3,2,1,0}};
                     for (int ip = 0; ip < 8; ++ip) {
-                        const int *g = img[ip];
+                        int g[4];
+#pragma unroll
+                        for (int ii = 0; ii < 4; ++ii) g[ii] = f[perm[ip][ii]];
+                        int ref = g[0] / S.nfuc;
+#pragma unroll
+                        for (int ii = 0; ii < 4; ++ii) g[ii] = tce_shift_to(g[ii], ref, S.nfuc, S.ncl);
                         long long e;
                         if (A.physicist)
                             e = g[0] + (long long)A.eri_size * (g[2] + (long long)S.nbas * (g[1] + (long long)S.nbas * g[3]));
@@ -617,16 +602,7 @@ __global__ void __launch_bounds__(128) k_quartets(DevSys S, QuartetArgs A)
                     }
                     continue;
                 }
-                if (!rep) continue;
-                for (int ip = 0; ip < 8; ++ip) {
-                    const int *g = img[ip];
-                    bool dup = false;
-                    for (int jp = 0; jp < ip && !dup; ++jp)
-                        dup = img[jp][0] == g[0] && img[jp][1] == g[1] && img[jp][2] == g[2] && img[jp][3] == g[3];
-                    if (dup) continue;
-                    atomicAdd(A.J + g[0] + (long long)S.nfuc * g[1], val * A.P[g[2] + (long long)S.nbas * g[3]]);
-                    atomicAdd(A.K + g[0] + (long long)S.nfuc * g[3], -0.5 * val * A.P[g[1] + (long long)S.nbas * g[2]]);
-                }
+                tce_scatter_jk(S, A.P, A.J, A.K, f, val, fI, nA, fJ, nB, fK, nC, fL, nD);
             }
         }
         __syncwarp();

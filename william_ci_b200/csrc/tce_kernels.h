@@ -30,6 +30,24 @@ struct QuartetHostArgs {
 };
 
 int tce_launch_quartets(const DevSys &S, const QuartetHostArgs &h, cudaStream_t st);
+
+// all-s shell quartets, J/K mode (k_quartets_s)
+struct SArgsHost {
+    const int4 *items = nullptr;
+    int nitems = 0;
+    int prim_screen = 0;
+    unsigned int *next = nullptr;
+    const double *P = nullptr;
+    double *J = nullptr, *K = nullptr;
+    int num_sms = 148;
+};
+int tce_launch_quartets_s(const DevSys &S, const SArgsHost &h, cudaStream_t st);
+// 1D s/p classes (k_quartets_r1); cls bit i = angular momentum (0/1) of shell i
+int tce_launch_quartets_r1(const DevSys &S, int cls, const SArgsHost &h, cudaStream_t st);
+inline bool tce_r1_supported(int ndp, int nq, int cls)
+{
+    return ndp == 1 && nq == 32 && cls >= 0 && cls < 16 && __builtin_popcount(cls) == 1;
+}
 int tce_launch_t_tables(int nq, int ndp, int ncap, const double *tnode, const double *a, double *tb, int *tnmax,
                         double *Tt, cudaStream_t st);
 int tce_launch_pair_scalars(const DevSys &S, long long npp_tot, const int *pp_unit, PairPrim *pp, UnitPair *up,
