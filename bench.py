@@ -32,6 +32,7 @@ sys.path.insert(0, ROOT)
 METRIC = "toroidal ERI quartets/s at ≤1e-10 err, learned-grid vs plain; RHF SCF iter time"
 WORKLOAD = "h_chain64"
 SYSTEM_FIXTURE = os.path.join(ROOT, "tests", "golden", "systems", WORKLOAD + ".npz")
+ONEE_FIXTURE = os.path.join(ROOT, "tests", "golden", "systems", WORKLOAD + "_onee.npz")
 PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "k_quartets_h_chain64_traffic.json")
 L2_FLUSH_BYTES = 512 << 20
 
@@ -84,6 +85,20 @@ def cpu_baseline(sysm, stride, reps=1):
             "sample": "direct_JK over every %d-th of the %d unique shell quartets (%d function quartets, %.2f s); "
                       "C restatement of the reference (no Fortran compiler here or on the GPU box)"
                       % (stride, len(items), nf, best)}
+
+
+def scf_iterations(eng, sysm, n_iter=5):
+    """RHF SCF iteration time (RHF_SAO mirror: host linear algebra + device direct J/K)."""
+    from william_ci_b200 import scf
+    z = np.load(ONEE_FIXTURE)
+    S_, T_, V_ = (scf.fill_with_symmetry(z[k], sysm.nfuc, sysm.ncell) for k in ("S", "T", "V"))
+    r = scf.rhf_sao(S_, T_, V_, float(z["enuc"]), scf.n_occupied(sysm), sysm.nfuc, sysm.ncell, eng.direct_JK,
+                    max_scf=n_iter)
+    it = r.iter_seconds[1:] if len(r.iter_seconds) > 1 else r.iter_seconds
+    jk = r.jk_seconds[1:] if len(r.jk_seconds) > 1 else r.jk_seconds
+    return {"iter_ms": 1e3 * float(np.mean(it)), "jk_ms": 1e3 * float(np.mean(jk)), "iterations_timed": len(it),
+            "energy_after": r.energy, "host": "numpy (SAO transforms, per-k eigh, DIIS)",
+            "note": "64-cell H chain, half-filled band: timing of SCF iterations, not a converged energy"}
 
 
 def reference_arm(args, sysm):
@@ -295,6 +310,8 @@ def main():
                                     "shell_quartets": info["n_shell_quartets"],
                                     "function_quartets": nq_total, "primitive_quartets": info["n_prim_quartets"]}),
             "e2e": e2e, "roofline": roofline, "clocks": clk, "gpu_launches": args.steps}
+    if world == 1:
+        line["rhf_scf"] = scf_iterations(eng, sysm)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(sysm, stride=1)
     print(json.dumps(line), flush=True)

@@ -77,6 +77,9 @@ def lib():
         L.orc_items.argtypes = [C.c_void_p, _ip, C.c_int64]
         L.orc_direct_jk_items.restype = C.c_int64
         L.orc_direct_jk_items.argtypes = [C.c_void_p, _ip, C.c_int64, _dp, _dp, _dp]
+        L.orc_one_electron.argtypes = [C.c_void_p, C.c_int, _dp, _ip, _dp, _dp, _dp]
+        L.orc_nuclear_repulsion.restype = C.c_double
+        L.orc_nuclear_repulsion.argtypes = [C.c_int, _dp, C.c_int, _dp, _ip]
         L.orc_overlap_pair.restype = C.c_double
         L.orc_overlap_pair.argtypes = [C.c_int, _dp, _ip, _ip, _dp, _dp, C.c_int, _dp, _dp, C.c_int, _dp, _dp]
         L.orc_normalize.restype = C.c_double
@@ -271,6 +274,15 @@ class Oracle:
         nf = lib().orc_direct_jk_items(self.h, iptr(it), len(it), dptr(Pf), dptr(Jf), dptr(Kf))
         return Jf.reshape(n, n, order="F"), Kf.reshape(n, n, order="F"), nf
 
+    def one_electron(self):
+        """S, T, V of the supercell (rows of the unit cell computed, the rest by translation)."""
+        n = self.sys.nbas
+        geo = np.ascontiguousarray(self.sys.geometry, dtype=np.float64).ravel()
+        Z = np.ascontiguousarray(self.sys.charges, dtype=np.int32)
+        S, T, V = (np.zeros(n * n) for _ in range(3))
+        lib().orc_one_electron(self.h, len(Z), dptr(geo), iptr(Z), dptr(S), dptr(T), dptr(V))
+        return tuple(M.reshape(n, n, order="F") for M in (S, T, V))
+
     def count(self):
         a, b, c = C.c_int64(), C.c_int64(), C.c_int64()
         lib().orc_count(self.h, C.byref(a), C.byref(b), C.byref(c))
@@ -285,3 +297,10 @@ def hartree_exchange(n1, P, eri, physicist=False):
     K = np.zeros(n * n)
     lib().orc_hartree_exchange(n1, n, int(physicist), dptr(Pf), dptr(E), dptr(J), dptr(K))
     return J.reshape(n, n, order="F"), K.reshape(n, n, order="F")
+
+
+def nuclear_repulsion(sys) -> float:
+    L = np.ascontiguousarray(sys.L, dtype=np.float64)
+    geo = np.ascontiguousarray(sys.geometry, dtype=np.float64).ravel()
+    Z = np.ascontiguousarray(sys.charges, dtype=np.int32)
+    return lib().orc_nuclear_repulsion(sys.ndp, dptr(L), len(Z), dptr(geo), iptr(Z))

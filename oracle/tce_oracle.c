@@ -290,7 +290,7 @@ void orc_hermite_E_1D(int i, int j, double p, double PA, double PB, double *E)
  * one-electron overlap (normalisation input): clifford_tools.f90:120-380,
  * 1D_Overlap_toroidal.f90:83-157, 2D/3D analogues.
  * ===================================================================== */
-static double Ttab[NMC + 1][NMC + 1][NMC / 2 + 1][NMC + 1];
+static double Ttab[NMC + 1][NMC + 1][NMC / 2 + 1][NMC + 1];   /* filled once by init_clifford, outside parallel regions */
 static double binom_t[NMC + 1][NMC + 1];
 static double dfact_t[2 * NMC + 2]; /* dfact(n) at [n+1] */
 static int clifford_ready = 0;
@@ -879,6 +879,7 @@ void orc_shell_block(orc_ctx *c, int S1, int S2, int S3, int S4, int mode, doubl
 
 orc_ctx *orc_create(const orc_system *sys)
 {
+    init_clifford();
     orc_ctx *c = calloc(1, sizeof(orc_ctx));
     c->s = *sys;
     int nbas = c->nbas = sys->nbas, nfuc = c->nfuc = sys->nfuc, ndp = c->ndp = sys->ndp;
@@ -1415,4 +1416,212 @@ int64_t orc_direct_jk_items(orc_ctx *c, const int32_t *items4, int64_t nitems, c
         free(Jl); free(Kl); free(hkey); free(used);
     }
     return nf;
+}
+
+/* =====================================================================
+ * one-electron matrices for the SCF consumer (inputs of RHF_SAO)
+ * ===================================================================== */
+
+/* kinetic_1D_clifford clifford_tools.f90:305-330 */
+static double kinetic_1D_clifford(int i, int l, double beta, double ax, double spa, double cpa, double spb,
+                                  double cpb, double R[NMC + 1][NMC + 1], double L)
+{
+    double inv_ax = 1.0 / ax, acc = 0.0;
+    if (l >= 2) acc += (double)(l * (l - 1)) * overlap_1D_clifford_ext(i, l - 2, 0, 0, spa, cpa, spb, cpb, inv_ax, R, L);
+    if (l >= 1) acc -= (double)(l * l) * ax * ax * overlap_1D_clifford_ext(i, l, 0, 0, spa, cpa, spb, cpb, inv_ax, R, L);
+    double cosu = cpb * overlap_1D_clifford_ext(i, l, 0, 1, spa, cpa, spb, cpb, inv_ax, R, L) -
+                  spb * overlap_1D_clifford_ext(i, l, 1, 0, spa, cpa, spb, cpb, inv_ax, R, L);
+    acc -= 2.0 * beta * (double)(2 * l + 1) * cosu;
+    acc += 4.0 * beta * beta * overlap_1D_clifford_ext(i, l + 2, 0, 0, spa, cpa, spb, cpb, inv_ax, R, L);
+    return acc;
+}
+
+/* kinetic_1D_real clifford_tools.f90:368-379 */
+static double kinetic_1D_real(int j, int m, double beta, double p, double pa, double pb)
+{
+    double acc = -2.0 * beta * (double)(2 * m + 1) * overlap_1D_real(j, m, p, pa, pb) +
+                 4.0 * beta * beta * overlap_1D_real(j, m + 2, p, pa, pb);
+    if (m >= 2) acc += (double)(m * (m - 1)) * overlap_1D_real(j, m - 2, p, pa, pb);
+    return acc;
+}
+
+/* kinetic_integral_toroidal_{1,2,3}D (1D_Kinetic_toroidal.f90:18-97, 3D_Kinetic_toroidal.f90) */
+double orc_kinetic_pair(int ndp, const double L[3], const int32_t l1[3], const int32_t l2[3], const double r1[3],
+                        const double r2[3], int n1, const double *e1, const double *c1, int n2, const double *e2,
+                        const double *c2)
+{
+    init_clifford();
+    double K = 0.0, R[NMC + 1][NMC + 1];
+    for (int i = 0; i < n1; ++i)
+        for (int j = 0; j < n2; ++j) {
+            double al = e1[i], be = e2[j], sd[3], dd[3];
+            for (int d = 0; d < 3; ++d) {
+                if (d < ndp) {
+                    double a = 2.0 * PI_D / L[d], pe, cen;
+                    orc_bary(al, be, r1[d], r2[d], L[d], a, &pe, &cen);
+                    double A = 2.0 * pe / (a * a), kd = exp(-2.0 * (al + be - pe) / (a * a));
+                    double spa = sin(a * (cen - r1[d])), cpa = cos(a * (cen - r1[d]));
+                    double spb = sin(a * (cen - r2[d])), cpb = cos(a * (cen - r2[d]));
+                    int nmax = l1[d] + l2[d] + 2 < NMC ? l1[d] + l2[d] + 2 : NMC;
+                    clifford_bessel_ratios(nmax, A, R);
+                    sd[d] = kd * overlap_1D_clifford_ext(l1[d], l2[d], 0, 0, spa, cpa, spb, cpb, 1.0 / a, R, L[d]);
+                    dd[d] = kd * kinetic_1D_clifford(l1[d], l2[d], be, a, spa, cpa, spb, cpb, R, L[d]);
+                } else {
+                    double es = al + be, mu = al * be / es, P = (al * r1[d] + be * r2[d]) / es;
+                    double k = exp(-mu * (r1[d] - r2[d]) * (r1[d] - r2[d]));
+                    sd[d] = k * overlap_1D_real(l1[d], l2[d], es, P - r1[d], P - r2[d]);
+                    dd[d] = k * kinetic_1D_real(l1[d], l2[d], be, es, P - r1[d], P - r2[d]);
+                }
+            }
+            K -= 0.5 * c1[i] * c2[j] * (dd[0] * sd[1] * sd[2] + sd[0] * dd[1] * sd[2] + sd[0] * sd[1] * dd[2]);
+        }
+    return K;
+}
+
+/* nuclear_attraction_integral_toroidal_{1,2,3}D (1D_Nuclear_attraction_toroidal.f90:26-163,
+ * 3D_Nuclear_attraction_toroidal.f90:18-113): periodic directions by the Fourier/Bessel
+ * t-quadrature, real directions by the Gaussian product with the nucleus. */
+static double nuclear_pair(const orc_ctx *c, const int32_t l1[3], const int32_t l2[3], const double r1[3],
+                           const double r2[3], int n1, const double *e1, const double *c1, int n2, const double *e2,
+                           const double *c2, int natoms, const double *geo, const int32_t *Z)
+{
+    const int ndp = c->ndp, nq = c->nq;
+    int M[3], Mmax = 0;
+    for (int d = 0; d < 3; ++d) { M[d] = l1[d] + l2[d]; if (d < ndp && M[d] > Mmax) Mmax = M[d]; }
+    int nw = c->ncap + Mmax + 2;
+    double *Iv = malloc(sizeof(double) * (nw + 64));
+    double *Gre = malloc(sizeof(double) * (nw + 1) * 3), *Gim = malloc(sizeof(double) * (nw + 1) * 3);
+    double *F = malloc(sizeof(double) * (nw + 1) * 3);
+    double V = 0.0;
+    for (int i = 0; i < n1; ++i)
+        for (int j = 0; j < n2; ++j) {
+            double al = e1[i], be = e2[j], es = al + be, mu = al * be / es;
+            double pref = c1[i] * c2[j] * 2.0 / sqrt(PI_D);
+            double cen[3];
+            int Np[3] = {0, 0, 0};
+            for (int d = 0; d < 3; ++d) {
+                if (d < ndp) {
+                    double a = c->a[d], pe;
+                    orc_bary(al, be, r1[d], r2[d], c->L[d], a, &pe, &cen[d]);
+                    double A = 2.0 * pe / (a * a);
+                    pref *= exp(-2.0 * (es - pe) / (a * a)) * c->L[d] / pow(a, M[d]);
+                    int est = orc_bessel_nmax_estimate(A);
+                    Np[d] = est < nw - Mmax - 2 ? est : nw - Mmax - 2;
+                    double dre[2 * NMC + 1], dim[2 * NMC + 1];
+                    orc_fourier_sin_product(l1[d], l2[d], a * (cen[d] - r1[d]), a * (cen[d] - r2[d]), dre, dim);
+                    orc_bessel_scaled_vector_fast(Np[d] + M[d], A, Iv);
+                    for (int n = 0; n <= Np[d]; ++n) {
+                        double ar = 0.0, ai = 0.0;
+                        for (int kk = -M[d]; kk <= M[d]; ++kk) {
+                            double b = Iv[abs(n + kk)];
+                            ar += dre[kk + M[d]] * b; ai += dim[kk + M[d]] * b;
+                        }
+                        Gre[n + (nw + 1) * d] = ar; Gim[n + (nw + 1) * d] = ai;
+                    }
+                } else {
+                    cen[d] = (al * r1[d] + be * r2[d]) / es;
+                    pref *= exp(-mu * (r1[d] - r2[d]) * (r1[d] - r2[d]));
+                }
+            }
+            for (int at = 0; at < natoms; ++at) {
+                const double *C = geo + 3 * at;
+                for (int d = 0; d < ndp; ++d) {
+                    double phi = c->a[d] * (cen[d] - C[d]);
+                    double cs1 = cos(phi), sn1 = sin(phi), cn = 1.0, sn = 0.0, tmp;
+                    for (int n = 0; n <= Np[d]; ++n) {
+                        if (n > 0) {
+                            if (n % 32 == 0) { cn = cos(n * phi); sn = sin(n * phi); }
+                            else { tmp = cn * cs1 - sn * sn1; sn = sn * cs1 + cn * sn1; cn = tmp; }
+                        }
+                        F[n + (nw + 1) * d] = Gre[n + (nw + 1) * d] * cn - Gim[n + (nw + 1) * d] * sn;
+                    }
+                }
+                double res = 0.0;
+                for (int k = 0; k < nq; ++k) {
+                    double prod = 1.0, t2 = c->t_node[k] * c->t_node[k];
+                    for (int d = 0; d < 3; ++d) {
+                        if (d < ndp) {
+                            int tn = c->t_nmax[k + nq * d], nt = Np[d] < tn ? Np[d] : tn;
+                            double sdv = F[(nw + 1) * d] * TB(c, 0, k, d), dot = 0.0;
+                            for (int n = 1; n <= nt; ++n) dot += F[n + (nw + 1) * d] * TB(c, n, k, d);
+                            if (nt >= 1) sdv += 2.0 * dot;
+                            prod *= sdv;
+                        } else {
+                            double ppt = es + t2, eta = t2 / ppt, pc = cen[d] - C[d];
+                            double ed = exp(-es * eta * pc * pc);
+                            double sdv = overlap_1D_real(l1[d], l2[d], ppt, (cen[d] - r1[d]) - eta * pc, (cen[d] - r2[d]) - eta * pc);
+                            prod *= ed * sdv;
+                        }
+                    }
+                    res += c->t_weight[k] * prod;
+                }
+                V -= (double)Z[at] * pref * res;
+            }
+        }
+    free(Iv); free(Gre); free(Gim); free(F);
+    return V;
+}
+
+/* fill_with_symmetry symmetric_matrix.f90:1-52: rows i >= nfuc from the first nfuc rows */
+static void fill_with_symmetry(int nbas, int nfuc, const int ncl[3], double *M)
+{
+    int nx = ncl[0], ny = ncl[1], nz = ncl[2];
+    for (int i = nfuc; i < nbas; ++i) {
+        int Ri = i / nfuc, a = i % nfuc;
+        int Rzi = Ri / (nx * ny), Ryi = (Ri / nx) % ny, Rxi = Ri % nx;
+        for (int j = 0; j < nbas; ++j) {
+            int Rj = j / nfuc, b = j % nfuc;
+            int Rzj = Rj / (nx * ny), Ryj = (Rj / nx) % ny, Rxj = Rj % nx;
+            int dx = mod_pos(Rxj - Rxi, nx), dy = mod_pos(Ryj - Ryi, ny), dz = mod_pos(Rzj - Rzi, nz);
+            int src = dz * nx * ny + dy * nx + dx;
+            M[i + (size_t)nbas * j] = M[a + (size_t)nbas * (b + src * nfuc)];
+        }
+    }
+}
+
+/* overlap / kinetic / nuclear-attraction matrices (rows < nfuc computed, |x| < 1e-14
+ * set to zero, the rest by translation), e.g. overlap_matrix_toroidal_1D
+ * 1D_Overlap_toroidal.f90:23-81 */
+void orc_one_electron(orc_ctx *c, int natoms, const double *geo, const int32_t *Z, double *S, double *T, double *V)
+{
+    int nbas = c->nbas, nfuc = c->nfuc;
+    init_clifford();   /* shared tables: fill them before the parallel region */
+    memset(S, 0, sizeof(double) * nbas * nbas);
+    memset(T, 0, sizeof(double) * nbas * nbas);
+    memset(V, 0, sizeof(double) * nbas * nbas);
+    #pragma omp parallel for schedule(dynamic, 4) collapse(2)
+    for (int i = 0; i < nfuc; ++i)
+        for (int j = 0; j < nbas; ++j) {
+            int pi = c->poff[i], ni = c->poff[i + 1] - pi, pj = c->poff[j], nj = c->poff[j + 1] - pj;
+            const int32_t *li = c->lxyz + 3 * i, *lj = c->lxyz + 3 * j;
+            const double *ri = c->ctr + 3 * i, *rj = c->ctr + 3 * j;
+            double s = orc_overlap_pair(c->ndp, c->L, li, lj, ri, rj, ni, c->exps + pi, c->coefs + pi, nj, c->exps + pj, c->coefs + pj);
+            double t = orc_kinetic_pair(c->ndp, c->L, li, lj, ri, rj, ni, c->exps + pi, c->coefs + pi, nj, c->exps + pj, c->coefs + pj);
+            double v = nuclear_pair(c, li, lj, ri, rj, ni, c->exps + pi, c->coefs + pi, nj, c->exps + pj, c->coefs + pj, natoms, geo, Z);
+            S[i + (size_t)nbas * j] = fabs(s) < 1e-14 ? 0.0 : s;
+            T[i + (size_t)nbas * j] = fabs(t) < 1e-14 ? 0.0 : t;
+            V[i + (size_t)nbas * j] = fabs(v) < 1e-14 ? 0.0 : v;
+        }
+    fill_with_symmetry(nbas, nfuc, c->ncl, S);
+    fill_with_symmetry(nbas, nfuc, c->ncl, T);
+    fill_with_symmetry(nbas, nfuc, c->ncl, V);
+}
+
+/* NRE Nuclear_repulsion.f90:1-59: chord distance along the periodic directions */
+double orc_nuclear_repulsion(int ndp, const double L[3], int natoms, const double *geo, const int32_t *Z)
+{
+    double E = 0.0;
+    for (int i = 0; i < natoms - 1; ++i)
+        for (int j = i + 1; j < natoms; ++j) {
+            double dd[3];
+            for (int d = 0; d < 3; ++d) {
+                dd[d] = geo[3 * i + d] - geo[3 * j + d];
+                if (d < ndp) {
+                    double a = 2.0 * PI_D / L[d];
+                    dd[d] = sqrt(2.0 * (1.0 - cos(a * dd[d])) / (a * a));
+                }
+            }
+            E += (double)Z[i] * (double)Z[j] / sqrt(dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]);
+        }
+    return E;
 }

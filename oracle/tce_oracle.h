@@ -113,6 +113,14 @@ double orc_overlap_pair(int ndp, const double L[3], const int32_t l1[3], const i
 double orc_normalize(int ndp, const double L[3], int nbas, const double *ctr, const int32_t *lxyz,
                      const int32_t *prim_off, const double *exps, double *coefs);
 
+/* ---- one-electron matrices and nuclear repulsion (RHF_SAO inputs) ---- */
+double orc_kinetic_pair(int ndp, const double L[3], const int32_t l1[3], const int32_t l2[3],
+                        const double r1[3], const double r2[3], int n1, const double *e1, const double *c1,
+                        int n2, const double *e2, const double *c2);
+/* S, T, V (nbas x nbas, col-major), geometry [3*natoms], charges [natoms] */
+void orc_one_electron(orc_ctx *c, int natoms, const double *geo, const int32_t *Z, double *S, double *T, double *V);
+double orc_nuclear_repulsion(int ndp, const double L[3], int natoms, const double *geo, const int32_t *Z);
+
 #ifdef __cplusplus
 }
 #endif

@@ -20,6 +20,7 @@ import pyoracle  # noqa: E402
 from william_ci_b200 import system as S  # noqa: E402
 
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "systems")
+ONE_ELECTRON = ("h2_ring", "h_chain64")   # RHF inputs stored for the SCF timing
 
 
 def main():
@@ -30,6 +31,15 @@ def main():
         path = os.path.join(OUT, name + ".npz")
         sysm.save(path)
         print("%-11s nbas %5d nfuc %3d  max|<phi|phi>-1| %.1e  -> %s" % (name, sysm.nbas, sysm.nfuc, dev, path))
+        if name in ONE_ELECTRON:
+            # S, T, V rows of the unit cell (the others follow by translation) and E_nuc,
+            # the inputs RHF_SAO receives (main.f90:379-500)
+            import numpy as np
+            o = pyoracle.Oracle(sysm)
+            S_, T_, V_ = o.one_electron()
+            nf = sysm.nfuc
+            np.savez(os.path.join(OUT, name + "_onee.npz"), S=S_[:nf], T=T_[:nf], V=V_[:nf],
+                     enuc=pyoracle.nuclear_repulsion(sysm))
 
 
 if __name__ == "__main__":
