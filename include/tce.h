@@ -160,6 +160,95 @@ int tce_shard_plan(const double *cost, int64_t n, int32_t nranks, int32_t *owner
  * probe kernel of independent FMA chains on every SM. */
 int tce_fp64_peak(double *tflops);
 
+/* ------------------------------------------------------------------------
+ * Learned-grid t-quadrature.  No counterpart in the reference, whose
+ * t-integral uses one fixed rule per run (fast_quad or the 64/128-point
+ * tables, precompute_t.f90:5-14, 906-942).  A dictionary of mapped
+ * Gauss-Kronrod rules (t = s u/(1-u), each with its embedded Gauss rule) is
+ * loaded once; a small network picks one rule per shell quartet from
+ * TCE_NFEAT features; in the J/K pass the Kronrod and Gauss estimates of the
+ * quartet's block are compared (the judge) and a quartet with
+ * max |K - G| > judge_tol is re-evaluated by the plain method: adaptive
+ * bisection in u with 15-point Kronrod / 7-point Gauss panels, the Bessel
+ * columns of every panel computed on the fly.
+ * ------------------------------------------------------------------------ */
+#define TCE_METHOD_FIXED   0   /* the system's rule (reference behaviour)      */
+#define TCE_METHOD_LEARNED 1   /* per-quartet rule + judge + plain fallback    */
+#define TCE_METHOD_PLAIN   2   /* plain adaptive method for every quartet      */
+#define TCE_NFEAT 12           /* features per shell quartet                   */
+
+/* The engine's work items (unique shell quartets, most expensive first):
+ * items[4*i .. 4*i+3], i < n_shell_quartets. */
+int tce_items(void *handle, int32_t *items);
+
+/* Features of n shell quartets (items 4*n ints, any cell; NULL: the engine's
+ * own items in order, n = n_shell_quartets) into feat[n*TCE_NFEAT]. */
+int tce_item_features(void *handle, int64_t n, const int32_t *items, float *feat);
+
+/* Rule dictionary: rule r has nn[r] <= 64 nodes t[64r+k], Kronrod weights
+ * wk[64r+k] and embedded Gauss weights wg[64r+k] (0 off the Gauss nodes).
+ * Builds each rule's Bessel table on the device. */
+int tce_lg_set_rules(void *handle, int32_t nrules, const int32_t *nn, const double *t, const double *wk,
+                     const double *wg);
+
+/* Per-rule truncation orders gmax[r*48 + d*16 + g] (node group g of 8 nodes,
+ * direction d): the last Bessel order with a nonzero table entry. */
+int tce_lg_rule_gmax(void *handle, int32_t *gmax);
+
+/* The plain method's panel rule: the 15-point Kronrod rule on u in [0,1]
+ * (n = 15) with the embedded 7-point Gauss weights, mapped t = scale u/(1-u). */
+int tce_set_plain_rule(void *handle, int32_t n, const double *u, const double *wk, const double *wg, double scale);
+
+/* Per-item rules (engine item order); value nrules sends the item straight to
+ * the plain method. */
+int tce_lg_set_item_rules(void *handle, const int32_t *rule);
+int tce_lg_item_rules(void *handle, int32_t *rule);
+
+/* Quadrature method of tce_direct_jk[_device] (TCE_METHOD_*). */
+int tce_set_method(void *handle, int32_t method);
+
+/* Judge tolerance on max |K - G| of a block (default 1e-10), plain-method
+ * tolerance on the summed panel estimates (default 1e-11) and its panel
+ * budget (1..24, default 24). */
+int tce_set_tolerances(void *handle, double judge_tol, double plain_tol, int32_t plain_max_panels);
+
+/* Counters of the last J/K pass: stats[0] quartets on the learned grid,
+ * stats[1] of those rejected by the judge, stats[2] quartets sent straight to
+ * the plain method, stats[3] t nodes the plain method evaluated. */
+int tce_lg_stats(void *handle, int64_t *stats);
+
+/* Blocks of n shell quartets with one quadrature, concatenated in item order
+ * (each column-major n1 n2 n3 n4): rule >= 0 a dictionary rule (Kronrod
+ * estimate in K, Gauss estimate in G when G is not NULL), -1 the system's
+ * rule, -2 the plain method.  mode as tce_shell_block. */
+int tce_rule_blocks(void *handle, int32_t rule, int32_t mode, int64_t n, const int32_t *items, double *K, double *G);
+
+/* The rule-picking network: TCE_NFEAT -> nh -> nh -> nc (ReLU), FP32 on the
+ * device, parameters flat W1[nh][nf] b1 W2[nh][nh] b2 W3[nc][nh] b3; inputs
+ * are standardised with per-feature mean mu and scale sig.  Output c is the
+ * logit of the probability that dictionary rule c is accepted by the judge
+ * and correct for the quartet (nc = number of rules). */
+int tce_mlp_create(int32_t nf, int32_t nh, int32_t nc, uint64_t seed, void **mlp);
+int tce_mlp_destroy(void *mlp);
+const char *tce_mlp_last_error(void *mlp);
+int tce_mlp_nparams(void *mlp, int64_t *np);
+int tce_mlp_get_params(void *mlp, float *p, float *mu, float *sig);
+int tce_mlp_set_params(void *mlp, const float *p, const float *mu, const float *sig);
+/* Sigmoid cross-entropy of the outputs against targets Y[n][nc] in [0,1],
+ * summed over outputs and averaged over rows, and its gradient (forward and
+ * backward kernels on the device). */
+int tce_mlp_loss_grad(void *mlp, int64_t n, const float *X, const float *Y, float *loss, float *grad);
+/* Adam training on shuffled mini-batches (standardisation set from X). */
+int tce_mlp_train(void *mlp, int64_t n, const float *X, const float *Y, int32_t epochs, int32_t batch, float lr,
+                  uint64_t seed, float *final_loss);
+/* Output probabilities prob[n][nc]. */
+int tce_mlp_predict(void *mlp, int64_t n, const float *X, float *prob);
+/* Features of every engine item, network forward and the rule of least
+ * expected cost on the device: cost_r + (1 - p_r) C_plain, C_plain =
+ * plain_factor x the dearest rule's cost (nrules, i.e. the plain method, when
+ * that is cheaper).  Sets the per-item rules; nc must equal nrules. */
+int tce_lg_predict_rules(void *handle, void *mlp, double plain_factor);
+
 /* Library build identification (sm_100a, version). */
 const char *tce_version(void);
 

@@ -1,0 +1,200 @@
+"""Learned-grid and plain-method quadrature on the device (through the C ABI).
+
+* plain adaptive method vs the 128-node reference rule (blocks), 1e-11;
+* the network's forward/backward kernels vs the numpy restatement
+  (oracle/mlp_ref.py), FP32 tolerance;
+* learned-grid J/K: rules picked by a network trained on the GPU; the blocks
+  of the picked rules are within 1e-10 of the reference, J/K agree with the
+  plain method's, the judge rejects few quartets, and the trained network
+  beats the method without it (one fixed dictionary rule + judge);
+* RHF energy with learned-grid J/K vs the oracle's, 1e-8 Eh.
+"""
+import numpy as np
+import pytest
+
+import mlp_ref
+from conftest import make_system, random_density
+
+pytestmark = pytest.mark.gpu
+
+TOL_INT = 1e-10
+
+CASES = [
+    ("h_chain64", (8, 1, 1)),
+    ("h2_sheet", (2, 2, 1)),
+    ("li_cube", (2, 2, 2)),
+]
+
+
+def _lg_engine(sysm):
+    from william_ci_b200 import learned_grid as LG
+    from william_ci_b200.engine import Engine
+    eng = Engine(sysm)
+    LG.setup(eng)
+    return eng
+
+
+def _sample(items, n, seed=0):
+    rng = np.random.default_rng(seed)
+    return items[rng.choice(len(items), min(n, len(items)), replace=False)]
+
+
+@pytest.mark.parametrize("name,ncell", CASES)
+def test_plain_blocks_vs_reference(systems, name, ncell):
+    from william_ci_b200 import learned_grid as LG
+    sysm = systems(name, ncell)
+    eng = _lg_engine(sysm)
+    ref = LG.ReferenceBlocks(sysm)
+    it = _sample(eng.items(), 400)
+    P, _, offs = eng.rule_blocks(-2, it, mode=1)
+    T, _, _ = ref.rule_blocks(-1, it, mode=1)
+    assert np.abs(P - T).max() < 1e-11
+
+
+def test_reference_blocks_split_equals_single_engine(systems):
+    """The 128-node reference evaluated as two 64-node halves equals one 128-node engine."""
+    from william_ci_b200 import learned_grid as LG
+    from william_ci_b200.engine import Engine
+    sysm = systems("h_chain64", (8, 1, 1))
+    t, w = LG.reference_rule()
+    one = Engine(sysm, t_nodes=t, t_weights=w)
+    ref = LG.ReferenceBlocks(sysm)
+    it = _sample(one.items(), 300)
+    A, _, _ = one.rule_blocks(-1, it)
+    B, _, _ = ref.rule_blocks(-1, it)
+    assert np.abs(A - B).max() < 1e-13
+
+
+def test_mlp_loss_grad_vs_oracle():
+    from william_ci_b200 import learned_grid as LG
+    rng = np.random.default_rng(3)
+    nc = 9
+    net = LG.RuleNet(nc, seed=5)
+    p, _, _ = net.params()
+    X = rng.standard_normal((257, 12)).astype(np.float32) * 3 + 1
+    Y = (rng.random((257, nc)) < 0.4).astype(np.float32)
+    mu = X.mean(0).astype(np.float32)
+    sig = X.std(0).astype(np.float32)
+    net.set_params(None, mu, sig)
+    L, g = net.loss_grad(X, Y)
+    Lr, gr = mlp_ref.loss_grad(p, mu, sig, X, Y, 12, 64, nc)
+    assert abs(L - Lr) <= 1e-5 * abs(Lr)
+    assert np.abs(g - gr).max() <= 1e-4 * np.abs(gr).max()
+    pr = net.predict(X)
+    np.testing.assert_allclose(pr, mlp_ref.predict(p, mu, sig, X, 12, 64, nc), atol=1e-5)
+
+
+def test_mlp_training_fits_separable_targets():
+    from william_ci_b200 import learned_grid as LG
+    rng = np.random.default_rng(4)
+    X = rng.standard_normal((4096, 12)).astype(np.float32)
+    W = rng.standard_normal((12, 5))
+    Y = (X @ W > 0).astype(np.float32)
+    net = LG.RuleNet(5, seed=1)
+    p0, _, _ = net.params()
+    L0, _ = net.loss_grad(X, Y)
+    L1 = net.train(X, Y, epochs=30, batch=128, lr=3e-3, seed=2)
+    assert L1 < 0.2 * L0
+    acc = ((net.predict(X) > 0.5) == (Y > 0.5)).mean()
+    assert acc > 0.97
+
+
+def _trained(eng, sysm, n_train=6000, seed=0):
+    from william_ci_b200 import learned_grid as LG
+    ref = LG.ReferenceBlocks(sysm)
+    items = eng.items()
+    tr = _sample(items, n_train, seed)
+    net, data, _ = LG.train_rule_net(eng, ref, tr, epochs=60, seed=seed)
+    return net, data, ref
+
+
+@pytest.mark.parametrize("name,ncell", [("h_chain64", (16, 1, 1)), ("li_cube", (2, 2, 2))])
+def test_learned_grid_jk(systems, name, ncell):
+    from william_ci_b200 import learned_grid as LG
+    from william_ci_b200.engine import TCE_METHOD_LEARNED, TCE_METHOD_PLAIN
+    sysm = systems(name, ncell)
+    eng = _lg_engine(sysm)
+    net, data, ref = _trained(eng, sysm)
+    eng.lg_predict_rules(net)
+    rules = eng.lg_item_rules()
+    items = eng.items()
+    # blocks of the chosen rules on a held-out sample: within 1e-10 of the reference
+    rng = np.random.default_rng(11)
+    sel = rng.choice(len(items), min(1500, len(items)), replace=False)
+    T, _, offs = ref.rule_blocks(-1, items[sel])
+    worst = 0.0
+    for r in np.unique(rules[sel]):
+        m = np.nonzero(rules[sel] == r)[0]
+        if r == eng.nrules:
+            K, _, o2 = eng.rule_blocks(-2, items[sel][m])
+        else:
+            K, G, o2 = eng.rule_blocks(int(r), items[sel][m], judge=True)
+            est = LG.judge_estimate(K, G, o2)
+            m, K, o2 = _accepted(m, K, o2, est)
+        for j, i in enumerate(m):
+            worst = max(worst, np.abs(K[o2[j]:o2[j + 1]] - T[offs[i]:offs[i + 1]]).max(initial=0.0))
+    assert worst <= TOL_INT
+    # J/K: learned grid vs the plain method
+    P = random_density(sysm.nbas, 1) * 0.05
+    eng.set_method(TCE_METHOD_PLAIN)
+    Jp, Kp = eng.direct_JK(P)
+    eng.set_method(TCE_METHOD_LEARNED)
+    Jl, Kl = eng.direct_JK(P)
+    st = eng.lg_stats()
+    assert st["learned"] + st["plain_direct"] == eng.info()["n_shell_quartets"]
+    assert st["rejected"] <= 0.01 * max(st["learned"], 1)
+    scale = np.abs(P).sum()
+    assert np.abs(Jl - Jp).max() <= 1e-10 * scale
+    assert np.abs(Kl - Kp).max() <= 1e-10 * scale
+
+
+def _accepted(m, K, offs, est):
+    """Keep the blocks the judge accepts (the others are re-evaluated by the plain method)."""
+    keep = np.nonzero(est <= 1e-10)[0]
+    Kk = np.concatenate([K[offs[j]:offs[j + 1]] for j in keep]) if len(keep) else np.zeros(0)
+    o = np.concatenate([[0], np.cumsum(np.diff(offs)[keep])]).astype(np.int64)
+    return m[keep], Kk, o
+
+
+def test_network_gain_over_single_rule(systems):
+    """What the trained network buys: the rules it picks cost less than the one
+    dictionary rule that is acceptable for the most quartets (the method
+    without the network), with few judge rejections."""
+    from william_ci_b200 import learned_grid as LG
+    sysm = systems("h_chain64", (16, 1, 1))
+    eng = _lg_engine(sysm)
+    net, data, ref = _trained(eng, sysm)
+    items = eng.items()
+    test = _sample(items, 3000, seed=9)
+    d = LG.make_labels(eng, ref, test)
+    eng.lg_predict_rules(net)
+    rule_of = {tuple(q): r for q, r in zip(items, eng.lg_item_rules())}
+    pr = np.array([rule_of[tuple(q)] for q in test])
+    R = eng.nrules
+    plain_cost = 10.0 * d["cost"].max(axis=1)
+    lg = np.where(pr < R, d["cost"][np.arange(len(pr)), np.minimum(pr, R - 1)], plain_cost)
+    rejected = (pr < R) & (d["judge"][np.arange(len(pr)), np.minimum(pr, R - 1)] > 1e-10)
+    lg_total = (lg + rejected * plain_cost).sum()
+    okfrac = data["ok"].mean(axis=0)
+    best = int(np.argmax(okfrac - 1e-9 * data["cost"].mean(axis=0)))
+    single = d["cost"][:, best] + (d["judge"][:, best] > 1e-10) * plain_cost
+    assert rejected.mean() < 0.01
+    assert lg_total < 0.9 * single.sum(), (lg_total, single.sum())
+
+
+@pytest.mark.parametrize("which", ["dimer_chain", "h2_sheet_2x2"])
+def test_rhf_energy_learned_grid_vs_oracle(which):
+    import pyoracle as po  # noqa: F401
+    from test_scf import dimer_chain, rhf_inputs
+    from william_ci_b200 import scf
+    from william_ci_b200.engine import TCE_METHOD_LEARNED
+    sysm = dimer_chain(8) if which == "dimer_chain" else make_system("h2_sheet", (2, 2, 1))
+    o, St, Tt, Vt, en, nO = rhf_inputs(sysm)
+    ref = scf.rhf_sao(St, Tt, Vt, en, nO, sysm.nfuc, sysm.ncell, lambda P: o.direct_jk(P)[:2])
+    eng = _lg_engine(sysm)
+    net, _, _ = _trained(eng, sysm, n_train=4000)
+    eng.lg_predict_rules(net)
+    eng.set_method(TCE_METHOD_LEARNED)
+    dev = scf.rhf_sao(St, Tt, Vt, en, nO, sysm.nfuc, sysm.ncell, eng.direct_JK)
+    assert ref.converged and dev.converged
+    assert abs(dev.energy - ref.energy) < 1e-8, (dev.energy, ref.energy)

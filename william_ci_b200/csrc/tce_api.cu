@@ -16,63 +16,9 @@
 #include <string>
 #include <vector>
 
-#include "tce_kernels.h"
+#include "tce_handle.h"
 
-namespace {
-
-constexpr double kPi = 3.14159265358979323846;
-
-struct Handle {
-    std::string err;
-    // system scalars
-    int ndp = 0, nq = 0, ncap = 0, nbas = 0, nfuc = 0, nsh = 0, nshuc = 0, ncell = 1;
-    int ncl[3] = {1, 1, 1};
-    double a[3] = {0, 0, 0}, L[3] = {0, 0, 0};
-    int physicist = 0, sao = 1, prim_screen = 1;
-    double thr = 1e-13, prim_thr = 1e-14;
-    // host copies
-    std::vector<double> ctr, exps, coefs, tnode, tweight;
-    std::vector<int> lxyz, poff;
-    std::vector<int> sh_first, sh_n, sh_l, sh_np, sh_eoff, sh_coff;
-    std::vector<double> sh_r, sh_exp, sh_coef, sh_cmax;
-    std::vector<UnitPair> up;
-    std::vector<double> Q, Qsh;
-    double Qmax = 0.0;
-    std::vector<int> tnmax;
-    // device
-    cudaStream_t st = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    int num_sms = 148;
-    std::vector<void *> allocs;
-    size_t bytes = 0;
-    DevSys S{};
-    PairPrim *d_pp = nullptr;
-    double *d_Qsh = nullptr;
-    int4 *d_items = nullptr;
-    long long nitems = 0;
-    int max_ncomb = 1;
-    long long n_func_q = 0, n_unit_sig = 0, n_prim_q = 0;
-    double jk_flops = 0.0;
-    std::vector<int4> items_host;       // sorted, most expensive first
-    std::vector<double> cost_host;
-    int shard_rank = 0, shard_nranks = 1;
-    // the J/K work of this shard, one list per kernel: kind 0 generic
-    // (k_quartets), 1 all-s (k_quartets_s), 2 one-periodic-direction s/p class
-    // `cls` (k_quartets_r1)
-    struct WorkList { int kind, cls; int4 *d = nullptr; long long n = 0; };
-    std::vector<WorkList> lists;
-    long long nitems_shard = 0;
-    int *d_tnmax = nullptr;
-    unsigned int *d_next = nullptr;
-    double *d_P = nullptr, *d_J = nullptr, *d_K = nullptr;
-    double *d_eri = nullptr;
-    long long eri_elems = 0;
-    int eri_size = 0;
-    double *d_blk = nullptr;
-    long long *d_blkoff = nullptr;
-    int4 *d_one = nullptr;
-    float last_ms = 0.f;
-};
+namespace tcehost {
 
 thread_local std::string g_err;
 
@@ -81,48 +27,6 @@ int fail(Handle *h, int code, const std::string &msg)
     if (h) h->err = msg;
     g_err = msg;
     return code;
-}
-
-#define CK(h, call)                                                                          \
-    do {                                                                                     \
-        cudaError_t e_ = (call);                                                             \
-        if (e_ != cudaSuccess)                                                               \
-            return fail((h), TCE_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-    } while (0)
-
-#define CKS(h, call)                                                  \
-    do {                                                              \
-        int s_ = (call);                                              \
-        if (s_ != TCE_OK) {                                           \
-            cudaError_t e_ = cudaGetLastError();                      \
-            return fail((h), s_, std::string(#call) + " failed" +     \
-                                     (e_ != cudaSuccess ? std::string(": ") + cudaGetErrorString(e_) : "")); \
-        }                                                             \
-    } while (0)
-
-template <class T>
-int dalloc(Handle *h, T **p, size_t n)
-{
-    *p = nullptr;
-    if (n == 0) n = 1;
-    cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return fail(h, TCE_ERR_NOMEM, "device allocation of " + std::to_string(n * sizeof(T)) + " bytes failed: " +
-                                          cudaGetErrorString(e));
-    }
-    h->allocs.push_back(*p);
-    h->bytes += n * sizeof(T);
-    return TCE_OK;
-}
-
-template <class T>
-int upload(Handle *h, T **p, const std::vector<T> &v)
-{
-    int s = dalloc(h, p, v.size());
-    if (s) return s;
-    if (!v.empty()) CK(h, cudaMemcpyAsync(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, h->st));
-    return TCE_OK;
 }
 
 void dfree(Handle *h, void *p)
@@ -281,6 +185,8 @@ int run_blocks(Handle *h, const std::vector<int4> &items, const std::vector<int>
     a.blk_off = d_off;
     a.pp_rw = h->d_pp;
     a.max_ncomb = mx;
+    a.max_ncq = h->max_ncq;
+    a.fixed_gmax = h->d_gmax;
     a.num_sms = h->num_sms;
     CKS(h, tce_launch_quartets(h->S, a, h->st));
     if (blocks) {
@@ -369,6 +275,11 @@ int build(Handle *h, const tce_system *sys)
         i += ncomp;
     }
     h->nsh = (int)h->sh_first.size();
+    {
+        int mxn = 1;
+        for (int n : h->sh_n) mxn = std::max(mxn, n);
+        h->max_ncq = mxn * mxn * mxn * mxn;
+    }
     h->nshuc = 0;
     for (int S = 0; S < h->nsh; ++S)
         if (h->sh_first[S] < h->nfuc) ++h->nshuc;
@@ -461,6 +372,10 @@ int build(Handle *h, const tce_system *sys)
                 for (int k = 8 * g; k < 8 * g + 8; ++k) m = std::max(m, h->tnmax[(size_t)d * h->nq + k]);
                 S.gmax[d][g] = m;
             }
+        std::vector<int> gm(3 * TCE_MAXG);
+        for (int d = 0; d < 3; ++d)
+            for (int g = 0; g < TCE_MAXG; ++g) gm[d * TCE_MAXG + g] = S.gmax[d][g];
+        if ((s = upload(h, &h->d_gmax, gm))) return s;
     }
 
     // ---------------- unit pairs + primitive-pair scalars ----------------
@@ -618,7 +533,10 @@ int build(Handle *h, const tce_system *sys)
         }
         if ((s = upload(h, &h->d_items, sorted))) return s;
         h->items_host = std::move(sorted);
+        h->shard_idx.resize(h->items_host.size());
+        std::iota(h->shard_idx.begin(), h->shard_idx.end(), 0LL);
         if ((s = make_lists(h, h->items_host))) return s;
+        if ((s = lg_rebuild_lists(h))) return s;
         // algorithmic work of one J/K pass
         unsigned long long *d_np = nullptr;
         double *d_fl = nullptr;
@@ -654,6 +572,12 @@ int direct_jk_device(Handle *h, const double *dP, double *dJ, double *dK, cudaSt
     CK(h, cudaMemsetAsync(dJ, 0, sizeof(double) * h->nfuc * h->nbas, st));
     CK(h, cudaMemsetAsync(dK, 0, sizeof(double) * h->nfuc * h->nbas, st));
     CK(h, cudaEventRecord(h->ev0, st));
+    if (h->method != TCE_METHOD_FIXED) {
+        int s = lg_jk_passes(h, dP, dJ, dK, st);
+        if (s) return s;
+        CK(h, cudaEventRecord(h->ev1, st));
+        return TCE_OK;
+    }
     for (const auto &w : h->lists) {
         if (w.n == 0) continue;
         if (w.kind == 0) {   // every other class: generic kernel
@@ -667,6 +591,8 @@ int direct_jk_device(Handle *h, const double *dP, double *dJ, double *dK, cudaSt
             a.J = dJ;
             a.K = dK;
             a.max_ncomb = h->max_ncomb;
+            a.max_ncq = h->max_ncq;
+            a.fixed_gmax = h->d_gmax;
             a.num_sms = h->num_sms;
             CKS(h, tce_launch_quartets(h->S, a, st));
         } else {             // register-resident kernels of the dominant classes
@@ -687,7 +613,9 @@ int direct_jk_device(Handle *h, const double *dP, double *dJ, double *dK, cudaSt
     return TCE_OK;
 }
 
-}  // namespace
+}  // namespace tcehost
+
+using namespace tcehost;
 
 // ============================================================================
 // C ABI
@@ -776,9 +704,14 @@ int tce_set_shard(void *handle, int32_t rank, int32_t nranks)
     int s = tce_shard_plan(h->cost_host.data(), (int64_t)owner.size(), nranks, owner.data());
     if (s) return fail(h, s, "shard plan failed");
     std::vector<int4> mine;
+    h->shard_idx.clear();
     for (size_t i = 0; i < owner.size(); ++i)
-        if (owner[i] == rank) mine.push_back(h->items_host[i]);
+        if (owner[i] == rank) {
+            mine.push_back(h->items_host[i]);
+            h->shard_idx.push_back((long long)i);
+        }
     if ((s = make_lists(h, mine))) return s;
+    if ((s = lg_rebuild_lists(h))) return s;
     h->shard_rank = rank;
     h->shard_nranks = nranks;
     CK(h, cudaStreamSynchronize(h->st));
@@ -936,6 +869,8 @@ int tce_shell_block_noalloc(void *handle, const int32_t sh4[4], int32_t mode, do
     a.blk_out = reinterpret_cast<double *>(base + TCE_STATIC_OFF_BLK);
     a.blk_off = reinterpret_cast<const long long *>(base + TCE_STATIC_OFF_BOFF);
     a.max_ncomb = ncomb_of(h, q.x, q.y, q.z, q.w);
+    a.max_ncq = h->max_ncq;
+    a.fixed_gmax = h->d_gmax;
     a.num_sms = h->num_sms;
     CKS(h, tce_launch_quartets(h->S, a, h->st));
     CK(h, cudaMemcpyAsync(blk, base + TCE_STATIC_OFF_BLK, sizeof(double) * nblk, cudaMemcpyDeviceToHost, h->st));
@@ -1008,6 +943,8 @@ int tce_eri_stored(void *handle, int64_t eri_size, double *eri)
         a.eri_size = esz;
         a.physicist = h->physicist;
         a.max_ncomb = h->max_ncomb;
+        a.max_ncq = h->max_ncq;
+        a.fixed_gmax = h->d_gmax;
         a.num_sms = h->num_sms;
         CKS(h, tce_launch_quartets(h->S, a, h->st));
     }

@@ -70,6 +70,17 @@ struct DevSys {
     const double *Q;
 };
 
+// One rule of the learned-grid dictionary: a mapped Gauss-Kronrod rule padded
+// to nq = 32 or 64 nodes (zero weights past nn), its T table [d][n][nq] at
+// T_off and the per-8-node-group truncation orders gmax[d*TCE_MAXG + g].
+struct RuleDev {
+    long long T_off;
+    int node_off;      // nodes / Kronrod / Gauss weights at node_off .. node_off+nq-1
+    int nn;            // real nodes (2n+1 of the Kronrod rule)
+    int nq;            // padded node count: 32 or 64
+    int gmax[3 * TCE_MAXG];
+};
+
 // ---------------------------------------------------------------------------
 // e^{-x} I_0(x): the v = 0 branches of iv_log (bessel_iv_log.f90:43-318):
 //   x > 1400   : mu-series, 3 terms   (method 1)

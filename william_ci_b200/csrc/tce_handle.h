@@ -1,0 +1,153 @@
+// tce_handle.h -- host-side state of one libtce handle and the helpers the
+// host translation units share (error reporting, device allocation).
+#pragma once
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "tce_kernels.h"
+
+namespace tcehost {
+
+constexpr double kPi = 3.14159265358979323846;
+
+struct Handle {
+    std::string err;
+    // system scalars
+    int ndp = 0, nq = 0, ncap = 0, nbas = 0, nfuc = 0, nsh = 0, nshuc = 0, ncell = 1;
+    int ncl[3] = {1, 1, 1};
+    double a[3] = {0, 0, 0}, L[3] = {0, 0, 0};
+    int physicist = 0, sao = 1, prim_screen = 1;
+    double thr = 1e-13, prim_thr = 1e-14;
+    // host copies
+    std::vector<double> ctr, exps, coefs, tnode, tweight;
+    std::vector<int> lxyz, poff;
+    std::vector<int> sh_first, sh_n, sh_l, sh_np, sh_eoff, sh_coff;
+    std::vector<double> sh_r, sh_exp, sh_coef, sh_cmax;
+    std::vector<UnitPair> up;
+    std::vector<double> Q, Qsh;
+    double Qmax = 0.0;
+    std::vector<int> tnmax;
+    // device
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int num_sms = 148;
+    std::vector<void *> allocs;
+    size_t bytes = 0;
+    DevSys S{};
+    PairPrim *d_pp = nullptr;
+    double *d_Qsh = nullptr;
+    int4 *d_items = nullptr;
+    long long nitems = 0;
+    int max_ncomb = 1, max_ncq = 1;
+    int *d_gmax = nullptr;              // [3*TCE_MAXG] of the system's rule
+    long long n_func_q = 0, n_unit_sig = 0, n_prim_q = 0;
+    double jk_flops = 0.0;
+    std::vector<int4> items_host;       // sorted, most expensive first
+    std::vector<double> cost_host;
+    int shard_rank = 0, shard_nranks = 1;
+    // the J/K work of this shard, one list per kernel: kind 0 generic
+    // (k_quartets), 1 all-s (k_quartets_s), 2 one-periodic-direction s/p class
+    // `cls` (k_quartets_r1)
+    struct WorkList { int kind, cls; int4 *d = nullptr; long long n = 0; };
+    std::vector<WorkList> lists;
+    long long nitems_shard = 0;
+    int *d_tnmax = nullptr;
+    unsigned int *d_next = nullptr;
+    double *d_P = nullptr, *d_J = nullptr, *d_K = nullptr;
+    double *d_eri = nullptr;
+    long long eri_elems = 0;
+    int eri_size = 0;
+    double *d_blk = nullptr;
+    long long *d_blkoff = nullptr;
+    int4 *d_one = nullptr;
+    float last_ms = 0.f;
+    // this shard's items (indices into items_host) and their device copy
+    std::vector<long long> shard_idx;
+    int4 *d_shard_items = nullptr;
+    // quadrature method of the J/K pass (TCE_METHOD_*)
+    int method = TCE_METHOD_FIXED;
+    // learned grid: rule dictionary, per-item rules, lists, fallback queue
+    int lg_nrules = 0;
+    std::vector<RuleDev> rules_host;
+    RuleDev *d_rules = nullptr;
+    double *d_rule_T = nullptr, *d_rule_t = nullptr, *d_rule_wk = nullptr, *d_rule_wg = nullptr;
+    std::vector<int> item_rule;          // per items_host entry; lg_nrules = plain directly
+    int4 *d_lg_items[2] = {nullptr, nullptr};   // learned-grid items with 32- / 64-node rules
+    int *d_lg_rule[2] = {nullptr, nullptr};
+    long long n_lg_q[2] = {0, 0};
+    long long n_lg = 0;
+    int4 *d_plain_items = nullptr;
+    long long n_plain_direct = 0;
+    int4 *d_fb_items = nullptr;
+    unsigned int *d_fb_count = nullptr;
+    double judge_tol = 1e-10, plain_tol = 1e-11;
+    int plain_max_panels = 24;
+    double plain_scale = 0.6;
+    double *d_gk = nullptr;              // 15-point Kronrod rule on [0,1]: u[16], wk[16], wg[16]
+    double *d_plain_scratch = nullptr;
+    long long plain_scratch_warps = 0;
+    unsigned long long *d_node_evals = nullptr;
+    unsigned int *d_next2 = nullptr;     // work counter of the second kernel of a pass
+    unsigned int *d_next3 = nullptr;
+};
+
+extern thread_local std::string g_err;
+
+int fail(Handle *h, int code, const std::string &msg);
+
+#define CK(h, call)                                                                          \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            return fail((h), TCE_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define CKS(h, call)                                                  \
+    do {                                                              \
+        int s_ = (call);                                              \
+        if (s_ != TCE_OK) {                                           \
+            cudaError_t e_ = cudaGetLastError();                      \
+            return fail((h), s_, std::string(#call) + " failed" +     \
+                                     (e_ != cudaSuccess ? std::string(": ") + cudaGetErrorString(e_) : "")); \
+        }                                                             \
+    } while (0)
+
+template <class T>
+int dalloc(Handle *h, T **p, size_t n)
+{
+    *p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(h, TCE_ERR_NOMEM, "device allocation of " + std::to_string(n * sizeof(T)) + " bytes failed: " +
+                                          cudaGetErrorString(e));
+    }
+    h->allocs.push_back(*p);
+    h->bytes += n * sizeof(T);
+    return TCE_OK;
+}
+
+template <class T>
+int upload(Handle *h, T **p, const std::vector<T> &v)
+{
+    int s = dalloc(h, p, v.size());
+    if (s) return s;
+    if (!v.empty()) CK(h, cudaMemcpyAsync(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, h->st));
+    return TCE_OK;
+}
+
+void dfree(Handle *h, void *p);
+
+
+// helpers defined in tce_api.cu
+int shift_to(const Handle *h, int idx, int refcell, int nblk);
+int ncomb_of(const Handle *h, int SI, int SJ, int SK, int SL);
+int make_lists(Handle *h, const std::vector<int4> &items);
+int direct_jk_device(Handle *h, const double *dP, double *dJ, double *dK, cudaStream_t st);
+// learned-grid / plain passes of direct_jk_device (tce_lg.cu)
+int lg_jk_passes(Handle *h, const double *dP, double *dJ, double *dK, cudaStream_t st);
+int lg_rebuild_lists(Handle *h);
+
+}  // namespace tcehost

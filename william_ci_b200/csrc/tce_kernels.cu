@@ -9,11 +9,8 @@
 //   k_pair_vectors Fourier pair vectors (pair_vector_cached / fourier_sin_product)
 //   k_enumerate    symmetry-unique shell quartets + Schwarz screen
 //                  (ERI_toroidal.f90:342-401, eri_direct.f90:298-326)
-//   k_quartets     the quartet kernel: ERI_shell_block_toroidal
-//                  (ERI_shell_block_toroidal.f90:28-366) for one shell quartet per
-//                  warp, fused with its consumer (J/K scatter eri_direct.f90:331-357,
-//                  stored-ERI scatter ERI_toroidal.f90:416-454, Schwarz blocks,
-//                  primitive Schwarz table)
+//   (the generic quartet kernels k_quartets / k_plain live in tce_quartets.cu,
+//    the register-resident ones in tce_kernels_s.cu)
 //   k_stored_jk    J/K from stored ERIs (hartree_exchange_potential.f90:157-200)
 //   k_sym_fill     rows i > nfuc by translation (symmetric_matrix.f90:62-131)
 #include "tce_device.cuh"
@@ -267,348 +264,6 @@ __global__ void k_enumerate(DevSys S, const double *Qsh, double Qmax, int4 *item
 // ============================================================================
 // the quartet kernel
 // ============================================================================
-struct QuartetArgs {
-    const int4 *items;       // shell quartets (SI in the unit cell)
-    const int *prim_sel;     // mode PRIMTAB: (p1, p2) per item, else null
-    int nitems;
-    int mode;                // TCE_MODE_*
-    int prim_screen;         // apply the primitive screen (main loops)
-    unsigned int *next;      // dynamic work counter
-    // outputs
-    double *blk_out;         // BLOCK: blocks at blk_off[item]
-    const long long *blk_off;
-    const double *P;         // JK: density (nbas x nbas)
-    double *J, *K;           // JK: nfuc x nbas
-    double *eri;             // STORE
-    int eri_size, physicist;
-    PairPrim *pp_rw;         // PRIMTAB: where ps values go
-    // smem layout (doubles per warp)
-    int bmax;                // primitive quartets per batch
-    int rowcap;              // rows per batch (>= bmax * ncomb * ndp)
-    int cstride;             // power combinations per real direction (largest class)
-    int warp_smem_doubles;
-};
-
-template <int NQ>
-__device__ __forceinline__ void row_dot(const DevSys &S, int d, const double2 *__restrict__ G, int nppb, int ib_,
-                                        const double2 *__restrict__ H, int nppk, int ik_, int nm, double phi,
-                                        double sgn, double *out)
-{
-    constexpr int NG = NQ / 8;
-    const double *__restrict__ T = S.Tt + (size_t)d * (S.ncap + 1) * NQ;
-    double c1, s1;
-    sincos(phi, &s1, &c1);
-#pragma unroll
-    for (int g0 = 0; g0 < NG; g0 += 4) {
-        constexpr int dummy = 0;
-        (void)dummy;
-        double acc[32];
-#pragma unroll
-        for (int x = 0; x < 32; ++x) acc[x] = 0.0;
-        double cn = 1.0, sn = 0.0;
-        int n = 0;
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            if (g0 + s >= NG) break;
-            int nend = S.gmax[d][g0 + s];
-            nend = nend < nm ? nend : nm;
-            for (; n <= nend; ++n) {
-                if (n > 0) {
-                    if ((n & 31) == 0) {
-                        sincos((double)n * phi, &sn, &cn);
-                    } else {
-                        double tmp = cn * c1 - sn * s1;
-                        sn = sn * c1 + cn * s1;
-                        cn = tmp;
-                    }
-                }
-                double2 g = __ldg(G + (size_t)n * nppb + ib_);
-                double2 h = __ldg(H + (size_t)n * nppk + ik_);
-                double ar = g.x * h.x - g.y * h.y, ai = g.x * h.y + g.y * h.x;
-                double F = ar * cn - ai * sn;
-                const double2 *Tn = reinterpret_cast<const double2 *>(T + (size_t)n * NQ + 8 * g0);
-#pragma unroll
-                for (int g = 0; g < 4; ++g) {
-                    if (g >= s && g0 + g < NG) {
-#pragma unroll
-                        for (int kk = 0; kk < 4; ++kk) {
-                            double2 t = __ldg(Tn + 4 * g + kk);
-                            acc[8 * g + 2 * kk] = fma(F, t.x, acc[8 * g + 2 * kk]);
-                            acc[8 * g + 2 * kk + 1] = fma(F, t.y, acc[8 * g + 2 * kk + 1]);
-                        }
-                    }
-                }
-            }
-        }
-#pragma unroll
-        for (int x = 0; x < 32; ++x)
-            if (8 * g0 + x < NQ) out[8 * g0 + x] = acc[x] * sgn;
-    }
-}
-
-// Context of one shell quartet, shared by the phases of the quartet kernel.
-struct QCtx {
-    int SI, SJ, SK, SL, nA, nB, nC, nD, lsA, lsB, lsC, lsD, ncomb, ncq, NN, R;
-    UnitPair Ub, Uk;
-    double Tsh[3];
-};
-
-// Phases 1+2 for a batch of nb primitive quartets (qlist/qfac), accumulating
-// into the shell-quartet block blk (warp-private shared memory).
-template <int NQ>
-__device__ void process_batch(const DevSys &S, const QCtx &Q, int nb, const int2 *qlist, const double *qfac,
-                              double *rows, double *realb, double *blk, int lane, int cstride)
-{
-    constexpr int RS = NQ + 1;
-    const int ndp = S.ndp, nreal = 3 - ndp;
-    const int lsA = Q.lsA, lsB = Q.lsB, lsC = Q.lsC, lsD = Q.lsD, ncomb = Q.ncomb, R = Q.R;
-    const int nppb = Q.Ub.npp, nppk = Q.Uk.npp;
-    // ---------------- phase 1: periodic-direction rows (lane = row) ----------------
-    const int nrows = nb * R;
-    for (int r = lane; r < nrows; r += 32) {
-        int p = r / R, rem = r - p * R;
-        int d = rem / ncomb, cmb = rem - d * ncomb;
-        int ia = cmb % (lsA + 1), t1 = cmb / (lsA + 1);
-        int ib = t1 % (lsB + 1), t2 = t1 / (lsB + 1);
-        int ic = t2 % (lsC + 1), id = t2 / (lsC + 1);
-        int2 pq = qlist[p];
-        const PairPrim &Pb = S.pp[Q.Ub.pp_off + pq.x];
-        const PairPrim &Pk = S.pp[Q.Uk.pp_off + pq.y];
-        const double2 *G = S.vec + Q.Ub.vec_off +
-                           ((((long long)d * (lsA + 1) + ia) * (lsB + 1) + ib) * 2 + 0) * (long long)Q.Ub.Nlen * nppb;
-        const double2 *H = S.vec + Q.Uk.vec_off +
-                           ((((long long)d * (lsC + 1) + ic) * (lsD + 1) + id) * 2 + 1) * (long long)Q.Uk.Nlen * nppk;
-        int nm = Pb.N[d] < Pk.N[d] ? Pb.N[d] : Pk.N[d];
-        double phi = S.a[d] * (Pb.cen[d] - (Pk.cen[d] + Q.Tsh[d]));
-        double sgn = pow(S.a[d], -(double)(ia + ib + ic + id));
-        row_dot<NQ>(S, d, G, nppb, pq.x, H, nppk, pq.y, nm, phi, sgn, rows + (size_t)r * RS);
-    }
-    __syncwarp();
-    // ---------------- phase 2: real directions + contraction (lane = node) ----------------
-    const int npA = S.sh_np[Q.SI], npB = S.sh_np[Q.SJ], npC = S.sh_np[Q.SK], npD = S.sh_np[Q.SL];
-    for (int p = 0; p < nb; ++p) {
-        int2 pq = qlist[p];
-        const PairPrim &Pb = S.pp[Q.Ub.pp_off + pq.x];
-        const PairPrim &Pk = S.pp[Q.Uk.pp_off + pq.y];
-        const double pp_ = Pb.esum, qq = Pk.esum;
-        if (nreal > 0) {
-            const double *Eb = S.ecoef + Q.Ub.e_off + (long long)pq.x * nreal * (lsA + 1) * (lsB + 1) * TCE_ECO;
-            const double *Ek = S.ecoef + Q.Uk.e_off + (long long)pq.y * nreal * (lsC + 1) * (lsD + 1) * TCE_ECO;
-            for (int k = lane; k < NQ; k += 32) {
-                double t = S.tnode[k], t2 = t * t;
-                double D2 = 1.0 / (pp_ * qq + (pp_ + qq) * t2);
-                double w = pp_ * qq * t2 * D2, rs = PI_D * sqrt(D2);
-                for (int dr = 0; dr < nreal; ++dr) {
-                    int d = ndp + dr;
-                    double Rr = Pb.cen[d] - (Pk.cen[d] + Q.Tsh[d]);
-                    double gt[4 * TCE_LMAX + 2];
-                    gt[0] = (Rr == 0.0) ? rs : rs * exp(-w * Rr * Rr);
-                    double gm1 = 0.0, g0 = gt[0];
-                    for (int n = 0; n < Q.NN; ++n) {
-                        double gp1 = 2.0 * w * Rr * g0 - 2.0 * (double)n * w * gm1;
-                        gt[n + 1] = gp1;
-                        gm1 = g0;
-                        g0 = gp1;
-                    }
-                    for (int cmb = 0; cmb < ncomb; ++cmb) {
-                        int ia = cmb % (lsA + 1), u1 = cmb / (lsA + 1);
-                        int ib = u1 % (lsB + 1), u2 = u1 / (lsB + 1);
-                        int ic = u2 % (lsC + 1), id = u2 / (lsC + 1);
-                        const double *eb = Eb + ((dr * (lsA + 1) + ia) * (lsB + 1) + ib) * TCE_ECO;
-                        const double *ek = Ek + ((dr * (lsC + 1) + ic) * (lsD + 1) + id) * TCE_ECO;
-                        double val = 0.0;
-                        for (int n = 0; n <= ia + ib; ++n) {
-                            double sb = (n & 1) ? -eb[n] : eb[n];
-                            for (int kk = 0; kk <= ic + id; ++kk) val += sb * ek[kk] * gt[n + kk];
-                        }
-                        realb[((size_t)dr * cstride + cmb) * RS + k] = val;
-                    }
-                }
-            }
-            __syncwarp();
-        }
-        const double fac = qfac[p];
-        const double *rowp = rows + (size_t)p * R * RS;
-        const int i = pq.x / Q.Ub.np2, j = pq.x % Q.Ub.np2;
-        const int kp = pq.y / Q.Uk.np2, lp = pq.y % Q.Uk.np2;
-        for (int cq = 0; cq < Q.ncq; ++cq) {
-            int ca = cq % Q.nA, r1 = cq / Q.nA;
-            int cb = r1 % Q.nB, r2 = r1 / Q.nB;
-            int cc = r2 % Q.nC, cd = r2 / Q.nC;
-            const int *pa = S.fn_pw + 3 * (S.sh_first[Q.SI] + ca);
-            const int *pb = S.fn_pw + 3 * (S.sh_first[Q.SJ] + cb);
-            const int *pc = S.fn_pw + 3 * (S.sh_first[Q.SK] + cc);
-            const int *pd = S.fn_pw + 3 * (S.sh_first[Q.SL] + cd);
-            int cm[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) cm[d] = pa[d] + (lsA + 1) * (pb[d] + (lsB + 1) * (pc[d] + (lsC + 1) * pd[d]));
-            double v = 0.0;
-            for (int k = lane; k < NQ; k += 32) {
-                double prod = S.tweight[k];
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    double x = (d < ndp) ? rowp[((size_t)d * ncomb + cm[d]) * RS + k]
-                                         : realb[((size_t)(d - ndp) * cstride + cm[d]) * RS + k];
-                    prod *= x;
-                }
-                v += prod;
-            }
-            v = tce_warp_sum(v);
-            if (lane == 0) {
-                double cf = S.sh_coef[S.sh_coff[Q.SI] + ca * npA + i] * S.sh_coef[S.sh_coff[Q.SJ] + cb * npB + j] *
-                            S.sh_coef[S.sh_coff[Q.SK] + cc * npC + kp] * S.sh_coef[S.sh_coff[Q.SL] + cd * npD + lp];
-                blk[cq] += fac * cf * v;
-            }
-        }
-        __syncwarp();
-    }
-}
-
-template <int NQ>
-__global__ void __launch_bounds__(128) k_quartets(DevSys S, QuartetArgs A)
-{
-    extern __shared__ double smem[];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    double *ws = smem + (size_t)wib * A.warp_smem_doubles;
-    constexpr int RS = NQ + 1;
-    const int ndp = S.ndp, nreal = 3 - ndp;
-    // per-warp smem: [qlist qcap][qfac qcap][rows rowcap*RS][real nreal*cstride*RS][blk 1296]
-    const int qcap = A.rowcap;
-    int2 *qlist = reinterpret_cast<int2 *>(ws);
-    double *qfac = ws + qcap;
-    double *rows = ws + 2 * qcap;
-    double *realb = rows + (size_t)A.rowcap * RS;
-    double *blk = realb + (size_t)nreal * A.cstride * RS;
-
-    while (true) {
-        int it = 0;
-        if (lane == 0) it = (int)atomicAdd(A.next, 1u);
-        it = __shfl_sync(0xffffffffu, it, 0);
-        if (it >= A.nitems) break;
-        const int4 q = A.items[it];
-        QCtx Q;
-        Q.SI = q.x; Q.SJ = q.y; Q.SK = q.z; Q.SL = q.w;
-        Q.nA = S.sh_n[Q.SI]; Q.nB = S.sh_n[Q.SJ]; Q.nC = S.sh_n[Q.SK]; Q.nD = S.sh_n[Q.SL];
-        Q.lsA = S.sh_l[Q.SI]; Q.lsB = S.sh_l[Q.SJ]; Q.lsC = S.sh_l[Q.SK]; Q.lsD = S.sh_l[Q.SL];
-        Q.ncomb = (Q.lsA + 1) * (Q.lsB + 1) * (Q.lsC + 1) * (Q.lsD + 1);
-        Q.ncq = Q.nA * Q.nB * Q.nC * Q.nD;
-        Q.NN = Q.lsA + Q.lsB + Q.lsC + Q.lsD;
-        Q.R = Q.ncomb * ndp;
-        // ket: translate (SK,SL) so that SK lies in the unit cell
-        const int cK = Q.SK / S.nshuc;
-        const int SK0 = Q.SK - cK * S.nshuc;
-        const int SLp = tce_shift_to(Q.SL, cK, S.nshuc, S.ncl);
-        Q.Ub = S.up[(long long)Q.SI * S.nsh + Q.SJ];
-        Q.Uk = S.up[(long long)SK0 * S.nsh + SLp];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) Q.Tsh[d] = S.sh_r[3 * Q.SK + d] - S.sh_r[3 * SK0 + d];
-        int B = A.rowcap / Q.R;
-        if (B < 1) B = 1;
-        if (B > qcap) B = qcap;
-
-        for (int c = lane; c < Q.ncq; c += 32) blk[c] = 0.0;
-        __syncwarp();
-
-        const int nppb = Q.Ub.npp, nppk = Q.Uk.npp;
-        const long long total = (long long)nppb * nppk;
-        int want = -1;
-        if (A.mode == TCE_MODE_PRIMTAB) want = A.prim_sel[2 * it] * Q.Ub.np2 + A.prim_sel[2 * it + 1];
-        int nb = 0;
-        for (long long base = 0; base < total; base += 32) {
-            long long idx = base + lane;
-            bool keep = idx < total;
-            int ipb = 0, ipk = 0;
-            double fac = 0.0;
-            if (keep) {
-                ipb = (int)(idx / nppk);
-                ipk = (int)(idx - (long long)ipb * nppk);
-                const PairPrim &Pb = S.pp[Q.Ub.pp_off + ipb];
-                const PairPrim &Pk = S.pp[Q.Uk.pp_off + ipk];
-                fac = S.fac_const * Pb.pfac * Pk.pfac;
-                if (A.mode == TCE_MODE_PRIMTAB) {
-                    keep = (ipb == want) && (ipk == want);
-                } else if (A.mode != TCE_MODE_NOSCREEN) {
-                    // prefactor screens (ERI_shell_block_toroidal.f90:191,216) and the
-                    // primitive Schwarz screen (:217-219)
-                    double bra = fabs(S.fac_const * Pb.pfac) * Pb.cmax12;
-                    if (bra * Q.Uk.ket_max <= 2.22e-16) keep = false;
-                    else if (fabs(fac) * Pb.cmax12 * Pk.cmax12 <= 2.22e-16) keep = false;
-                    else if (A.prim_screen && Pb.ps * Pk.ps < S.prim_thr) keep = false;
-                }
-            }
-            const unsigned msk = __ballot_sync(0xffffffffu, keep);
-            const int pos = __popc(msk & ((1u << lane) - 1u));
-            const int cnt = __popc(msk);
-            int done = 0;
-            while (done < cnt) {
-                int take = B - nb;
-                if (take > cnt - done) take = cnt - done;
-                if (keep && pos >= done && pos < done + take) {
-                    qlist[nb + pos - done] = make_int2(ipb, ipk);
-                    qfac[nb + pos - done] = fac;
-                }
-                nb += take;
-                done += take;
-                __syncwarp();
-                if (nb == B) {
-                    process_batch<NQ>(S, Q, nb, qlist, qfac, rows, realb, blk, lane, A.cstride);
-                    nb = 0;
-                    __syncwarp();
-                }
-            }
-        }
-        if (nb > 0) process_batch<NQ>(S, Q, nb, qlist, qfac, rows, realb, blk, lane, A.cstride);
-        __syncwarp();
-
-        // ---------------- phase 3: the consumer of the block ----------------
-        const int nA = Q.nA, nB = Q.nB, nC = Q.nC, nD = Q.nD;
-        if (A.mode == TCE_MODE_BLOCK || A.mode == TCE_MODE_NOSCREEN) {
-            double *o = A.blk_out + A.blk_off[it];
-            for (int c = lane; c < Q.ncq; c += 32) o[c] = blk[c];
-        } else if (A.mode == TCE_MODE_PRIMTAB) {
-            if (lane == 0) {
-                double m = 0.0;
-                for (int a = 0; a < nA; ++a)
-                    for (int b = 0; b < nB; ++b) {
-                        double v = sqrt(fabs(blk[a + nA * (b + nB * (a + nA * b))]));
-                        if (v > m) m = v;
-                    }
-                A.pp_rw[Q.Ub.pp_off + want].ps = m;
-            }
-        } else {
-            const int fI = S.sh_first[Q.SI], fJ = S.sh_first[Q.SJ], fK = S.sh_first[Q.SK], fL = S.sh_first[Q.SL];
-            for (int cq = lane; cq < Q.ncq; cq += 32) {
-                int ca = cq % nA, r1 = cq / nA;
-                int cb = r1 % nB, r2 = r1 / nB;
-                int cc = r2 % nC, cd = r2 / nC;
-                int f[4] = {fI + ca, fJ + cb, fK + cc, fL + cd};
-                if (S.Q[f[0] + (long long)S.nbas * f[1]] * S.Q[f[2] + (long long)S.nbas * f[3]] < S.thr) continue;
-                const double val = blk[cq];
-                if (A.mode == TCE_MODE_STORE) {
-                    const int perm[8][4] = {{0,1,2,3},{1,0,2,3},{0,1,3,2},{1,0,3,2},{2,3,0,1},{3,2,0,1},{2,3,1,0},{3,2,1,0}};
-                    for (int ip = 0; ip < 8; ++ip) {
-                        int g[4];
-#pragma unroll
-                        for (int ii = 0; ii < 4; ++ii) g[ii] = f[perm[ip][ii]];
-                        int ref = g[0] / S.nfuc;
-#pragma unroll
-                        for (int ii = 0; ii < 4; ++ii) g[ii] = tce_shift_to(g[ii], ref, S.nfuc, S.ncl);
-                        long long e;
-                        if (A.physicist)
-                            e = g[0] + (long long)A.eri_size * (g[2] + (long long)S.nbas * (g[1] + (long long)S.nbas * g[3]));
-                        else
-                            e = g[0] + (long long)A.eri_size * (g[1] + (long long)S.nbas * (g[2] + (long long)S.nbas * g[3]));
-                        A.eri[e] = val;
-                    }
-                    continue;
-                }
-                tce_scatter_jk(S, A.P, A.J, A.K, f, val, fI, nA, fJ, nB, fK, nC, fL, nD);
-            }
-        }
-        __syncwarp();
-    }
-}
-
 // ============================================================================
 // algorithmic work of one J/K pass, counted from the reference algorithm's
 // operation counts per executed primitive quartet (ERI_shell_block_toroidal.f90):
@@ -782,88 +437,6 @@ __global__ void k_sym_fill(int nf, int fpuc, int nx, int ny, int nz, double *eri
 // ============================================================================
 // launch wrappers (host)
 // ============================================================================
-int tce_launch_quartets(const DevSys &S, const QuartetHostArgs &h, cudaStream_t st)
-{
-    QuartetArgs A;
-    A.items = h.items;
-    A.prim_sel = h.prim_sel;
-    A.nitems = h.nitems;
-    A.mode = h.mode;
-    A.prim_screen = h.prim_screen;
-    A.next = h.next;
-    A.blk_out = h.blk_out;
-    A.blk_off = h.blk_off;
-    A.P = h.P;
-    A.J = h.J;
-    A.K = h.K;
-    A.eri = h.eri;
-    A.eri_size = h.eri_size;
-    A.physicist = h.physicist;
-    A.pp_rw = h.pp_rw;
-    // batch sizing from the largest class present (rows of 32 lanes at least)
-    int R = h.max_ncomb * S.ndp;
-    int rowcap = R > 32 ? R : 32;
-    int bmax = rowcap;
-    const int RS = S.nq + 1;
-    int nreal = 3 - S.ndp;
-    long long wdoubles = 2LL * rowcap + (long long)rowcap * RS + (long long)nreal * h.max_ncomb * RS + 1296 + 8;
-    wdoubles = (wdoubles + 31) / 32 * 32;
-    A.bmax = bmax;
-    A.rowcap = rowcap;
-    A.cstride = h.max_ncomb;
-    A.warp_smem_doubles = (int)wdoubles;
-    size_t wbytes = (size_t)wdoubles * sizeof(double);
-    int warps = 4;
-    while (warps > 1 && wbytes * warps > 220 * 1024) --warps;
-    if (wbytes > 220 * 1024) return TCE_ERR_UNSUPPORTED;
-    size_t smem = wbytes * warps;
-    cudaMemsetAsync(h.next, 0, sizeof(unsigned int), st);
-    int nsm = h.num_sms > 0 ? h.num_sms : 148;
-    cudaError_t e;
-    switch (S.nq) {
-    case 32:
-        cudaFuncSetAttribute(k_quartets<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        {
-            int per = 0;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_quartets<32>, 32 * warps, smem);
-            if (per < 1) per = 1;
-            k_quartets<32><<<nsm * per, 32 * warps, smem, st>>>(S, A);
-        }
-        break;
-    case 40:
-        cudaFuncSetAttribute(k_quartets<40>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        {
-            int per = 0;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_quartets<40>, 32 * warps, smem);
-            if (per < 1) per = 1;
-            k_quartets<40><<<nsm * per, 32 * warps, smem, st>>>(S, A);
-        }
-        break;
-    case 64:
-        cudaFuncSetAttribute(k_quartets<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        {
-            int per = 0;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_quartets<64>, 32 * warps, smem);
-            if (per < 1) per = 1;
-            k_quartets<64><<<nsm * per, 32 * warps, smem, st>>>(S, A);
-        }
-        break;
-    case 128:
-        cudaFuncSetAttribute(k_quartets<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        {
-            int per = 0;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_quartets<128>, 32 * warps, smem);
-            if (per < 1) per = 1;
-            k_quartets<128><<<nsm * per, 32 * warps, smem, st>>>(S, A);
-        }
-        break;
-    default:
-        return TCE_ERR_UNSUPPORTED;
-    }
-    e = cudaGetLastError();
-    return e == cudaSuccess ? TCE_OK : TCE_ERR_CUDA;
-}
-
 int tce_launch_t_tables(int nq, int ndp, int ncap, const double *tnode, const double *a, double *tb, int *tnmax,
                         double *Tt, cudaStream_t st)
 {

@@ -4,21 +4,28 @@
 #include "tce_device.cuh"
 #include "../../include/tce.h"
 
-// consumers of a shell-quartet block (k_quartets)
+// consumers of a shell-quartet block (k_quartets, k_plain)
 #define TCE_MODE_BLOCK    0   // prefactor screens, block written out (Schwarz pass)
 #define TCE_MODE_NOSCREEN 1   // no screens, block written out (ps_noscreen)
 #define TCE_MODE_PRIMTAB  2   // single primitive pair, no screens -> PairPrim::ps
 #define TCE_MODE_JK       3   // fused J/K scatter (direct_JK)
 #define TCE_MODE_STORE    4   // stored-ERI scatter (ERI_integral_toroidal)
 
+// t-quadrature of the generic path: TCE_METHOD_* of tce.h (FIXED: the system's
+// rule or one dictionary rule, rule_override; LEARNED: per-item dictionary rule
+// + Kronrod/Gauss judge, rejects queued; PLAIN: adaptive 15/7 bisection, k_plain)
+
 struct QuartetHostArgs {
     const int4 *items = nullptr;
     const int *prim_sel = nullptr;
     int nitems = 0;
+    const unsigned int *nitems_dev = nullptr;   // item count read on the device (fallback lists)
     int mode = TCE_MODE_BLOCK;
+    int method = TCE_METHOD_FIXED;
     int prim_screen = 0;
     unsigned int *next = nullptr;
     double *blk_out = nullptr;
+    double *blk_out2 = nullptr;      // judge estimate of each block (dictionary rule override)
     const long long *blk_off = nullptr;
     const double *P = nullptr;
     double *J = nullptr, *K = nullptr;
@@ -26,9 +33,29 @@ struct QuartetHostArgs {
     int eri_size = 0, physicist = 0;
     PairPrim *pp_rw = nullptr;
     int max_ncomb = 1;   // largest (lA+1)(lB+1)(lC+1)(lD+1) among the items
+    int max_ncq = 1296;  // largest block (components) among the items
     int num_sms = 148;
+    const int *fixed_gmax = nullptr;   // [3*TCE_MAXG] of the system's rule
+    // learned grid
+    const RuleDev *rules = nullptr;
+    const double *rule_T = nullptr, *rule_t = nullptr, *rule_wk = nullptr, *rule_wg = nullptr;
+    const int *item_rule = nullptr;
+    int rule_override = -1;
+    int dict_nq = 32;                // padded node count of the dictionary rules in use (32 or 64)
+    double judge_tol = 1e-10;
+    int4 *fb_items = nullptr;        // capacity >= nitems
+    int *fb_index = nullptr;
+    unsigned int *fb_count = nullptr;
+    // plain
+    double *scratch = nullptr;       // scratch_warps x tce_plain_scratch_per_warp doubles
+    long long scratch_warps = 0;
+    double plain_tol = 1e-11, plain_scale = 0.6;
+    int plain_max_panels = 24;
+    const double *gk_u = nullptr, *gk_wk = nullptr, *gk_wg = nullptr;   // 15 nodes on [0,1]
+    unsigned long long *node_evals = nullptr;
 };
 
+long long tce_plain_scratch_per_warp(const DevSys &S, int max_ncq);
 int tce_launch_quartets(const DevSys &S, const QuartetHostArgs &h, cudaStream_t st);
 
 // all-s shell quartets, J/K mode (k_quartets_s)

@@ -1,0 +1,1032 @@
+// tce_lg.cu -- learned-grid quadrature: rule dictionary, per-quartet features,
+// the small MLP that picks a rule per quartet (trained on the device by the
+// forward/backward/Adam kernels below), the judge-and-fallback J/K passes and
+// the plain adaptive method.  No counterpart in the reference: its t-integral
+// uses one fixed rule per run (fast_quad or the 64/128 tables,
+// precompute_t.f90:5-14, 906-942).
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <random>
+
+#include "tce_handle.h"
+
+using namespace tcehost;
+
+
+// ============================================================================
+// device kernels
+// ============================================================================
+// Per-item features (one thread per shell quartet):
+//  0,1 log min/max e_sum of the bra primitive pairs; 2,3 the same for the ket;
+//  4 log rho of the most diffuse pairs (rho = p q / (p + q));
+//  5 log(2 / a_min^2), the Bessel-argument scale of the lattice;
+//  6 log1p(rho * chord^2) over the periodic directions (chord^2 = 2(1 - cos a D)/a^2);
+//  7 log1p(rho * D^2) over the real directions;
+//  8 total angular momentum; 9 log10 of the shell-pair Schwarz product;
+//  10 periodic directions; 11 log(1 + largest bra truncation order).
+__global__ void k_item_features(DevSys S, const int4 *items, long long n, const double *Qsh, float *F)
+{
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int4 q = items[i];
+    const int cK = q.z / S.nshuc, SK0 = q.z - cK * S.nshuc;
+    const int SLp = tce_shift_to(q.w, cK, S.nshuc, S.ncl);
+    const UnitPair Ub = S.up[(long long)q.x * S.nsh + q.y];
+    const UnitPair Uk = S.up[(long long)SK0 * S.nsh + SLp];
+    double pmin = 1e300, pmax = 0.0, qmin = 1e300, qmax = 0.0;
+    long long ib = 0, ik = 0;
+    int Nb = 0;
+    for (int x = 0; x < Ub.npp; ++x) {
+        const PairPrim &P = S.pp[Ub.pp_off + x];
+        if (P.esum < pmin) { pmin = P.esum; ib = x; }
+        pmax = fmax(pmax, P.esum);
+        for (int d = 0; d < S.ndp; ++d) Nb = max(Nb, P.N[d]);
+    }
+    for (int x = 0; x < Uk.npp; ++x) {
+        const PairPrim &P = S.pp[Uk.pp_off + x];
+        if (P.esum < qmin) { qmin = P.esum; ik = x; }
+        qmax = fmax(qmax, P.esum);
+    }
+    const PairPrim &Pb = S.pp[Ub.pp_off + ib];
+    const PairPrim &Pk = S.pp[Uk.pp_off + ik];
+    const double rho = pmin * qmin / (pmin + qmin);
+    double chord = 0.0, real2 = 0.0, amin = 1e300;
+    for (int d = 0; d < 3; ++d) {
+        const double tsh = S.sh_r[3 * q.z + d] - S.sh_r[3 * SK0 + d];
+        const double D = Pb.cen[d] - (Pk.cen[d] + tsh);
+        if (d < S.ndp) {
+            chord += 2.0 * (1.0 - cos(S.a[d] * D)) / (S.a[d] * S.a[d]);
+            amin = fmin(amin, S.a[d]);
+        } else {
+            real2 += D * D;
+        }
+    }
+    const double qq = Qsh[q.x + (long long)S.nsh * q.y] * Qsh[q.z + (long long)S.nsh * q.w];
+    float *f = F + i * TCE_NFEAT;
+    f[0] = (float)log(pmin);
+    f[1] = (float)log(pmax);
+    f[2] = (float)log(qmin);
+    f[3] = (float)log(qmax);
+    f[4] = (float)log(rho);
+    f[5] = (float)log(2.0 / (amin * amin));
+    f[6] = (float)log1p(rho * chord);
+    f[7] = (float)log1p(rho * real2);
+    f[8] = (float)(S.sh_l[q.x] + S.sh_l[q.y] + S.sh_l[q.z] + S.sh_l[q.w]);
+    f[9] = (float)log10(qq + 1e-300);
+    f[10] = (float)S.ndp;
+    f[11] = (float)log(1.0 + Nb);
+}
+
+// ---------------------------------------------------------------------------
+// MLP: nf -> nh (ReLU) -> nh (ReLU) -> nc, FP32.  Parameters flat:
+// W1[nh][nf] b1[nh] W2[nh][nh] b2[nh] W3[nc][nh] b3[nc].
+// ---------------------------------------------------------------------------
+__global__ void k_norm_rows(const float *Xraw, const int *perm, int B, int nf, const float *mu, const float *sig,
+                            float *X)
+{
+    int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= B * nf) return;
+    int r = id / nf, c = id % nf;
+    long long src = perm ? perm[r] : r;
+    X[id] = (Xraw[src * nf + c] - mu[c]) / sig[c];
+}
+
+__global__ void k_dense_fwd(const float *X, int B, int in, const float *W, const float *b, int out, float *Y, int relu)
+{
+    int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= B * out) return;
+    int r = id / out, o = id % out;
+    const float *x = X + (size_t)r * in, *w = W + (size_t)o * in;
+    float acc = b[o];
+    for (int i = 0; i < in; ++i) acc = fmaf(x[i], w[i], acc);
+    Y[id] = (relu && acc < 0.f) ? 0.f : acc;
+}
+
+// per-output sigmoid cross-entropy against targets Y in [0,1]:
+// row loss sum_c [max(z,0) - z y + log(1 + e^{-|z|})], dZ = (sigmoid(z) - y) / B
+__global__ void k_sigmoid_bce(const float *Z, const float *Y, const int *perm, int B, int C, float *dZ, float *lrow)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= B) return;
+    const float *z = Z + (size_t)r * C;
+    const float *y = Y + (size_t)(perm ? perm[r] : r) * C;
+    float L = 0.f;
+    for (int c = 0; c < C; ++c) {
+        const float zc = z[c];
+        L += fmaxf(zc, 0.f) - zc * y[c] + log1pf(expf(-fabsf(zc)));
+        if (dZ) dZ[(size_t)r * C + c] = (1.f / (1.f + expf(-zc)) - y[c]) / (float)B;
+    }
+    lrow[r] = L;
+}
+
+// dX = dY W, masked by the ReLU of the layer input (Xact > 0)
+__global__ void k_dense_bwd_dx(const float *dY, int B, int out, const float *W, int in, const float *Xact, float *dX)
+{
+    int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= B * in) return;
+    int r = id / in, i = id % in;
+    float acc = 0.f;
+    for (int o = 0; o < out; ++o) acc = fmaf(dY[(size_t)r * out + o], W[(size_t)o * in + i], acc);
+    dX[id] = Xact[id] > 0.f ? acc : 0.f;
+}
+
+// dW[o][i] = sum_r dY[r][o] X[r][i]; db[o] = sum_r dY[r][o] (thread (o, i), i == in: bias)
+__global__ void k_dense_bwd_dw(const float *dY, const float *X, int B, int in, int out, float *dW, float *db)
+{
+    int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= out * (in + 1)) return;
+    int o = id / (in + 1), i = id % (in + 1);
+    float acc = 0.f;
+    if (i < in)
+        for (int r = 0; r < B; ++r) acc = fmaf(dY[(size_t)r * out + o], X[(size_t)r * in + i], acc);
+    else
+        for (int r = 0; r < B; ++r) acc += dY[(size_t)r * out + o];
+    if (i < in) dW[(size_t)o * in + i] = acc;
+    else db[o] = acc;
+}
+
+__global__ void k_adam(float *p, const float *g, float *m, float *v, long long n, float lr, float b1, float b2, float eps,
+                       float bc1, float bc2)
+{
+    long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= n) return;
+    float gi = g[id];
+    float mi = b1 * m[id] + (1.f - b1) * gi;
+    float vi = b2 * v[id] + (1.f - b2) * gi * gi;
+    m[id] = mi;
+    v[id] = vi;
+    p[id] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+}
+
+// single-block sum of n floats (deterministic order)
+__global__ void k_sum(const float *x, int n, float *out)
+{
+    __shared__ float sh[256];
+    float acc = 0.f;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) acc += x[i];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = sh[0];
+}
+
+__global__ void k_sigmoid(const float *Z, long long n, float *P)
+{
+    long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id < n) P[id] = 1.f / (1.f + expf(-Z[id]));
+}
+
+// Work of a dictionary rule for a quartet whose Bessel orders stop at nmax:
+// 8 nodes x (orders used) summed over node groups and periodic directions.
+__device__ __forceinline__ double rule_cost(const RuleDev &R, int ndp, int nmax)
+{
+    double c = 0.0;
+    for (int d = 0; d < ndp; ++d)
+        for (int g = 0; g < R.nq / 8; ++g) {
+            const int m = R.gmax[d * TCE_MAXG + g];
+            if (m >= 0) c += 8.0 * ((m < nmax ? m : nmax) + 1);
+        }
+    return c;
+}
+
+// Rule of least expected cost per quartet: cost_r + (1 - p_r) C_plain, with
+// p_r = sigmoid(z_r) the network's probability that rule r is accepted and
+// correct, and C_plain = plain_factor x the dearest rule's cost; nrules (the
+// plain method directly) when no rule is expected to be cheaper than it.
+__global__ void k_choose_rule(const float *Z, long long n, int nrules, const float *F, const RuleDev *rules, int ndp,
+                              double plain_factor, int *rule)
+{
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int nmax = (int)lrint(expm1((double)F[i * TCE_NFEAT + 11]));
+    double cmax = 0.0;
+    for (int r = 0; r < nrules; ++r) cmax = fmax(cmax, rule_cost(rules[r], ndp, nmax));
+    const double cplain = plain_factor * cmax;
+    double best = cplain;
+    int br = nrules;
+    const float *z = Z + i * nrules;
+    for (int r = 0; r < nrules; ++r) {
+        const double p = 1.0 / (1.0 + exp(-(double)z[r]));
+        const double e = rule_cost(rules[r], ndp, nmax) + (1.0 - p) * cplain;
+        if (e < best) {
+            best = e;
+            br = r;
+        }
+    }
+    rule[i] = br;
+}
+
+static inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// ============================================================================
+// MLP host object
+// ============================================================================
+namespace {
+
+struct Mlp {
+    int nf = 0, nh = 0, nc = 0;
+    long long np = 0;
+    std::string err;
+    cudaStream_t st = nullptr;
+    float *d_p = nullptr, *d_g = nullptr, *d_m = nullptr, *d_v = nullptr;
+    float *d_mu = nullptr, *d_sig = nullptr;
+    long long step = 0;
+    int cap = 0;   // rows the batch buffers hold
+    float *d_X = nullptr, *d_h1 = nullptr, *d_h2 = nullptr, *d_z = nullptr, *d_dz = nullptr, *d_dh2 = nullptr,
+          *d_dh1 = nullptr, *d_lrow = nullptr, *d_loss = nullptr;
+    std::vector<void *> allocs;
+    long long off_W1() const { return 0; }
+    long long off_b1() const { return (long long)nh * nf; }
+    long long off_W2() const { return off_b1() + nh; }
+    long long off_b2() const { return off_W2() + (long long)nh * nh; }
+    long long off_W3() const { return off_b2() + nh; }
+    long long off_b3() const { return off_W3() + (long long)nc * nh; }
+};
+
+thread_local std::string g_mlp_err;
+
+int mfail(Mlp *m, int code, const std::string &msg)
+{
+    if (m) m->err = msg;
+    g_mlp_err = msg;
+    return code;
+}
+
+#define MCK(m, call)                                                                            \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess) return mfail((m), TCE_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <class T>
+int malloc_m(Mlp *m, T **p, size_t n)
+{
+    *p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return mfail(m, TCE_ERR_NOMEM, "MLP device allocation failed");
+    }
+    m->allocs.push_back(*p);
+    return TCE_OK;
+}
+
+void mfree(Mlp *m, void *p)
+{
+    if (!p) return;
+    cudaFree(p);
+    auto it = std::find(m->allocs.begin(), m->allocs.end(), p);
+    if (it != m->allocs.end()) m->allocs.erase(it);
+}
+
+int ensure_cap(Mlp *m, int B)
+{
+    if (B <= m->cap) return TCE_OK;
+    float **bufs[] = {&m->d_X, &m->d_h1, &m->d_h2, &m->d_z, &m->d_dz, &m->d_dh2, &m->d_dh1, &m->d_lrow};
+    for (float **b : bufs) mfree(m, *b);
+    int s;
+    const int w = std::max(std::max(m->nf, m->nh), m->nc);
+    if ((s = malloc_m(m, &m->d_X, (size_t)B * m->nf))) return s;
+    if ((s = malloc_m(m, &m->d_h1, (size_t)B * m->nh))) return s;
+    if ((s = malloc_m(m, &m->d_h2, (size_t)B * m->nh))) return s;
+    if ((s = malloc_m(m, &m->d_z, (size_t)B * m->nc))) return s;
+    if ((s = malloc_m(m, &m->d_dz, (size_t)B * m->nc))) return s;
+    if ((s = malloc_m(m, &m->d_dh2, (size_t)B * w))) return s;
+    if ((s = malloc_m(m, &m->d_dh1, (size_t)B * w))) return s;
+    if ((s = malloc_m(m, &m->d_lrow, (size_t)B))) return s;
+    m->cap = B;
+    return TCE_OK;
+}
+
+// forward over B rows already normalised in d_X; logits in d_z
+void forward(Mlp *m, int B)
+{
+    const float *p = m->d_p;
+    const int T = 256;
+    k_dense_fwd<<<nblk((long long)B * m->nh, T), T, 0, m->st>>>(m->d_X, B, m->nf, p + m->off_W1(), p + m->off_b1(),
+                                                                   m->nh, m->d_h1, 1);
+    k_dense_fwd<<<nblk((long long)B * m->nh, T), T, 0, m->st>>>(m->d_h1, B, m->nh, p + m->off_W2(), p + m->off_b2(),
+                                                                   m->nh, m->d_h2, 1);
+    k_dense_fwd<<<nblk((long long)B * m->nc, T), T, 0, m->st>>>(m->d_h2, B, m->nh, p + m->off_W3(), p + m->off_b3(),
+                                                                   m->nc, m->d_z, 0);
+}
+
+// loss rows + gradients into d_g (target rows indexed through perm when given)
+void backward(Mlp *m, int B, const float *d_Y, const int *d_perm)
+{
+    const float *p = m->d_p;
+    float *g = m->d_g;
+    const int T = 256;
+    k_sigmoid_bce<<<nblk(B, T), T, 0, m->st>>>(m->d_z, d_Y, d_perm, B, m->nc, m->d_dz, m->d_lrow);
+    k_dense_bwd_dw<<<nblk((long long)m->nc * (m->nh + 1), T), T, 0, m->st>>>(m->d_dz, m->d_h2, B, m->nh, m->nc,
+                                                                               g + m->off_W3(), g + m->off_b3());
+    k_dense_bwd_dx<<<nblk((long long)B * m->nh, T), T, 0, m->st>>>(m->d_dz, B, m->nc, p + m->off_W3(), m->nh, m->d_h2,
+                                                                     m->d_dh2);
+    k_dense_bwd_dw<<<nblk((long long)m->nh * (m->nh + 1), T), T, 0, m->st>>>(m->d_dh2, m->d_h1, B, m->nh, m->nh,
+                                                                               g + m->off_W2(), g + m->off_b2());
+    k_dense_bwd_dx<<<nblk((long long)B * m->nh, T), T, 0, m->st>>>(m->d_dh2, B, m->nh, p + m->off_W2(), m->nh,
+                                                                     m->d_h1, m->d_dh1);
+    k_dense_bwd_dw<<<nblk((long long)m->nh * (m->nf + 1), T), T, 0, m->st>>>(m->d_dh1, m->d_X, B, m->nf, m->nh,
+                                                                               g + m->off_W1(), g + m->off_b1());
+}
+
+}  // namespace
+
+// ============================================================================
+// learned-grid passes and lists (host side of the handle)
+// ============================================================================
+namespace tcehost {
+
+static int ensure_plain(Handle *h)
+{
+    if (!h->d_gk) return fail(h, TCE_ERR_STATE, "plain method needs tce_set_plain_rule first");
+    int s;
+    if (!h->d_node_evals && (s = dalloc(h, &h->d_node_evals, 1))) return s;
+    if (!h->d_next2 && (s = dalloc(h, &h->d_next2, 1))) return s;
+    if (!h->d_next3 && (s = dalloc(h, &h->d_next3, 1))) return s;
+    if (!h->d_plain_scratch) {
+        const long long warps = (long long)h->num_sms * 16;
+        const long long per = tce_plain_scratch_per_warp(h->S, h->max_ncq);
+        if ((s = dalloc(h, &h->d_plain_scratch, (size_t)(warps * per)))) return s;
+        h->plain_scratch_warps = warps;
+    }
+    return TCE_OK;
+}
+
+static void fill_common(Handle *h, QuartetHostArgs &a)
+{
+    a.max_ncomb = h->max_ncomb;
+    a.max_ncq = h->max_ncq;
+    a.fixed_gmax = h->d_gmax;
+    a.num_sms = h->num_sms;
+    a.rules = h->d_rules;
+    a.rule_T = h->d_rule_T;
+    a.rule_t = h->d_rule_t;
+    a.rule_wk = h->d_rule_wk;
+    a.rule_wg = h->d_rule_wg;
+    a.judge_tol = h->judge_tol;
+    a.scratch = h->d_plain_scratch;
+    a.scratch_warps = h->plain_scratch_warps;
+    a.plain_tol = h->plain_tol;
+    a.plain_scale = h->plain_scale;
+    a.plain_max_panels = h->plain_max_panels;
+    if (h->d_gk) {
+        a.gk_u = h->d_gk;
+        a.gk_wk = h->d_gk + 16;
+        a.gk_wg = h->d_gk + 32;
+    }
+    a.node_evals = h->d_node_evals;
+    a.pp_rw = h->d_pp;
+}
+
+int lg_rebuild_lists(Handle *h)
+{
+    int s;
+    dfree(h, h->d_shard_items);
+    h->d_shard_items = nullptr;
+    std::vector<int4> mine;
+    mine.reserve(h->shard_idx.size());
+    for (long long i : h->shard_idx) mine.push_back(h->items_host[(size_t)i]);
+    if ((s = upload(h, &h->d_shard_items, mine))) return s;
+    for (int c = 0; c < 2; ++c) {
+        dfree(h, h->d_lg_items[c]);
+        dfree(h, h->d_lg_rule[c]);
+        h->d_lg_items[c] = nullptr;
+        h->d_lg_rule[c] = nullptr;
+        h->n_lg_q[c] = 0;
+    }
+    dfree(h, h->d_plain_items);
+    dfree(h, h->d_fb_items);
+    h->d_plain_items = h->d_fb_items = nullptr;
+    h->n_lg = h->n_plain_direct = 0;
+    if (h->item_rule.size() != h->items_host.size() || h->lg_nrules == 0) return TCE_OK;
+    std::vector<int4> lg[2], pl;
+    std::vector<int> rl[2];
+    for (long long i : h->shard_idx) {
+        const int r = h->item_rule[(size_t)i];
+        if (r >= 0 && r < h->lg_nrules) {
+            const int c = h->rules_host[r].nq == 32 ? 0 : 1;
+            lg[c].push_back(h->items_host[(size_t)i]);
+            rl[c].push_back(r);
+        } else {
+            pl.push_back(h->items_host[(size_t)i]);
+        }
+    }
+    for (int c = 0; c < 2; ++c) {
+        if ((s = upload(h, &h->d_lg_items[c], lg[c]))) return s;
+        if ((s = upload(h, &h->d_lg_rule[c], rl[c]))) return s;
+        h->n_lg_q[c] = (long long)lg[c].size();
+    }
+    h->n_lg = h->n_lg_q[0] + h->n_lg_q[1];
+    if ((s = upload(h, &h->d_plain_items, pl))) return s;
+    if ((s = dalloc(h, &h->d_fb_items, (size_t)std::max<long long>(h->n_lg, 1)))) return s;
+    if (!h->d_fb_count && (s = dalloc(h, &h->d_fb_count, 1))) return s;
+    h->n_plain_direct = (long long)pl.size();
+    CK(h, cudaStreamSynchronize(h->st));
+    return TCE_OK;
+}
+
+int lg_jk_passes(Handle *h, const double *dP, double *dJ, double *dK, cudaStream_t st)
+{
+    int s;
+    if ((s = ensure_plain(h))) return s;
+    CK(h, cudaMemsetAsync(h->d_node_evals, 0, sizeof(unsigned long long), st));
+    QuartetHostArgs a;
+    fill_common(h, a);
+    a.mode = TCE_MODE_JK;
+    a.prim_screen = h->prim_screen;
+    a.P = dP;
+    a.J = dJ;
+    a.K = dK;
+    if (h->method == TCE_METHOD_PLAIN) {
+        const long long n = (long long)h->shard_idx.size();
+        if (n == 0) return TCE_OK;
+        a.method = TCE_METHOD_PLAIN;
+        a.items = h->d_shard_items;
+        a.nitems = (int)n;
+        a.next = h->d_next;
+        CKS(h, tce_launch_quartets(h->S, a, st));
+        return TCE_OK;
+    }
+    if (!h->d_rules || h->item_rule.size() != h->items_host.size())
+        return fail(h, TCE_ERR_STATE, "learned grid needs rules and per-item rules");
+    CK(h, cudaMemsetAsync(h->d_fb_count, 0, sizeof(unsigned int), st));
+    for (int c = 0; c < 2; ++c) {
+        if (h->n_lg_q[c] == 0) continue;
+        QuartetHostArgs b = a;
+        b.method = TCE_METHOD_LEARNED;
+        b.dict_nq = c == 0 ? 32 : 64;
+        b.items = h->d_lg_items[c];
+        b.nitems = (int)h->n_lg_q[c];
+        b.item_rule = h->d_lg_rule[c];
+        b.fb_items = h->d_fb_items;
+        b.fb_count = h->d_fb_count;
+        b.next = h->d_next;
+        CKS(h, tce_launch_quartets(h->S, b, st));
+    }
+    if (h->n_plain_direct > 0) {
+        QuartetHostArgs b = a;
+        b.method = TCE_METHOD_PLAIN;
+        b.items = h->d_plain_items;
+        b.nitems = (int)h->n_plain_direct;
+        b.next = h->d_next2;
+        CKS(h, tce_launch_quartets(h->S, b, st));
+    }
+    if (h->n_lg > 0) {   // the judge's rejects, count read on the device
+        QuartetHostArgs b = a;
+        b.method = TCE_METHOD_PLAIN;
+        b.items = h->d_fb_items;
+        b.nitems = (int)h->n_lg;
+        b.nitems_dev = h->d_fb_count;
+        b.next = h->d_next3;
+        CKS(h, tce_launch_quartets(h->S, b, st));
+    }
+    return TCE_OK;
+}
+
+}  // namespace tcehost
+
+namespace {
+
+// items given by the caller (any cell): translate S1 to the unit cell
+int translate_items(Handle *h, int64_t n, const int32_t *items, std::vector<int4> &out)
+{
+    out.resize((size_t)n);
+    for (int64_t i = 0; i < n; ++i) {
+        const int32_t *q = items + 4 * i;
+        for (int k = 0; k < 4; ++k)
+            if (q[k] < 0 || q[k] >= h->nsh) return fail(h, TCE_ERR_ARG, "shell index out of range");
+        const int c1 = q[0] / h->nshuc;
+        out[(size_t)i] = make_int4(shift_to(h, q[0], c1, h->nshuc), shift_to(h, q[1], c1, h->nshuc),
+                                   shift_to(h, q[2], c1, h->nshuc), shift_to(h, q[3], c1, h->nshuc));
+    }
+    return TCE_OK;
+}
+
+}  // namespace
+
+// ============================================================================
+// C ABI
+// ============================================================================
+extern "C" {
+
+int tce_items(void *handle, int32_t *items)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !items) return fail(h, TCE_ERR_ARG, "NULL argument");
+    for (size_t i = 0; i < h->items_host.size(); ++i) {
+        const int4 &q = h->items_host[i];
+        items[4 * i] = q.x;
+        items[4 * i + 1] = q.y;
+        items[4 * i + 2] = q.z;
+        items[4 * i + 3] = q.w;
+    }
+    return TCE_OK;
+}
+
+int tce_item_features(void *handle, int64_t n, const int32_t *items, float *feat)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !feat || n < 0) return fail(h, TCE_ERR_ARG, "bad argument");
+    if (n == 0) return TCE_OK;
+    int s;
+    int4 *d_it = nullptr;
+    bool own = false;
+    if (items) {
+        std::vector<int4> v;
+        if ((s = translate_items(h, n, items, v))) return s;
+        if ((s = upload(h, &d_it, v))) return s;
+        own = true;
+    } else {
+        if (n != (int64_t)h->items_host.size()) return fail(h, TCE_ERR_ARG, "n must equal the engine's item count");
+        d_it = h->d_items;
+    }
+    float *d_f = nullptr;
+    if ((s = dalloc(h, &d_f, (size_t)n * TCE_NFEAT))) return s;
+    k_item_features<<<nblk(n, 128), 128, 0, h->st>>>(h->S, d_it, n, h->d_Qsh, d_f);
+    CK(h, cudaGetLastError());
+    CK(h, cudaMemcpyAsync(feat, d_f, sizeof(float) * n * TCE_NFEAT, cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    if (own) dfree(h, d_it);
+    dfree(h, d_f);
+    return TCE_OK;
+}
+
+int tce_lg_set_rules(void *handle, int32_t nrules, const int32_t *nn, const double *t, const double *wk,
+                     const double *wg)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || nrules < 1 || !nn || !t || !wk || !wg) return fail(h, TCE_ERR_ARG, "bad argument");
+    for (int r = 0; r < nrules; ++r)
+        if (nn[r] < 1 || nn[r] > 64) return fail(h, TCE_ERR_ARG, "a rule has 1..64 nodes");
+    int s;
+    for (void *p : {(void *)h->d_rules, (void *)h->d_rule_T, (void *)h->d_rule_t, (void *)h->d_rule_wk,
+                    (void *)h->d_rule_wg})
+        dfree(h, p);
+    h->d_rules = nullptr;
+    h->d_rule_T = h->d_rule_t = h->d_rule_wk = h->d_rule_wg = nullptr;
+    h->lg_nrules = 0;
+    // rule r: nodes at 64 r (padded to nq_r = 32 or 64), T table of (ncap+1) nq_r ndp doubles
+    std::vector<double> tt((size_t)nrules * 64, 0.0), ww((size_t)nrules * 64, 0.0), gg((size_t)nrules * 64, 0.0);
+    h->rules_host.assign(nrules, RuleDev{});
+    long long Ttot = 0;
+    for (int r = 0; r < nrules; ++r) {
+        RuleDev &R = h->rules_host[r];
+        R.nn = nn[r];
+        R.nq = nn[r] <= 32 ? 32 : 64;
+        R.node_off = 64 * r;
+        R.T_off = Ttot;
+        Ttot += (long long)(h->ncap + 1) * R.nq * h->ndp;
+        for (int k = 0; k < nn[r]; ++k) {
+            tt[(size_t)r * 64 + k] = t[(size_t)r * 64 + k];
+            ww[(size_t)r * 64 + k] = wk[(size_t)r * 64 + k];
+            gg[(size_t)r * 64 + k] = wg[(size_t)r * 64 + k];
+        }
+    }
+    if ((s = upload(h, &h->d_rule_t, tt))) return s;
+    if ((s = upload(h, &h->d_rule_wk, ww))) return s;
+    if ((s = upload(h, &h->d_rule_wg, gg))) return s;
+    if ((s = dalloc(h, &h->d_rule_T, (size_t)Ttot))) return s;
+    double *tb = nullptr;
+    int *tn = nullptr;
+    if ((s = dalloc(h, &tb, (size_t)(h->ncap + 1) * 64 * h->ndp))) return s;
+    if ((s = dalloc(h, &tn, (size_t)64 * h->ndp))) return s;
+    std::vector<int> tnmax((size_t)64 * h->ndp);
+    for (int r = 0; r < nrules; ++r) {
+        RuleDev &R = h->rules_host[r];
+        CKS(h, tce_launch_t_tables(R.nq, h->ndp, h->ncap, h->d_rule_t + R.node_off, h->a, tb, tn,
+                                   h->d_rule_T + R.T_off, h->st));
+        CK(h, cudaMemcpyAsync(tnmax.data(), tn, sizeof(int) * R.nq * h->ndp, cudaMemcpyDeviceToHost, h->st));
+        CK(h, cudaStreamSynchronize(h->st));
+        for (int i = 0; i < 3 * TCE_MAXG; ++i) R.gmax[i] = -1;
+        for (int d = 0; d < h->ndp; ++d)
+            for (int g = 0; g < R.nq / 8; ++g) {
+                int m = -1;
+                for (int k = 8 * g; k < 8 * g + 8; ++k)
+                    if (k < nn[r]) m = std::max(m, tnmax[(size_t)d * R.nq + k]);
+                R.gmax[d * TCE_MAXG + g] = m;
+            }
+    }
+    dfree(h, tb);
+    dfree(h, tn);
+    if ((s = upload(h, &h->d_rules, h->rules_host))) return s;
+    h->lg_nrules = nrules;
+    CK(h, cudaStreamSynchronize(h->st));
+    return lg_rebuild_lists(h);
+}
+
+int tce_lg_rule_gmax(void *handle, int32_t *gmax)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !gmax) return fail(h, TCE_ERR_ARG, "NULL argument");
+    if (h->lg_nrules == 0) return fail(h, TCE_ERR_STATE, "no rule dictionary");
+    for (int r = 0; r < h->lg_nrules; ++r)
+        for (int i = 0; i < 3 * TCE_MAXG; ++i) gmax[(size_t)r * 3 * TCE_MAXG + i] = h->rules_host[r].gmax[i];
+    return TCE_OK;
+}
+
+int tce_set_plain_rule(void *handle, int32_t n, const double *u, const double *wk, const double *wg, double scale)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !u || !wk || !wg) return fail(h, TCE_ERR_ARG, "NULL argument");
+    if (n != 15) return fail(h, TCE_ERR_UNSUPPORTED, "the plain method uses the 15-point Kronrod rule");
+    if (!(scale > 0)) return fail(h, TCE_ERR_ARG, "scale must be positive");
+    std::vector<double> g(48, 0.0);
+    for (int k = 0; k < 15; ++k) {
+        g[k] = u[k];
+        g[16 + k] = wk[k];
+        g[32 + k] = wg[k];
+    }
+    dfree(h, h->d_gk);
+    int s = upload(h, &h->d_gk, g);
+    if (s) return s;
+    h->plain_scale = scale;
+    CK(h, cudaStreamSynchronize(h->st));
+    return TCE_OK;
+}
+
+int tce_lg_set_item_rules(void *handle, const int32_t *rule)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !rule) return fail(h, TCE_ERR_ARG, "NULL argument");
+    if (h->lg_nrules == 0) return fail(h, TCE_ERR_STATE, "no rule dictionary");
+    h->item_rule.assign(rule, rule + h->items_host.size());
+    for (int &r : h->item_rule)
+        if (r < 0 || r > h->lg_nrules) return fail(h, TCE_ERR_ARG, "rule index out of range");
+    return lg_rebuild_lists(h);
+}
+
+int tce_set_method(void *handle, int32_t method)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h) return fail(h, TCE_ERR_ARG, "NULL handle");
+    if (method < TCE_METHOD_FIXED || method > TCE_METHOD_PLAIN) return fail(h, TCE_ERR_ARG, "method must be 0, 1 or 2");
+    if (method != TCE_METHOD_FIXED) {
+        int s = ensure_plain(h);
+        if (s) return s;
+    }
+    if (method == TCE_METHOD_LEARNED && (h->lg_nrules == 0 || h->item_rule.size() != h->items_host.size()))
+        return fail(h, TCE_ERR_STATE, "learned grid needs tce_lg_set_rules and per-item rules");
+    h->method = method;
+    return TCE_OK;
+}
+
+int tce_set_tolerances(void *handle, double judge_tol, double plain_tol, int32_t plain_max_panels)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h) return fail(h, TCE_ERR_ARG, "NULL handle");
+    if (!(judge_tol > 0) || !(plain_tol > 0) || plain_max_panels < 1 || plain_max_panels > 24)
+        return fail(h, TCE_ERR_ARG, "tolerances must be positive, panels 1..24");
+    h->judge_tol = judge_tol;
+    h->plain_tol = plain_tol;
+    h->plain_max_panels = plain_max_panels;
+    return TCE_OK;
+}
+
+int tce_lg_stats(void *handle, int64_t *stats)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !stats) return fail(h, TCE_ERR_ARG, "NULL argument");
+    unsigned int fb = 0;
+    unsigned long long ev = 0;
+    if (h->d_fb_count) CK(h, cudaMemcpyAsync(&fb, h->d_fb_count, sizeof fb, cudaMemcpyDeviceToHost, h->st));
+    if (h->d_node_evals) CK(h, cudaMemcpyAsync(&ev, h->d_node_evals, sizeof ev, cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    stats[0] = h->n_lg;
+    stats[1] = fb;
+    stats[2] = h->n_plain_direct;
+    stats[3] = (int64_t)ev;
+    return TCE_OK;
+}
+
+int tce_rule_blocks(void *handle, int32_t rule, int32_t mode, int64_t n, const int32_t *items, double *K, double *G)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !items || !K || n < 0) return fail(h, TCE_ERR_ARG, "bad argument");
+    if (mode < 0 || mode > 2) return fail(h, TCE_ERR_ARG, "mode must be 0, 1 or 2");
+    if (mode == 1 && !h->prim_screen) return fail(h, TCE_ERR_STATE, "mode 1 needs prim_screen");
+    if (rule < -2 || rule >= h->lg_nrules) return fail(h, TCE_ERR_ARG, "rule out of range");
+    if (n == 0) return TCE_OK;
+    int s;
+    if (rule == -2 && (s = ensure_plain(h))) return s;
+    std::vector<int4> v;
+    if ((s = translate_items(h, n, items, v))) return s;
+    std::vector<long long> off(v.size() + 1, 0);
+    for (size_t i = 0; i < v.size(); ++i)
+        off[i + 1] = off[i] + (long long)h->sh_n[v[i].x] * h->sh_n[v[i].y] * h->sh_n[v[i].z] * h->sh_n[v[i].w];
+    int4 *d_it = nullptr;
+    long long *d_off = nullptr;
+    double *d_K = nullptr, *d_G = nullptr;
+    if ((s = upload(h, &d_it, v))) return s;
+    if ((s = upload(h, &d_off, off))) return s;
+    if ((s = dalloc(h, &d_K, (size_t)off.back()))) return s;
+    if (rule >= 0 && G && (s = dalloc(h, &d_G, (size_t)off.back()))) return s;
+    QuartetHostArgs a;
+    fill_common(h, a);
+    a.items = d_it;
+    a.nitems = (int)n;
+    a.mode = mode == 2 ? TCE_MODE_NOSCREEN : TCE_MODE_BLOCK;
+    a.prim_screen = mode == 1;
+    a.next = h->d_next;
+    a.blk_out = d_K;
+    a.blk_out2 = d_G;
+    a.blk_off = d_off;
+    if (rule >= 0) {
+        a.rule_override = rule;
+        a.dict_nq = h->rules_host[rule].nq;
+    }
+    if (rule == -2) a.method = TCE_METHOD_PLAIN;
+    CKS(h, tce_launch_quartets(h->S, a, h->st));
+    CK(h, cudaMemcpyAsync(K, d_K, sizeof(double) * off.back(), cudaMemcpyDeviceToHost, h->st));
+    if (d_G) CK(h, cudaMemcpyAsync(G, d_G, sizeof(double) * off.back(), cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    dfree(h, d_it);
+    dfree(h, d_off);
+    dfree(h, d_K);
+    dfree(h, d_G);
+    return TCE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// MLP
+// ---------------------------------------------------------------------------
+const char *tce_mlp_last_error(void *mlp)
+{
+    if (mlp) return static_cast<Mlp *>(mlp)->err.c_str();
+    return g_mlp_err.c_str();
+}
+
+int tce_mlp_create(int32_t nf, int32_t nh, int32_t nc, uint64_t seed, void **out)
+{
+    if (!out || nf < 1 || nh < 1 || nc < 2) return mfail(nullptr, TCE_ERR_ARG, "bad MLP shape");
+    *out = nullptr;
+    Mlp *m = new Mlp();
+    m->nf = nf;
+    m->nh = nh;
+    m->nc = nc;
+    m->np = m->off_b3() + nc;
+    int s = 0;
+    if (cudaStreamCreateWithFlags(&m->st, cudaStreamNonBlocking) != cudaSuccess) s = TCE_ERR_CUDA;
+    if (!s) s = malloc_m(m, &m->d_p, m->np);
+    if (!s) s = malloc_m(m, &m->d_g, m->np);
+    if (!s) s = malloc_m(m, &m->d_m, m->np);
+    if (!s) s = malloc_m(m, &m->d_v, m->np);
+    if (!s) s = malloc_m(m, &m->d_mu, nf);
+    if (!s) s = malloc_m(m, &m->d_sig, nf);
+    if (!s) s = malloc_m(m, &m->d_loss, 1);
+    if (s) {
+        g_mlp_err = m->err.empty() ? "MLP create failed" : m->err;
+        for (void *p : m->allocs) cudaFree(p);
+        if (m->st) cudaStreamDestroy(m->st);
+        delete m;
+        return s;
+    }
+    // He-uniform weights, zero biases (seeded)
+    std::mt19937_64 rng(seed);
+    std::vector<float> p((size_t)m->np, 0.f);
+    auto fill = [&](long long off, int rows, int cols) {
+        const double lim = std::sqrt(6.0 / cols);
+        std::uniform_real_distribution<double> U(-lim, lim);
+        for (long long i = 0; i < (long long)rows * cols; ++i) p[(size_t)(off + i)] = (float)U(rng);
+    };
+    fill(m->off_W1(), nh, nf);
+    fill(m->off_W2(), nh, nh);
+    fill(m->off_W3(), nc, nh);
+    std::vector<float> mu(nf, 0.f), sg(nf, 1.f);
+    cudaMemcpyAsync(m->d_p, p.data(), sizeof(float) * m->np, cudaMemcpyHostToDevice, m->st);
+    cudaMemsetAsync(m->d_m, 0, sizeof(float) * m->np, m->st);
+    cudaMemsetAsync(m->d_v, 0, sizeof(float) * m->np, m->st);
+    cudaMemcpyAsync(m->d_mu, mu.data(), sizeof(float) * nf, cudaMemcpyHostToDevice, m->st);
+    cudaMemcpyAsync(m->d_sig, sg.data(), sizeof(float) * nf, cudaMemcpyHostToDevice, m->st);
+    if (cudaStreamSynchronize(m->st) != cudaSuccess) {
+        g_mlp_err = "MLP initialisation failed";
+        for (void *q : m->allocs) cudaFree(q);
+        cudaStreamDestroy(m->st);
+        delete m;
+        return TCE_ERR_CUDA;
+    }
+    *out = m;
+    return TCE_OK;
+}
+
+int tce_mlp_destroy(void *mlp)
+{
+    Mlp *m = static_cast<Mlp *>(mlp);
+    if (!m) return TCE_OK;
+    cudaStreamSynchronize(m->st);
+    for (void *p : m->allocs) cudaFree(p);
+    cudaStreamDestroy(m->st);
+    delete m;
+    return TCE_OK;
+}
+
+int tce_mlp_nparams(void *mlp, int64_t *np)
+{
+    Mlp *m = static_cast<Mlp *>(mlp);
+    if (!m || !np) return mfail(m, TCE_ERR_ARG, "NULL argument");
+    *np = m->np;
+    return TCE_OK;
+}
+
+int tce_mlp_get_params(void *mlp, float *p, float *mu, float *sig)
+{
+    Mlp *m = static_cast<Mlp *>(mlp);
+    if (!m) return mfail(m, TCE_ERR_ARG, "NULL argument");
+    if (p) MCK(m, cudaMemcpyAsync(p, m->d_p, sizeof(float) * m->np, cudaMemcpyDeviceToHost, m->st));
+    if (mu) MCK(m, cudaMemcpyAsync(mu, m->d_mu, sizeof(float) * m->nf, cudaMemcpyDeviceToHost, m->st));
+    if (sig) MCK(m, cudaMemcpyAsync(sig, m->d_sig, sizeof(float) * m->nf, cudaMemcpyDeviceToHost, m->st));
+    MCK(m, cudaStreamSynchronize(m->st));
+    return TCE_OK;
+}
+
+int tce_mlp_set_params(void *mlp, const float *p, const float *mu, const float *sig)
+{
+    Mlp *m = static_cast<Mlp *>(mlp);
+    if (!m) return mfail(m, TCE_ERR_ARG, "NULL argument");
+    if (sig)
+        for (int c = 0; c < m->nf; ++c)
+            if (!(sig[c] > 0.f)) return mfail(m, TCE_ERR_ARG, "feature scales must be positive");
+    if (p) MCK(m, cudaMemcpyAsync(m->d_p, p, sizeof(float) * m->np, cudaMemcpyHostToDevice, m->st));
+    if (mu) MCK(m, cudaMemcpyAsync(m->d_mu, mu, sizeof(float) * m->nf, cudaMemcpyHostToDevice, m->st));
+    if (sig) MCK(m, cudaMemcpyAsync(m->d_sig, sig, sizeof(float) * m->nf, cudaMemcpyHostToDevice, m->st));
+    MCK(m, cudaStreamSynchronize(m->st));
+    return TCE_OK;
+}
+
+// mean over rows of the summed sigmoid cross-entropy, and its gradient w.r.t.
+// the flat parameters
+int tce_mlp_loss_grad(void *mlp, int64_t n, const float *X, const float *Y, float *loss, float *grad)
+{
+    Mlp *m = static_cast<Mlp *>(mlp);
+    if (!m || !X || !Y || !loss || n < 1 || n > (1 << 24)) return mfail(m, TCE_ERR_ARG, "bad argument");
+    int s;
+    if ((s = ensure_cap(m, (int)n))) return s;
+    float *d_raw = nullptr, *d_Y = nullptr;
+    if ((s = malloc_m(m, &d_raw, (size_t)n * m->nf))) return s;
+    if ((s = malloc_m(m, &d_Y, (size_t)n * m->nc))) return s;
+    MCK(m, cudaMemcpyAsync(d_raw, X, sizeof(float) * n * m->nf, cudaMemcpyHostToDevice, m->st));
+    MCK(m, cudaMemcpyAsync(d_Y, Y, sizeof(float) * n * m->nc, cudaMemcpyHostToDevice, m->st));
+    k_norm_rows<<<nblk(n * m->nf, 256), 256, 0, m->st>>>(d_raw, nullptr, (int)n, m->nf, m->d_mu, m->d_sig, m->d_X);
+    forward(m, (int)n);
+    backward(m, (int)n, d_Y, nullptr);
+    k_sum<<<1, 256, 0, m->st>>>(m->d_lrow, (int)n, m->d_loss);
+    MCK(m, cudaGetLastError());
+    float L = 0.f;
+    MCK(m, cudaMemcpyAsync(&L, m->d_loss, sizeof(float), cudaMemcpyDeviceToHost, m->st));
+    if (grad) MCK(m, cudaMemcpyAsync(grad, m->d_g, sizeof(float) * m->np, cudaMemcpyDeviceToHost, m->st));
+    MCK(m, cudaStreamSynchronize(m->st));
+    *loss = L / (float)n;
+    mfree(m, d_raw);
+    mfree(m, d_Y);
+    return TCE_OK;
+}
+
+// Adam on mini-batches of a shuffled copy of (X, Y); the feature scaling is
+// set from X first (mean, standard deviation floored at 1e-3).
+int tce_mlp_train(void *mlp, int64_t n, const float *X, const float *Y, int32_t epochs, int32_t batch, float lr,
+                  uint64_t seed, float *final_loss)
+{
+    Mlp *m = static_cast<Mlp *>(mlp);
+    if (!m || !X || !Y || n < 1 || n > (1 << 24) || epochs < 0 || batch < 1 || !(lr > 0.f))
+        return mfail(m, TCE_ERR_ARG, "bad argument");
+    std::vector<float> mu(m->nf, 0.f), sg(m->nf, 0.f);
+    for (int c = 0; c < m->nf; ++c) {
+        double s1 = 0, s2 = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            double v = X[i * m->nf + c];
+            s1 += v;
+            s2 += v * v;
+        }
+        double mean = s1 / n, var = std::max(0.0, s2 / n - mean * mean);
+        mu[c] = (float)mean;
+        sg[c] = (float)std::max(std::sqrt(var), 1e-3);
+    }
+    int s;
+    if ((s = tce_mlp_set_params(m, nullptr, mu.data(), sg.data()))) return s;
+    const int B = (int)std::min<int64_t>(batch, n);
+    if ((s = ensure_cap(m, (int)std::max<int64_t>(B, std::min<int64_t>(n, 65536))))) return s;
+    float *d_raw = nullptr, *d_Y = nullptr;
+    int *d_perm = nullptr;
+    if ((s = malloc_m(m, &d_raw, (size_t)n * m->nf))) return s;
+    if ((s = malloc_m(m, &d_Y, (size_t)n * m->nc))) return s;
+    if ((s = malloc_m(m, &d_perm, (size_t)n))) return s;
+    MCK(m, cudaMemcpyAsync(d_raw, X, sizeof(float) * n * m->nf, cudaMemcpyHostToDevice, m->st));
+    MCK(m, cudaMemcpyAsync(d_Y, Y, sizeof(float) * n * m->nc, cudaMemcpyHostToDevice, m->st));
+    std::vector<int> perm((size_t)n);
+    std::iota(perm.begin(), perm.end(), 0);
+    std::mt19937_64 rng(seed);
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    for (int ep = 0; ep < epochs; ++ep) {
+        std::shuffle(perm.begin(), perm.end(), rng);
+        MCK(m, cudaMemcpyAsync(d_perm, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, m->st));
+        // the copy source must stay valid until it completes
+        MCK(m, cudaStreamSynchronize(m->st));
+        for (int64_t b0 = 0; b0 + B <= n; b0 += B) {
+            k_norm_rows<<<nblk((long long)B * m->nf, 256), 256, 0, m->st>>>(d_raw, d_perm + b0, B, m->nf, m->d_mu,
+                                                                             m->d_sig, m->d_X);
+            forward(m, B);
+            backward(m, B, d_Y, d_perm + b0);
+            ++m->step;
+            const float bc1 = 1.f - std::pow(b1, (float)m->step), bc2 = 1.f - std::pow(b2, (float)m->step);
+            k_adam<<<nblk(m->np, 256), 256, 0, m->st>>>(m->d_p, m->d_g, m->d_m, m->d_v, m->np, lr, b1, b2, eps, bc1,
+                                                        bc2);
+        }
+        MCK(m, cudaGetLastError());
+    }
+    MCK(m, cudaStreamSynchronize(m->st));
+    mfree(m, d_raw);
+    mfree(m, d_Y);
+    mfree(m, d_perm);
+    if (final_loss) {
+        s = tce_mlp_loss_grad(m, n, X, Y, final_loss, nullptr);
+        if (s) return s;
+    }
+    return TCE_OK;
+}
+
+// logits of n rows (raw features on the device) into d_z-sized chunks of Z
+static int mlp_logits_dev(Mlp *m, long long n, const float *d_raw, float *d_Z)
+{
+    const int CH = 65536;
+    int s;
+    if ((s = ensure_cap(m, (int)std::min<long long>(n, CH)))) return s;
+    for (long long r0 = 0; r0 < n; r0 += CH) {
+        const int B = (int)std::min<long long>(CH, n - r0);
+        k_norm_rows<<<nblk((long long)B * m->nf, 256), 256, 0, m->st>>>(d_raw + r0 * m->nf, nullptr, B, m->nf,
+                                                                         m->d_mu, m->d_sig, m->d_X);
+        forward(m, B);
+        MCK(m, cudaMemcpyAsync(d_Z + r0 * m->nc, m->d_z, sizeof(float) * B * m->nc, cudaMemcpyDeviceToDevice, m->st));
+    }
+    MCK(m, cudaGetLastError());
+    return TCE_OK;
+}
+
+int tce_mlp_predict(void *mlp, int64_t n, const float *X, float *prob)
+{
+    Mlp *m = static_cast<Mlp *>(mlp);
+    if (!m || !X || !prob || n < 0) return mfail(m, TCE_ERR_ARG, "bad argument");
+    if (n == 0) return TCE_OK;
+    float *d_raw = nullptr, *d_Z = nullptr;
+    int s;
+    if ((s = malloc_m(m, &d_raw, (size_t)n * m->nf))) return s;
+    if ((s = malloc_m(m, &d_Z, (size_t)n * m->nc))) return s;
+    MCK(m, cudaMemcpyAsync(d_raw, X, sizeof(float) * n * m->nf, cudaMemcpyHostToDevice, m->st));
+    if ((s = mlp_logits_dev(m, n, d_raw, d_Z))) return s;
+    k_sigmoid<<<nblk(n * m->nc, 256), 256, 0, m->st>>>(d_Z, n * m->nc, d_Z);
+    MCK(m, cudaMemcpyAsync(prob, d_Z, sizeof(float) * n * m->nc, cudaMemcpyDeviceToHost, m->st));
+    MCK(m, cudaStreamSynchronize(m->st));
+    mfree(m, d_raw);
+    mfree(m, d_Z);
+    return TCE_OK;
+}
+
+// Rules of every engine item from the network, on the device: features,
+// forward pass, least-expected-cost choice (k_choose_rule); then the
+// learned-grid lists are rebuilt.
+int tce_lg_predict_rules(void *handle, void *mlp, double plain_factor)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    Mlp *m = static_cast<Mlp *>(mlp);
+    if (!h || !m) return fail(h, TCE_ERR_ARG, "NULL argument");
+    if (!(plain_factor > 0)) return fail(h, TCE_ERR_ARG, "plain_factor must be positive");
+    if (h->lg_nrules == 0) return fail(h, TCE_ERR_STATE, "no rule dictionary");
+    if (m->nf != TCE_NFEAT || m->nc != h->lg_nrules)
+        return fail(h, TCE_ERR_ARG, "network shape does not match the features / rule dictionary");
+    const long long n = (long long)h->items_host.size();
+    if (n == 0) return TCE_OK;
+    int s;
+    float *d_f = nullptr, *d_Z = nullptr;
+    int *d_c = nullptr;
+    if ((s = dalloc(h, &d_f, (size_t)n * TCE_NFEAT))) return s;
+    if ((s = dalloc(h, &d_Z, (size_t)n * m->nc))) return s;
+    if ((s = dalloc(h, &d_c, (size_t)n))) return s;
+    k_item_features<<<nblk(n, 128), 128, 0, h->st>>>(h->S, h->d_items, n, h->d_Qsh, d_f);
+    CK(h, cudaGetLastError());
+    CK(h, cudaStreamSynchronize(h->st));
+    if ((s = mlp_logits_dev(m, n, d_f, d_Z))) return fail(h, s, "network forward: " + m->err);
+    k_choose_rule<<<nblk(n, 128), 128, 0, m->st>>>(d_Z, n, h->lg_nrules, d_f, h->d_rules, h->ndp, plain_factor, d_c);
+    CK(h, cudaGetLastError());
+    h->item_rule.resize((size_t)n);
+    CK(h, cudaMemcpyAsync(h->item_rule.data(), d_c, sizeof(int) * n, cudaMemcpyDeviceToHost, m->st));
+    CK(h, cudaStreamSynchronize(m->st));
+    dfree(h, d_f);
+    dfree(h, d_Z);
+    dfree(h, d_c);
+    return lg_rebuild_lists(h);
+}
+
+int tce_lg_item_rules(void *handle, int32_t *rule)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !rule) return fail(h, TCE_ERR_ARG, "NULL argument");
+    if (h->item_rule.size() != h->items_host.size()) return fail(h, TCE_ERR_STATE, "no per-item rules");
+    std::memcpy(rule, h->item_rule.data(), sizeof(int) * h->item_rule.size());
+    return TCE_OK;
+}
+
+}  // extern "C"

@@ -36,7 +36,17 @@ TCE_OK, TCE_ERR_ARG, TCE_ERR_UNSUPPORTED, TCE_ERR_CUDA, TCE_ERR_STATE, TCE_ERR_N
 EXPORTS = ["tce_create", "tce_destroy", "tce_last_error", "tce_get_info", "tce_shell_block", "tce_shells",
            "tce_schwarz", "tce_eri_stored", "tce_stored_jk", "tce_hartree_exchange", "tce_direct_jk",
            "tce_direct_jk_device", "tce_last_kernel_ms", "tce_set_shard", "tce_shard_plan", "tce_fp64_peak",
-           "tce_shell_block_noalloc", "tce_version"]
+           "tce_shell_block_noalloc", "tce_version",
+           "tce_items", "tce_item_features", "tce_lg_set_rules", "tce_lg_rule_gmax", "tce_set_plain_rule",
+           "tce_lg_set_item_rules", "tce_lg_item_rules", "tce_set_method", "tce_set_tolerances", "tce_lg_stats",
+           "tce_rule_blocks", "tce_mlp_create", "tce_mlp_destroy", "tce_mlp_last_error", "tce_mlp_nparams",
+           "tce_mlp_get_params", "tce_mlp_set_params", "tce_mlp_loss_grad", "tce_mlp_train", "tce_mlp_predict",
+           "tce_lg_predict_rules"]
+
+TCE_METHOD_FIXED, TCE_METHOD_LEARNED, TCE_METHOD_PLAIN = 0, 1, 2
+TCE_NFEAT = 12
+_fp = C.POINTER(C.c_float)
+_lp = C.POINTER(C.c_int64)
 
 
 class TCEError(RuntimeError):
@@ -90,6 +100,29 @@ def lib():
         L.tce_shard_plan.argtypes = [_dp, C.c_int64, C.c_int32, _ip]
         L.tce_fp64_peak.argtypes = [_dp]
         L.tce_version.restype = C.c_char_p
+        L.tce_items.argtypes = [C.c_void_p, _ip]
+        L.tce_item_features.argtypes = [C.c_void_p, C.c_int64, _ip, _fp]
+        L.tce_lg_set_rules.argtypes = [C.c_void_p, C.c_int32, _ip, _dp, _dp, _dp]
+        L.tce_lg_rule_gmax.argtypes = [C.c_void_p, _ip]
+        L.tce_set_plain_rule.argtypes = [C.c_void_p, C.c_int32, _dp, _dp, _dp, C.c_double]
+        L.tce_lg_set_item_rules.argtypes = [C.c_void_p, _ip]
+        L.tce_lg_item_rules.argtypes = [C.c_void_p, _ip]
+        L.tce_set_method.argtypes = [C.c_void_p, C.c_int32]
+        L.tce_set_tolerances.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int32]
+        L.tce_lg_stats.argtypes = [C.c_void_p, _lp]
+        L.tce_rule_blocks.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int64, _ip, _dp, _dp]
+        L.tce_mlp_create.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.POINTER(C.c_void_p)]
+        L.tce_mlp_destroy.argtypes = [C.c_void_p]
+        L.tce_mlp_last_error.restype = C.c_char_p
+        L.tce_mlp_last_error.argtypes = [C.c_void_p]
+        L.tce_mlp_nparams.argtypes = [C.c_void_p, _lp]
+        L.tce_mlp_get_params.argtypes = [C.c_void_p, _fp, _fp, _fp]
+        L.tce_mlp_set_params.argtypes = [C.c_void_p, _fp, _fp, _fp]
+        L.tce_mlp_loss_grad.argtypes = [C.c_void_p, C.c_int64, _fp, _fp, _fp, _fp]
+        L.tce_mlp_train.argtypes = [C.c_void_p, C.c_int64, _fp, _fp, C.c_int32, C.c_int32, C.c_float, C.c_uint64,
+                                    _fp]
+        L.tce_mlp_predict.argtypes = [C.c_void_p, C.c_int64, _fp, _fp]
+        L.tce_lg_predict_rules.argtypes = [C.c_void_p, C.c_void_p, C.c_double]
         _lib = L
     return _lib
 
@@ -240,6 +273,88 @@ class Engine:
         K = np.zeros(n * n)
         _check(lib().tce_stored_jk(self.h, _d(Pf), _d(J), _d(K)), self.h)
         return J.reshape(n, n, order="F"), K.reshape(n, n, order="F")
+
+
+    # ---------------- learned grid / plain method ----------------
+    def items(self) -> np.ndarray:
+        """The engine's unique shell quartets (most expensive first), shape (n, 4)."""
+        n = self.info()["n_shell_quartets"]
+        it = np.zeros(4 * n, dtype=np.int32)
+        if n:
+            _check(lib().tce_items(self.h, _i(it)), self.h)
+        return it.reshape(n, 4)
+
+    def item_features(self, items: Optional[np.ndarray] = None) -> np.ndarray:
+        if items is None:
+            n = self.info()["n_shell_quartets"]
+            ptr = None
+        else:
+            items = np.ascontiguousarray(items, dtype=np.int32).reshape(-1, 4)
+            n = len(items)
+            ptr = _i(items)
+        F = np.zeros(n * TCE_NFEAT, dtype=np.float32)
+        if n:
+            _check(lib().tce_item_features(self.h, n, ptr, F.ctypes.data_as(_fp)), self.h)
+        return F.reshape(n, TCE_NFEAT)
+
+    def lg_set_rules(self, rules):
+        """rules: list of (t, wk, wg) arrays of at most 64 nodes each."""
+        R = len(rules)
+        nn = np.array([len(r[0]) for r in rules], dtype=np.int32)
+        t = np.zeros((R, 64))
+        wk = np.zeros((R, 64))
+        wg = np.zeros((R, 64))
+        for r, (tt, kk, gg) in enumerate(rules):
+            t[r, :len(tt)], wk[r, :len(tt)], wg[r, :len(tt)] = tt, kk, gg
+        _check(lib().tce_lg_set_rules(self.h, R, _i(nn), _d(t), _d(wk), _d(wg)), self.h)
+        self.nrules = R
+
+    def lg_rule_gmax(self) -> np.ndarray:
+        g = np.zeros(self.nrules * 48, dtype=np.int32)
+        _check(lib().tce_lg_rule_gmax(self.h, _i(g)), self.h)
+        return g.reshape(self.nrules, 3, 16)
+
+    def set_plain_rule(self, u, wk, wg, scale=0.6):
+        u, wk, wg = (np.ascontiguousarray(x, dtype=np.float64) for x in (u, wk, wg))
+        _check(lib().tce_set_plain_rule(self.h, len(u), _d(u), _d(wk), _d(wg), float(scale)), self.h)
+
+    def lg_set_item_rules(self, rule: np.ndarray):
+        r = np.ascontiguousarray(rule, dtype=np.int32)
+        _check(lib().tce_lg_set_item_rules(self.h, _i(r)), self.h)
+
+    def lg_item_rules(self) -> np.ndarray:
+        r = np.zeros(self.info()["n_shell_quartets"], dtype=np.int32)
+        _check(lib().tce_lg_item_rules(self.h, _i(r)), self.h)
+        return r
+
+    def lg_predict_rules(self, net, plain_factor: float = 10.0):
+        _check(lib().tce_lg_predict_rules(self.h, net.h, float(plain_factor)), self.h)
+
+    def set_method(self, method: int):
+        _check(lib().tce_set_method(self.h, int(method)), self.h)
+
+    def set_tolerances(self, judge_tol=1e-10, plain_tol=1e-11, plain_max_panels=24):
+        _check(lib().tce_set_tolerances(self.h, float(judge_tol), float(plain_tol), int(plain_max_panels)), self.h)
+
+    def lg_stats(self) -> dict:
+        st = np.zeros(4, dtype=np.int64)
+        _check(lib().tce_lg_stats(self.h, st.ctypes.data_as(_lp)), self.h)
+        return {"learned": int(st[0]), "rejected": int(st[1]), "plain_direct": int(st[2]),
+                "plain_node_evals": int(st[3])}
+
+    def rule_blocks(self, rule: int, items: np.ndarray, mode: int = 1, judge: bool = False):
+        """Blocks of the given shell quartets with one quadrature (rule >= 0 dictionary,
+        -1 the system's rule, -2 the plain method); list of arrays (and Gauss estimates)."""
+        items = np.ascontiguousarray(items, dtype=np.int32).reshape(-1, 4)
+        sh = self.shells()
+        sizes = [int(np.prod([sh[S][1] for S in q])) for q in items]
+        tot = int(sum(sizes))
+        K = np.zeros(max(tot, 1))
+        G = np.zeros(max(tot, 1)) if (judge and rule >= 0) else None
+        _check(lib().tce_rule_blocks(self.h, int(rule), int(mode), len(items), _i(items), _d(K),
+                                     _d(G) if G is not None else None), self.h)
+        offs = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+        return K[:tot], (G[:tot] if G is not None else None), offs
 
 
 def hartree_exchange_potential(n1: int, P: np.ndarray, ERI: np.ndarray, physicist: bool = False):
