@@ -1,5 +1,6 @@
 #!/usr/bin/env python
-"""Benchmark: toroidal ERI quartets/s of one integral-direct J/K build.
+"""Benchmark: toroidal ERI quartets/s of one integral-direct J/K build,
+learned grid vs the plain adaptive method.
 
 Workload (BASELINE config "Tori1D RHF H chain", the quoted one): 64 cells,
 spacing 1.8 bohr, torus length 115.2 bohr, per H 3 contracted s (4 primitives,
@@ -10,6 +11,14 @@ A step is one direct_JK pass (eri_direct.f90:262): every symmetry-unique shell
 quartet evaluated and contracted with the density into J and K.  Unit of the
 metric: function quartets (ij|kl) of the translation- and 8-fold-unique set
 after the Schwarz screen, counted the same way for the CPU baseline.
+
+The headline pass uses the learned grid: before timing, labels for a sample
+of quartets are made against a 128-node reference rule and the rule-picking
+network is trained on the GPU (reported as set-up time, not timed); each
+quartet then gets one Gauss-Kronrod rule, the judge re-routes the quartets it
+rejects to the plain method inside the same pass.  The plain adaptive method
+and the reference's fixed 32-node rule are timed on the same device for
+comparison, and the held-out error of each against the reference is reported.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -183,6 +192,78 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
+# learned-grid set-up (untimed): labels on a sample, network trained on the GPU
+# ---------------------------------------------------------------------------
+def learned_grid_setup(eng, sysm, n_train=16000, seed=2026):
+    from william_ci_b200 import learned_grid as LG
+    t0 = time.perf_counter()
+    LG.setup(eng)
+    ref = LG.ReferenceBlocks(sysm)
+    items = eng.items()
+    rng = np.random.default_rng(seed)
+    idx = rng.choice(len(items), min(n_train + 2000, len(items)), replace=False)
+    tr, ho = items[idx[:-2000]], items[idx[-2000:]]
+    t1 = time.perf_counter()
+    data = LG.make_labels(eng, ref, tr)
+    t2 = time.perf_counter()
+    net = LG.RuleNet(eng.nrules, seed=0)
+    loss = net.train(data["X"], data["ok"], epochs=80, batch=256, lr=2e-3, seed=0)
+    t3 = time.perf_counter()
+    eng.lg_predict_rules(net, 10.0)
+    rules = eng.lg_item_rules()
+    t4 = time.perf_counter()
+    # accuracy on a held-out sample: the blocks the learned-grid pass keeps (judge-accepted
+    # dictionary rules; the rest go to the plain method), the plain method and the
+    # system's 32-node rule, each against the 128-node reference
+    rule_of = {tuple(q): r for q, r in zip(items, rules)}
+    T, _, offs = ref.rule_blocks(-1, ho)
+    seg = np.repeat(np.arange(len(ho)), np.diff(offs))
+    worst_lg = 0.0
+    hr = np.array([rule_of[tuple(q)] for q in ho])
+    for r in np.unique(hr):
+        m = np.nonzero(hr == r)[0]
+        if r == eng.nrules:
+            K, _, o2 = eng.rule_blocks(-2, ho[m])
+            keep = np.ones(len(m), bool)
+        else:
+            K, G, o2 = eng.rule_blocks(int(r), ho[m], judge=True)
+            keep = LG.judge_estimate(K, G, o2) <= LG.JUDGE_TOL
+        for j in np.nonzero(keep)[0]:
+            i = m[j]
+            worst_lg = max(worst_lg, float(np.abs(K[o2[j]:o2[j + 1]] - T[offs[i]:offs[i + 1]]).max(initial=0.0)))
+    Pl, _, _ = eng.rule_blocks(-2, ho)
+    Fx, _, _ = eng.rule_blocks(-1, ho)
+    ref.close()
+    R = eng.nrules
+    return net, {"labels_s": t2 - t1, "train_s": t3 - t2, "predict_s": t4 - t3, "setup_total_s": t4 - t0,
+                 "train_quartets": int(len(tr)), "rules": R, "train_loss": float(loss),
+                 "on_learned_grid": int(np.sum(rules < R)), "plain_direct": int(np.sum(rules >= R)),
+                 "max_err_vs_reference": {"learned_grid": worst_lg, "plain": float(np.abs(Pl - T).max()),
+                                          "fixed_32_node_rule": float(np.abs(Fx - T).max()),
+                                          "sample": "%d held-out shell quartets, 128-node mapped Gauss-Legendre "
+                                                    "reference" % len(ho)}}
+
+
+def timed_passes(eng, step, steps, flush, stream, world, dist):
+    import torch
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    kern = []
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for i in range(steps):
+        flush.fill_(float(i))                     # evict L2 between timed steps (not timed)
+        ev[i][0].record(stream)
+        step()
+        ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        kern.append(eng.last_kernel_ms())
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    return sum(a.elapsed_time(b) for a, b in ev), float(np.mean(kern))
+
+
 def main():
     args = parse()
     from william_ci_b200.system import AOSystem
@@ -193,7 +274,8 @@ def main():
 
     import torch
     import torch.distributed as dist
-    from william_ci_b200.engine import Engine, fp64_peak_tflops
+    from william_ci_b200.engine import (TCE_METHOD_FIXED, TCE_METHOD_LEARNED, TCE_METHOD_PLAIN, Engine,
+                                        fp64_peak_tflops)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -202,9 +284,10 @@ def main():
     dev = torch.device("cuda", local)
     if world > 1:
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
 
     eng = Engine(sysm)
+    net, lg_info = learned_grid_setup(eng, sysm)
     if world > 1:
         eng.set_shard(rank, world)
     info = eng.info()
@@ -222,36 +305,44 @@ def main():
             dist.all_reduce(dJ)
             dist.all_reduce(dK)
 
+    def run(method, steps, warmup):
+        eng.set_method(method)
+        for _ in range(warmup):
+            step()
+        torch.cuda.synchronize()
+        tot, kern = timed_passes(eng, step, steps, flush, stream, world, dist)
+        t = torch.tensor([tot, kern], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t[0]) / steps, float(t[1])
+
+    nq_total = info["n_func_quartets"]
+    # the headline: learned-grid J/K passes, clocks sampled during them
+    clocks = ClockSampler(local)
+    eng.set_method(TCE_METHOD_LEARNED)
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-
-    clocks = ClockSampler(local)
     clocks.start()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    kern_ms = []
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    for i in range(args.steps):
-        flush.fill_(float(i))                     # evict L2 between timed steps (not timed)
-        ev[i][0].record(stream)
-        step()
-        ev[i][1].record(stream)
-        torch.cuda.synchronize()
-        kern_ms.append(eng.last_kernel_ms())
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    tot_ms, lg_kern = timed_passes(eng, step, args.steps, flush, stream, world, dist)
     clk = clocks.stop()
-    tot_ms = sum(a.elapsed_time(b) for a, b in ev)
-    t = torch.tensor([tot_ms, float(np.mean(kern_ms))], dtype=torch.float64, device=dev)
+    t = torch.tensor([tot_ms, lg_kern], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    tot_ms, kmax = float(t[0]), float(t[1])
-    ms_step = tot_ms / args.steps
-    nq_total = info["n_func_quartets"]
+    ms_step, lg_kern = float(t[0]) / args.steps, float(t[1])
     value = nq_total / (ms_step * 1e-3)
+    st = eng.lg_stats()
+    from william_ci_b200 import learned_grid as LG
+    _, meta = LG.dictionary()
+    used = set(int(r) for r in eng.lg_item_rules() if r < eng.nrules)
+    classes = {2 * meta[r][1] + 1 <= 32 for r in used}
+    # learned-grid launches (one per node-count class), the fallback launch, the plain-direct launch
+    launches_per_step = len(classes) + int(len(used) > 0) + int(st["plain_direct"] > 0)
+    # comparison arms on the same device: the plain adaptive method and the system's 32-node rule
+    plain_steps = max(2, min(args.steps, 3))
+    plain_ms, _ = run(TCE_METHOD_PLAIN, plain_steps, 1)
+    fixed_ms, fixed_kern = run(TCE_METHOD_FIXED, args.steps, args.warmup)
+    eng.set_method(TCE_METHOD_LEARNED)
 
     # ---- end to end through the public API: pinned host P in, J/K out, every step
     Pp = torch.from_numpy(Ph.ravel(order="F").copy()).pin_memory()
@@ -279,7 +370,7 @@ def main():
         e2e_s = float(te[0])
     e2e = {"value": nq_total / e2e_s, "unit": "quartets/s", "h2d_bytes_per_step": 8 * n * n,
            "d2h_bytes_per_step": 2 * 8 * nf * n, "ms_per_step": 1e3 * e2e_s,
-           "api": "tce_direct_jk (host buffers, pinned)" if world == 1 else
+           "api": "tce_direct_jk, learned grid (host buffers, pinned)" if world == 1 else
                   "tce_direct_jk_device + NCCL all-reduce + pinned copies"}
 
     if rank != 0:
@@ -289,27 +380,37 @@ def main():
         return
 
     peak = fp64_peak_tflops()
-    achieved = info["jk_flops"] / (kmax * 1e-3) / 1e12 if world == 1 else None
+    lg_flops, lg_nprim = eng.lg_work() if world == 1 else (None, None)
+    achieved = lg_flops / (lg_kern * 1e-3) / 1e12 if world == 1 else None
     traffic = None
     if os.path.exists(PROFILE_TRAFFIC):
         try:
             traffic = json.load(open(PROFILE_TRAFFIC)).get("dram_bytes_per_launch")
         except Exception:
             traffic = None
-    roofline = {"bound": "fp64", "kernel": "k_quartets<32> (fused quartet evaluation + J/K scatter)",
+    roofline = {"bound": "fp64", "kernel": "k_quartets<32|64> learned grid (per-quartet rule, judge, fused J/K "
+                                           "scatter) + the plain fallback launch",
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if (achieved and peak) else None, "traffic": traffic,
                 "peak_source": "measured FP64 FMA throughput of this GPU (tce_fp64_peak probe); MEASURED_PEAKS.json "
                                "holds no FP64 figure",
-                "algorithmic_flops_per_launch": info["jk_flops"], "kernel_ms": kmax}
+                "algorithmic_flops_per_launch": lg_flops, "primitive_quartets": lg_nprim, "pass_ms": lg_kern}
     line = {"metric": METRIC, "value": value, "unit": "quartets/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded exponents/coefficients)",
             "config": config(sysm, {"parallelism": "quartet shards x%d + NCCL all-reduce of J/K" % world
                                     if world > 1 else "single GPU",
+                                    "quadrature": "learned grid: per-quartet Gauss-Kronrod rule (K15..K61, 21 map "
+                                                  "scales) picked by the network, judge <= 1e-10, plain fallback",
                                     "shell_quartets": info["n_shell_quartets"],
-                                    "function_quartets": nq_total, "primitive_quartets": info["n_prim_quartets"]}),
-            "e2e": e2e, "roofline": roofline, "clocks": clk, "gpu_launches": args.steps}
+                                    "function_quartets": nq_total}),
+            "plain": {"value": nq_total / (plain_ms * 1e-3), "ms_per_step": plain_ms, "steps": plain_steps,
+                      "method": "device adaptive Gauss-Kronrod bisection (15/7 panels, Bessel columns per panel)"},
+            "lg_over_plain": plain_ms / ms_step,
+            "fixed_rule": {"value": nq_total / (fixed_ms * 1e-3), "ms_per_step": fixed_ms,
+                           "method": "the reference's 32-node mapped Gauss-Legendre rule on the same engine"},
+            "learned_grid": dict(lg_info, judge_rejected_last_pass=st["rejected"]),
+            "e2e": e2e, "roofline": roofline, "clocks": clk, "gpu_launches": args.steps * launches_per_step}
     if world == 1:
         line["rhf_scf"] = scf_iterations(eng, sysm)
     if world == 1 and not args.no_cpu_baseline:

@@ -217,6 +217,11 @@ int tce_set_tolerances(void *handle, double judge_tol, double plain_tol, int32_t
  * the plain method, stats[3] t nodes the plain method evaluated. */
 int tce_lg_stats(void *handle, int64_t *stats);
 
+/* Algorithmic FP64 operations and primitive quartets of the learned-grid pass
+ * with the current per-item rules (quartets sent to the plain method
+ * excluded), counted like tce_info.jk_flops with each quartet's own rule. */
+int tce_lg_work(void *handle, double *flops, int64_t *nprim);
+
 /* Blocks of n shell quartets with one quadrature, concatenated in item order
  * (each column-major n1 n2 n3 n4): rule >= 0 a dictionary rule (Kronrod
  * estimate in K, Gauss estimate in G when G is not NULL), -1 the system's

@@ -524,7 +524,16 @@ int build(Handle *h, const tce_system *sys)
         }
         std::vector<size_t> ord(items.size());
         std::iota(ord.begin(), ord.end(), 0);
-        std::stable_sort(ord.begin(), ord.end(), [&](size_t x, size_t y) { return cost[x] > cost[y]; });
+        // ties broken by the quartet itself: the enumeration kernel emits items in
+        // no fixed order, and every rank of a sharded run must see the same list
+        std::sort(ord.begin(), ord.end(), [&](size_t x, size_t y) {
+            if (cost[x] != cost[y]) return cost[x] > cost[y];
+            const int4 &a = items[x], &b = items[y];
+            if (a.x != b.x) return a.x < b.x;
+            if (a.y != b.y) return a.y < b.y;
+            if (a.z != b.z) return a.z < b.z;
+            return a.w < b.w;
+        });
         std::vector<int4> sorted(items.size());
         h->cost_host.resize(items.size());
         for (size_t i = 0; i < ord.size(); ++i) {

@@ -72,6 +72,7 @@ struct Handle {
     std::vector<RuleDev> rules_host;
     RuleDev *d_rules = nullptr;
     double *d_rule_T = nullptr, *d_rule_t = nullptr, *d_rule_wk = nullptr, *d_rule_wg = nullptr;
+    int *d_rule_tnmax = nullptr;         // [r][3][64] truncation order per rule node
     std::vector<int> item_rule;          // per items_host entry; lg_nrules = plain directly
     int4 *d_lg_items[2] = {nullptr, nullptr};   // learned-grid items with 32- / 64-node rules
     int *d_lg_rule[2] = {nullptr, nullptr};

@@ -273,7 +273,10 @@ __global__ void k_enumerate(DevSys S, const double *Qsh, double Qmax, int4 *item
 //   + ncomb*nq weight fold + nA nB nC nD (3 nq + 5) component contraction
 // one warp per shell quartet, lanes over primitive quartets; same screens as k_quartets.
 // ============================================================================
+// With item_rule set, item it uses dictionary rule item_rule[it] (rules[r].nn
+// nodes, truncation orders rule_tnmax[(r*3 + d)*64 + k]) and its judge sum.
 __global__ void k_count_work(DevSys S, const int4 *items, int nitems, int prim_screen, const int *tnmax,
+                             const int *item_rule, const RuleDev *rules, const int *rule_tnmax,
                              unsigned long long *nprim, double *flops)
 {
     const int lane = threadIdx.x & 31;
@@ -283,6 +286,17 @@ __global__ void k_count_work(DevSys S, const int4 *items, int nitems, int prim_s
     double myf = 0.0;
     for (int it = warp; it < nitems; it += nw) {
         int4 q = items[it];
+        int nq = S.nq;
+        const int *tnm = tnmax;
+        int tstride = S.nq;
+        double judge = 0.0;
+        if (item_rule) {
+            const int r = item_rule[it];
+            nq = rules[r].nn;
+            tnm = rule_tnmax + (long long)r * 3 * 64;
+            tstride = 64;
+            judge = 1.0;
+        }
         int lsA = S.sh_l[q.x], lsB = S.sh_l[q.y], lsC = S.sh_l[q.z], lsD = S.sh_l[q.w];
         int ncomb = (lsA + 1) * (lsB + 1) * (lsC + 1) * (lsD + 1);
         int NN = lsA + lsB + lsC + lsD;
@@ -296,7 +310,7 @@ __global__ void k_count_work(DevSys S, const int4 *items, int nitems, int prim_s
             int ia = cmb % (lsA + 1), t1 = cmb / (lsA + 1);
             int ib = t1 % (lsB + 1), t2 = t1 / (lsB + 1);
             int ic = t2 % (lsC + 1), id = t2 / (lsC + 1);
-            realc += 3.0 * (ia + ib + 1) * (ic + id + 1) + 2.0 * S.nq * (ia + ib + ic + id + 1);
+            realc += 3.0 * (ia + ib + 1) * (ic + id + 1) + 2.0 * nq * (ia + ib + ic + id + 1);
         }
         long long total = (long long)Ub.npp * Uk.npp;
         for (long long idx = lane; idx < total; idx += 32) {
@@ -313,14 +327,14 @@ __global__ void k_count_work(DevSys S, const int4 *items, int nitems, int prim_s
             for (int d = 0; d < S.ndp; ++d) {
                 int nm = Pb.N[d] < Pk.N[d] ? Pb.N[d] : Pk.N[d];
                 double dots = 0.0;
-                for (int k = 0; k < S.nq; ++k) {
-                    int tn = tnmax[d * S.nq + k];
+                for (int k = 0; k < nq; ++k) {
+                    int tn = tnm[d * tstride + k];
                     dots += 2.0 * ((nm < tn ? nm : tn) + 1);
                 }
                 f += 6.0 * (nm + 1) + ncomb * 8.0 * (nm + 1) + ncomb * dots;
             }
-            for (int d = S.ndp; d < 3; ++d) f += S.nq * (8.0 + 2.0 * NN) + realc;
-            f += (double)ncomb * S.nq + (double)ncq * (3.0 * S.nq + 5.0);
+            for (int d = S.ndp; d < 3; ++d) f += nq * (8.0 + 2.0 * NN) + realc;
+            f += (double)ncomb * nq + (double)ncq * (3.0 * nq + 5.0) + judge * (double)ncq * 2.0 * nq;
             myf += f;
         }
     }
@@ -336,10 +350,12 @@ __global__ void k_count_work(DevSys S, const int4 *items, int nitems, int prim_s
 }
 
 int tce_launch_count_work(const DevSys &S, const int4 *items, int nitems, int prim_screen, const int *tnmax,
-                          unsigned long long *nprim, double *flops, cudaStream_t st)
+                          unsigned long long *nprim, double *flops, cudaStream_t st, const int *item_rule,
+                          const RuleDev *rules, const int *rule_tnmax)
 {
     if (nitems == 0) return TCE_OK;
-    k_count_work<<<148 * 8, 128, 0, st>>>(S, items, nitems, prim_screen, tnmax, nprim, flops);
+    k_count_work<<<148 * 8, 128, 0, st>>>(S, items, nitems, prim_screen, tnmax, item_rule, rules, rule_tnmax, nprim,
+                                          flops);
     return cudaGetLastError() == cudaSuccess ? TCE_OK : TCE_ERR_CUDA;
 }
 

@@ -87,5 +87,6 @@ int tce_launch_stored_jk(int n1, int nbas, int physicist, const double *P, const
                          cudaStream_t st);
 int tce_launch_sym_fill(int nf, int fpuc, const int *ncl, double *eri, cudaStream_t st);
 int tce_launch_count_work(const DevSys &S, const int4 *items, int nitems, int prim_screen, const int *tnmax,
-                          unsigned long long *nprim, double *flops, cudaStream_t st);
+                          unsigned long long *nprim, double *flops, cudaStream_t st, const int *item_rule = nullptr,
+                          const RuleDev *rules = nullptr, const int *rule_tnmax = nullptr);
 int tce_launch_fp64_probe(int nsm, int iters, double *sink, cudaStream_t st, long long *flops);

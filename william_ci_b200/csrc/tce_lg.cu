@@ -566,8 +566,9 @@ int tce_lg_set_rules(void *handle, int32_t nrules, const int32_t *nn, const doub
         if (nn[r] < 1 || nn[r] > 64) return fail(h, TCE_ERR_ARG, "a rule has 1..64 nodes");
     int s;
     for (void *p : {(void *)h->d_rules, (void *)h->d_rule_T, (void *)h->d_rule_t, (void *)h->d_rule_wk,
-                    (void *)h->d_rule_wg})
+                    (void *)h->d_rule_wg, (void *)h->d_rule_tnmax})
         dfree(h, p);
+    h->d_rule_tnmax = nullptr;
     h->d_rules = nullptr;
     h->d_rule_T = h->d_rule_t = h->d_rule_wk = h->d_rule_wg = nullptr;
     h->lg_nrules = 0;
@@ -597,6 +598,7 @@ int tce_lg_set_rules(void *handle, int32_t nrules, const int32_t *nn, const doub
     if ((s = dalloc(h, &tb, (size_t)(h->ncap + 1) * 64 * h->ndp))) return s;
     if ((s = dalloc(h, &tn, (size_t)64 * h->ndp))) return s;
     std::vector<int> tnmax((size_t)64 * h->ndp);
+    std::vector<int> all_tn((size_t)nrules * 3 * 64, 0);
     for (int r = 0; r < nrules; ++r) {
         RuleDev &R = h->rules_host[r];
         CKS(h, tce_launch_t_tables(R.nq, h->ndp, h->ncap, h->d_rule_t + R.node_off, h->a, tb, tn,
@@ -604,6 +606,8 @@ int tce_lg_set_rules(void *handle, int32_t nrules, const int32_t *nn, const doub
         CK(h, cudaMemcpyAsync(tnmax.data(), tn, sizeof(int) * R.nq * h->ndp, cudaMemcpyDeviceToHost, h->st));
         CK(h, cudaStreamSynchronize(h->st));
         for (int i = 0; i < 3 * TCE_MAXG; ++i) R.gmax[i] = -1;
+        for (int d = 0; d < h->ndp; ++d)
+            for (int k = 0; k < R.nq; ++k) all_tn[((size_t)r * 3 + d) * 64 + k] = tnmax[(size_t)d * R.nq + k];
         for (int d = 0; d < h->ndp; ++d)
             for (int g = 0; g < R.nq / 8; ++g) {
                 int m = -1;
@@ -615,6 +619,7 @@ int tce_lg_set_rules(void *handle, int32_t nrules, const int32_t *nn, const doub
     dfree(h, tb);
     dfree(h, tn);
     if ((s = upload(h, &h->d_rules, h->rules_host))) return s;
+    if ((s = upload(h, &h->d_rule_tnmax, all_tn))) return s;
     h->lg_nrules = nrules;
     CK(h, cudaStreamSynchronize(h->st));
     return lg_rebuild_lists(h);
@@ -1018,6 +1023,36 @@ int tce_lg_predict_rules(void *handle, void *mlp, double plain_factor)
     dfree(h, d_Z);
     dfree(h, d_c);
     return lg_rebuild_lists(h);
+}
+
+// Algorithmic work of the learned-grid pass with the current per-item rules
+// (the quartets on the learned grid; adaptive plain-method work is not
+// included): FP64 operations and primitive quartets, counted as for the
+// system's rule, with each quartet's own rule and its judge sum.
+int tce_lg_work(void *handle, double *flops, int64_t *nprim)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !flops || !nprim) return fail(h, TCE_ERR_ARG, "NULL argument");
+    if (h->n_lg == 0) return fail(h, TCE_ERR_STATE, "no learned-grid items");
+    int s;
+    unsigned long long *d_np = nullptr;
+    double *d_fl = nullptr;
+    if ((s = dalloc(h, &d_np, 1))) return s;
+    if ((s = dalloc(h, &d_fl, 1))) return s;
+    CK(h, cudaMemsetAsync(d_np, 0, sizeof(unsigned long long), h->st));
+    CK(h, cudaMemsetAsync(d_fl, 0, sizeof(double), h->st));
+    for (int c = 0; c < 2; ++c)
+        if (h->n_lg_q[c] > 0)
+            CKS(h, tce_launch_count_work(h->S, h->d_lg_items[c], (int)h->n_lg_q[c], h->prim_screen, h->d_tnmax, d_np,
+                                         d_fl, h->st, h->d_lg_rule[c], h->d_rules, h->d_rule_tnmax));
+    unsigned long long np_ = 0;
+    CK(h, cudaMemcpyAsync(&np_, d_np, sizeof np_, cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaMemcpyAsync(flops, d_fl, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    *nprim = (int64_t)np_;
+    dfree(h, d_np);
+    dfree(h, d_fl);
+    return TCE_OK;
 }
 
 int tce_lg_item_rules(void *handle, int32_t *rule)

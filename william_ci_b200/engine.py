@@ -41,7 +41,7 @@ EXPORTS = ["tce_create", "tce_destroy", "tce_last_error", "tce_get_info", "tce_s
            "tce_lg_set_item_rules", "tce_lg_item_rules", "tce_set_method", "tce_set_tolerances", "tce_lg_stats",
            "tce_rule_blocks", "tce_mlp_create", "tce_mlp_destroy", "tce_mlp_last_error", "tce_mlp_nparams",
            "tce_mlp_get_params", "tce_mlp_set_params", "tce_mlp_loss_grad", "tce_mlp_train", "tce_mlp_predict",
-           "tce_lg_predict_rules"]
+           "tce_lg_predict_rules", "tce_lg_work"]
 
 TCE_METHOD_FIXED, TCE_METHOD_LEARNED, TCE_METHOD_PLAIN = 0, 1, 2
 TCE_NFEAT = 12
@@ -123,6 +123,7 @@ def lib():
                                     _fp]
         L.tce_mlp_predict.argtypes = [C.c_void_p, C.c_int64, _fp, _fp]
         L.tce_lg_predict_rules.argtypes = [C.c_void_p, C.c_void_p, C.c_double]
+        L.tce_lg_work.argtypes = [C.c_void_p, _dp, _lp]
         _lib = L
     return _lib
 
@@ -329,6 +330,13 @@ class Engine:
 
     def lg_predict_rules(self, net, plain_factor: float = 10.0):
         _check(lib().tce_lg_predict_rules(self.h, net.h, float(plain_factor)), self.h)
+
+    def lg_work(self):
+        """(FP64 operations, primitive quartets) of the learned-grid pass."""
+        f = C.c_double()
+        n = C.c_int64()
+        _check(lib().tce_lg_work(self.h, C.byref(f), C.byref(n)), self.h)
+        return f.value, n.value
 
     def set_method(self, method: int):
         _check(lib().tce_set_method(self.h, int(method)), self.h)
