@@ -13,9 +13,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtce.so")
-SOURCES = ["tce_api.cu", "tce_kernels.cu", "tce_kernels_s.cu", "tce_quartets.cu", "tce_lg.cu"]
+SOURCES = ["tce_api.cu", "tce_kernels.cu", "tce_kernels_s.cu", "tce_kernels_slg.cu", "tce_quartets.cu", "tce_lg.cu"]
 OBJDIR = os.path.join(HERE, "_build")
-HEADERS = ["tce_device.cuh", "tce_kernels.h", "tce_handle.h"]
+HEADERS = ["tce_device.cuh", "tce_kernels.h", "tce_handle.h", "tce_kernels_s.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -50,19 +50,25 @@ def _compile(src: str, obj: str, verbose: bool, ptxas_info: bool) -> None:
 
 
 def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
-    """Compile each source to an object (only when it or a header changed), then link."""
+    """Compile each source to an object (only when it or a header changed, in
+    parallel), then link."""
+    from concurrent.futures import ThreadPoolExecutor
     os.makedirs(OBJDIR, exist_ok=True)
     hdr_t = max(_mtime(h) for h in _headers())
-    objs, relink = [], force or not os.path.exists(LIB)
+    objs, relink, todo = [], force or not os.path.exists(LIB), []
     for f in SOURCES:
         src = os.path.join(CSRC, f)
         obj = os.path.join(OBJDIR, f.replace(".cu", ".o"))
         objs.append(obj)
         if force or _mtime(obj) < max(_mtime(src), hdr_t):
-            _compile(src, obj, verbose, ptxas_info)
+            todo.append((src, obj))
             relink = True
         elif _mtime(obj) > _mtime(LIB):
             relink = True
+    if todo:
+        with ThreadPoolExecutor(max_workers=min(len(todo), os.cpu_count() or 1)) as ex:
+            for fut in [ex.submit(_compile, s, o, verbose, ptxas_info) for s, o in todo]:
+                fut.result()
     if relink:
         cmd = [nvcc(), *ARCH, "-shared", "-o", LIB + ".tmp", *objs]
         r = subprocess.run(cmd, capture_output=True, text=True)

@@ -74,9 +74,11 @@ struct Handle {
     double *d_rule_T = nullptr, *d_rule_t = nullptr, *d_rule_wk = nullptr, *d_rule_wg = nullptr;
     int *d_rule_tnmax = nullptr;         // [r][3][64] truncation order per rule node
     std::vector<int> item_rule;          // per items_host entry; lg_nrules = plain directly
-    int4 *d_lg_items[2] = {nullptr, nullptr};   // learned-grid items with 32- / 64-node rules
-    int *d_lg_rule[2] = {nullptr, nullptr};
-    long long n_lg_q[2] = {0, 0};
+    // learned-grid work, one list per kernel and rule size: kind 0 generic
+    // (k_quartets), 1 all-s (k_quartets_s), 2 one-periodic-direction s/p class
+    // `cls` (k_quartets_r1); nq = 32 or 64 padded rule nodes
+    struct LgList { int kind, cls, nq; int4 *d = nullptr; int *rule = nullptr; long long n = 0; };
+    std::vector<LgList> lg_lists;
     long long n_lg = 0;
     int4 *d_plain_items = nullptr;
     long long n_plain_direct = 0;

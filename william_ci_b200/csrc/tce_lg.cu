@@ -358,6 +358,31 @@ static int ensure_plain(Handle *h)
     return TCE_OK;
 }
 
+// which kernel evaluates a learned-grid quartet: kind * 16 + cls (kind 1 all-s,
+// 2 one periodic direction with a single p shell in the reference component
+// order, 0 everything else)
+static int lg_route(const Handle *h, const int4 &q)
+{
+    const int l[4] = {h->sh_l[q.x], h->sh_l[q.y], h->sh_l[q.z], h->sh_l[q.w]};
+    int cls = 0;
+    bool sp = true;
+    for (int i = 0; i < 4; ++i) {
+        if (l[i] > 1) sp = false;
+        else cls |= l[i] << i;
+    }
+    if (!sp) return 0;
+    for (int i = 0; i < 4; ++i) {
+        const int S = (&q.x)[i];
+        if (l[i] == 1)
+            for (int c = 0; c < 3; ++c)
+                for (int d = 0; d < 3; ++d)
+                    if (h->lxyz[3 * (h->sh_first[S] + c) + d] != (c == d ? 1 : 0)) return 0;
+    }
+    if (cls == 0) return 16;
+    if (h->ndp == 1 && __builtin_popcount(cls) == 1) return 32 + cls;
+    return 0;
+}
+
 static void fill_common(Handle *h, QuartetHostArgs &a)
 {
     a.max_ncomb = h->max_ncomb;
@@ -393,36 +418,43 @@ int lg_rebuild_lists(Handle *h)
     mine.reserve(h->shard_idx.size());
     for (long long i : h->shard_idx) mine.push_back(h->items_host[(size_t)i]);
     if ((s = upload(h, &h->d_shard_items, mine))) return s;
-    for (int c = 0; c < 2; ++c) {
-        dfree(h, h->d_lg_items[c]);
-        dfree(h, h->d_lg_rule[c]);
-        h->d_lg_items[c] = nullptr;
-        h->d_lg_rule[c] = nullptr;
-        h->n_lg_q[c] = 0;
+    for (auto &w : h->lg_lists) {
+        dfree(h, w.d);
+        dfree(h, w.rule);
     }
+    h->lg_lists.clear();
     dfree(h, h->d_plain_items);
     dfree(h, h->d_fb_items);
     h->d_plain_items = h->d_fb_items = nullptr;
     h->n_lg = h->n_plain_direct = 0;
     if (h->item_rule.size() != h->items_host.size() || h->lg_nrules == 0) return TCE_OK;
-    std::vector<int4> lg[2], pl;
-    std::vector<int> rl[2];
+    // key = (kind * 16 + cls) * 2 + (nq == 64)
+    std::vector<std::vector<int4>> lg(3 * 16 * 2);
+    std::vector<std::vector<int>> rl(3 * 16 * 2);
+    std::vector<int4> pl;
     for (long long i : h->shard_idx) {
         const int r = h->item_rule[(size_t)i];
+        const int4 &q = h->items_host[(size_t)i];
         if (r >= 0 && r < h->lg_nrules) {
-            const int c = h->rules_host[r].nq == 32 ? 0 : 1;
-            lg[c].push_back(h->items_host[(size_t)i]);
-            rl[c].push_back(r);
+            const int key = lg_route(h, q) * 2 + (h->rules_host[r].nq == 64 ? 1 : 0);
+            lg[key].push_back(q);
+            rl[key].push_back(r);
         } else {
-            pl.push_back(h->items_host[(size_t)i]);
+            pl.push_back(q);
         }
     }
-    for (int c = 0; c < 2; ++c) {
-        if ((s = upload(h, &h->d_lg_items[c], lg[c]))) return s;
-        if ((s = upload(h, &h->d_lg_rule[c], rl[c]))) return s;
-        h->n_lg_q[c] = (long long)lg[c].size();
+    for (int key = 0; key < 3 * 16 * 2; ++key) {
+        if (lg[key].empty()) continue;
+        Handle::LgList w;
+        w.kind = key / 32;
+        w.cls = (key / 2) % 16;
+        w.nq = (key & 1) ? 64 : 32;
+        w.n = (long long)lg[key].size();
+        if ((s = upload(h, &w.d, lg[key]))) return s;
+        if ((s = upload(h, &w.rule, rl[key]))) return s;
+        h->lg_lists.push_back(w);
+        h->n_lg += w.n;
     }
-    h->n_lg = h->n_lg_q[0] + h->n_lg_q[1];
     if ((s = upload(h, &h->d_plain_items, pl))) return s;
     if ((s = dalloc(h, &h->d_fb_items, (size_t)std::max<long long>(h->n_lg, 1)))) return s;
     if (!h->d_fb_count && (s = dalloc(h, &h->d_fb_count, 1))) return s;
@@ -456,18 +488,40 @@ int lg_jk_passes(Handle *h, const double *dP, double *dJ, double *dK, cudaStream
     if (!h->d_rules || h->item_rule.size() != h->items_host.size())
         return fail(h, TCE_ERR_STATE, "learned grid needs rules and per-item rules");
     CK(h, cudaMemsetAsync(h->d_fb_count, 0, sizeof(unsigned int), st));
-    for (int c = 0; c < 2; ++c) {
-        if (h->n_lg_q[c] == 0) continue;
-        QuartetHostArgs b = a;
-        b.method = TCE_METHOD_LEARNED;
-        b.dict_nq = c == 0 ? 32 : 64;
-        b.items = h->d_lg_items[c];
-        b.nitems = (int)h->n_lg_q[c];
-        b.item_rule = h->d_lg_rule[c];
-        b.fb_items = h->d_fb_items;
-        b.fb_count = h->d_fb_count;
-        b.next = h->d_next;
-        CKS(h, tce_launch_quartets(h->S, b, st));
+    for (const auto &w : h->lg_lists) {
+        if (w.kind == 0) {
+            QuartetHostArgs b = a;
+            b.method = TCE_METHOD_LEARNED;
+            b.dict_nq = w.nq;
+            b.items = w.d;
+            b.nitems = (int)w.n;
+            b.item_rule = w.rule;
+            b.fb_items = h->d_fb_items;
+            b.fb_count = h->d_fb_count;
+            b.next = h->d_next;
+            CKS(h, tce_launch_quartets(h->S, b, st));
+        } else {
+            SArgsHost b;
+            b.items = w.d;
+            b.nitems = (int)w.n;
+            b.prim_screen = h->prim_screen;
+            b.next = h->d_next;
+            b.P = dP;
+            b.J = dJ;
+            b.K = dK;
+            b.num_sms = h->num_sms;
+            b.item_rule = w.rule;
+            b.rules = h->d_rules;
+            b.rule_T = h->d_rule_T;
+            b.rule_t = h->d_rule_t;
+            b.rule_wk = h->d_rule_wk;
+            b.rule_wg = h->d_rule_wg;
+            b.judge_tol = h->judge_tol;
+            b.fb_items = h->d_fb_items;
+            b.fb_count = h->d_fb_count;
+            if (w.kind == 1) CKS(h, tce_launch_quartets_s_lg(h->S, b, w.nq, st));
+            else CKS(h, tce_launch_quartets_r1_lg(h->S, w.cls, b, w.nq, st));
+        }
     }
     if (h->n_plain_direct > 0) {
         QuartetHostArgs b = a;
@@ -1041,10 +1095,9 @@ int tce_lg_work(void *handle, double *flops, int64_t *nprim)
     if ((s = dalloc(h, &d_fl, 1))) return s;
     CK(h, cudaMemsetAsync(d_np, 0, sizeof(unsigned long long), h->st));
     CK(h, cudaMemsetAsync(d_fl, 0, sizeof(double), h->st));
-    for (int c = 0; c < 2; ++c)
-        if (h->n_lg_q[c] > 0)
-            CKS(h, tce_launch_count_work(h->S, h->d_lg_items[c], (int)h->n_lg_q[c], h->prim_screen, h->d_tnmax, d_np,
-                                         d_fl, h->st, h->d_lg_rule[c], h->d_rules, h->d_rule_tnmax));
+    for (const auto &w : h->lg_lists)
+        CKS(h, tce_launch_count_work(h->S, w.d, (int)w.n, h->prim_screen, h->d_tnmax, d_np, d_fl, h->st, w.rule,
+                                     h->d_rules, h->d_rule_tnmax));
     unsigned long long np_ = 0;
     CK(h, cudaMemcpyAsync(&np_, d_np, sizeof np_, cudaMemcpyDeviceToHost, h->st));
     CK(h, cudaMemcpyAsync(flops, d_fl, sizeof(double), cudaMemcpyDeviceToHost, h->st));
