@@ -106,6 +106,15 @@ int tce_shell_block(void *handle, const int32_t sh4[4], int32_t mode, double *bl
  * them concurrently from several threads or handles. */
 int tce_shell_block_noalloc(void *handle, const int32_t sh4[4], int32_t mode, double *blk);
 
+/* Start-up accuracy gate of the fast rule (replaces the ERI part of
+ * fast_quad_self_check, fast_quad_self_check.f90:30-233): `fast` and `full`
+ * are handles of the same system built with the 32/40-node rule and with the
+ * 64/128-point table.  The on-site quartets (SI SI|SI SI) of the unit cell and
+ * 50 pseudo-random quartets (the reference's generator and seed) are
+ * evaluated on both; dmax is the largest difference.  The reference keeps the
+ * fast rule when dmax <= 1e-10, the caller does the same with its handles. */
+int tce_quad_self_check(void *fast, void *full, double *dmax, int32_t *nsample);
+
 /* Shell list: first function and component count of each shell. */
 int tce_shells(void *handle, int32_t *first, int32_t *n);
 
@@ -142,6 +151,13 @@ int tce_direct_jk_device(void *handle, const double *dP, double *dJ, double *dK,
 /* Elapsed device time (ms) of the last tce_direct_jk[_device] call's quartet
  * kernel, measured with CUDA events on the launching stream. */
 int tce_last_kernel_ms(void *handle, double *ms);
+
+/* CUDA graphs: with on != 0, every J/K pass of this handle (all its kernel
+ * launches and the zeroing of J and K) is captured once into a CUDA graph and
+ * replayed as one graph launch per call, e.g. once per SCF iteration.  The
+ * graph is re-captured when the pointers, the stream, the method or the work
+ * lists change.  Default off. */
+int tce_set_graph(void *handle, int32_t on);
 
 /* Multi-GPU: restrict tce_direct_jk[_device] on this handle to shard `rank`
  * of `nranks` (cost-balanced partition of the unique shell quartets, the same
@@ -204,6 +220,13 @@ int tce_set_plain_rule(void *handle, int32_t n, const double *u, const double *w
 int tce_lg_set_item_rules(void *handle, const int32_t *rule);
 int tce_lg_item_rules(void *handle, int32_t *rule);
 
+/* FP32 panels: learned-grid quartets of the register kernels (one periodic
+ * direction) whose shell-pair Schwarz product Q(ij)Q(kl) is below thr sum
+ * their periodic-direction node sums in FP32 (FP32 copy of the rule tables);
+ * phases, Bessel vectors, real directions, weights, the judge and the J/K
+ * accumulation stay FP64.  thr = 0 (default) turns it off; at most 1e-3. */
+int tce_set_fp32_threshold(void *handle, double thr);
+
 /* Quadrature method of tce_direct_jk[_device] (TCE_METHOD_*). */
 int tce_set_method(void *handle, int32_t method);
 
@@ -214,7 +237,8 @@ int tce_set_tolerances(void *handle, double judge_tol, double plain_tol, int32_t
 
 /* Counters of the last J/K pass: stats[0] quartets on the learned grid,
  * stats[1] of those rejected by the judge, stats[2] quartets sent straight to
- * the plain method, stats[3] t nodes the plain method evaluated. */
+ * the plain method, stats[3] t nodes the plain method evaluated, stats[4]
+ * learned-grid quartets with FP32 node sums (array of 5). */
 int tce_lg_stats(void *handle, int64_t *stats);
 
 /* Algorithmic FP64 operations and primitive quartets of the learned-grid pass

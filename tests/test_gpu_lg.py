@@ -198,3 +198,48 @@ def test_rhf_energy_learned_grid_vs_oracle(which):
     dev = scf.rhf_sao(St, Tt, Vt, en, nO, sysm.nfuc, sysm.ncell, eng.direct_JK)
     assert ref.converged and dev.converged
     assert abs(dev.energy - ref.energy) < 1e-8, (dev.energy, ref.energy)
+
+
+@pytest.fixture(scope="module")
+def chain16_lg(systems):
+    sysm = systems("h_chain64", (16, 1, 1))
+    eng = _lg_engine(sysm)
+    net, _, _ = _trained(eng, sysm)
+    eng.lg_predict_rules(net)
+    return sysm, eng
+
+
+def test_graph_replay_matches_direct_launches(chain16_lg):
+    from william_ci_b200.engine import TCE_METHOD_FIXED, TCE_METHOD_LEARNED
+    sysm, eng = chain16_lg
+    P = random_density(sysm.nbas, 3) * 0.05
+    scale = np.abs(P).sum()
+    for method in (TCE_METHOD_LEARNED, TCE_METHOD_FIXED):
+        eng.set_graph(False)
+        eng.set_method(method)
+        J0, K0 = eng.direct_JK(P)
+        eng.set_graph(True)
+        J1, K1 = eng.direct_JK(P)          # captured
+        J2, K2 = eng.direct_JK(0.5 * P)    # replayed with new data in the same buffers
+        assert np.abs(J1 - J0).max() <= 1e-13 * scale and np.abs(K1 - K0).max() <= 1e-13 * scale
+        assert np.abs(J2 - 0.5 * J0).max() <= 1e-13 * scale and np.abs(K2 - 0.5 * K0).max() <= 1e-13 * scale
+    eng.set_graph(False)
+
+
+def test_fp32_panels_error_vs_fp64(chain16_lg):
+    """FP32 node sums for quartets with Schwarz product below 1e-6: the J/K
+    difference from the all-FP64 pass stays below 1e-10 per unit density."""
+    from william_ci_b200.engine import TCE_METHOD_LEARNED
+    sysm, eng = chain16_lg
+    P = random_density(sysm.nbas, 4) * 0.05
+    scale = np.abs(P).sum()
+    eng.set_method(TCE_METHOD_LEARNED)
+    eng.set_fp32_threshold(0.0)
+    J0, K0 = eng.direct_JK(P)
+    eng.set_fp32_threshold(1e-6)
+    J1, K1 = eng.direct_JK(P)
+    st = eng.lg_stats()
+    eng.set_fp32_threshold(0.0)
+    assert st["fp32"] > 0.2 * st["learned"]
+    err = max(np.abs(J1 - J0).max(), np.abs(K1 - K0).max())
+    assert err <= 1e-10 * scale, err

@@ -102,3 +102,37 @@ def test_direct_jk_full_chain64(systems):
     Jo, Ko, _ = orc.direct_jk(P)
     np.testing.assert_allclose(J, Jo, rtol=0, atol=TOL_JK)
     np.testing.assert_allclose(K, Ko, rtol=0, atol=TOL_JK)
+
+
+def _lcg_sample(nshuc, nsh, nrand=50):
+    """The self-check sample of fast_quad_self_check.f90:105-124 (0-based shells)."""
+    seed = 12345
+    out = [(i, i, i, i) for i in range(max(nshuc, 1))]
+    for _ in range(nrand):
+        q = []
+        for m in (nshuc, nsh, nsh, nsh):
+            seed = (seed * 1103515245 + 12345) % 2147483648
+            q.append((seed // 16) % m)
+        out.append(tuple(q))
+    return out
+
+
+@pytest.mark.parametrize("name,ncell", [("h_chain64", (8, 1, 1)), ("li_cube", (2, 2, 2))])
+def test_fast_quad_self_check_vs_oracle(systems, name, ncell):
+    import json
+    import os
+    import pyoracle
+    from william_ci_b200.engine import Engine, fast_quad_self_check
+    tab = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "quad_tables.json")))["128"]
+    sysm = systems(name, ncell)
+    fast = Engine(sysm)
+    full = Engine(sysm, t_nodes=tab["t_val"], t_weights=tab["w_val"])
+    d, n, keep = fast_quad_self_check(fast, full)
+    o32 = pyoracle.Oracle(sysm)
+    o128 = pyoracle.Oracle(sysm, t_nodes=tab["t_val"], t_weights=tab["w_val"])
+    sh, nshuc, _ = o32.shells()
+    sample = _lcg_sample(nshuc, len(sh))
+    assert n == len(sample)
+    dref = max(np.abs(o32.shell_block(*q, mode=0) - o128.shell_block(*q, mode=0)).max() for q in sample)
+    assert abs(d - dref) <= 1e-12, (d, dref)
+    assert keep == (dref <= 1e-10)

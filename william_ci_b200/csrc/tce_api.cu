@@ -127,6 +127,7 @@ int route(const Handle *h, const int4 &q)
 // split a list of quartets (most expensive first) into per-kernel device lists
 int make_lists(Handle *h, const std::vector<int4> &items)
 {
+    ++h->work_version;
     for (auto &w : h->lists) dfree(h, w.d);
     h->lists.clear();
     std::vector<std::vector<int4>> by(3 * 16);
@@ -576,17 +577,12 @@ int build(Handle *h, const tce_system *sys)
     return TCE_OK;
 }
 
-int direct_jk_device(Handle *h, const double *dP, double *dJ, double *dK, cudaStream_t st)
+// the launches of one J/K pass (zeroing of J and K included)
+static int jk_body(Handle *h, const double *dP, double *dJ, double *dK, cudaStream_t st)
 {
     CK(h, cudaMemsetAsync(dJ, 0, sizeof(double) * h->nfuc * h->nbas, st));
     CK(h, cudaMemsetAsync(dK, 0, sizeof(double) * h->nfuc * h->nbas, st));
-    CK(h, cudaEventRecord(h->ev0, st));
-    if (h->method != TCE_METHOD_FIXED) {
-        int s = lg_jk_passes(h, dP, dJ, dK, st);
-        if (s) return s;
-        CK(h, cudaEventRecord(h->ev1, st));
-        return TCE_OK;
-    }
+    if (h->method != TCE_METHOD_FIXED) return lg_jk_passes(h, dP, dJ, dK, st);
     for (const auto &w : h->lists) {
         if (w.n == 0) continue;
         if (w.kind == 0) {   // every other class: generic kernel
@@ -618,6 +614,55 @@ int direct_jk_device(Handle *h, const double *dP, double *dJ, double *dK, cudaSt
             else CKS(h, tce_launch_quartets_r1(h->S, w.cls, b, st));
         }
     }
+    return TCE_OK;
+}
+
+void drop_graph(Handle *h)
+{
+    if (h->jk_exec) cudaGraphExecDestroy(h->jk_exec);
+    h->jk_exec = nullptr;
+}
+
+// One J/K pass.  With graphs on, the pass is captured once into a CUDA graph
+// (per pointer triple, stream, method and work lists) and replayed as one
+// graph launch per call; the events around it time the whole pass.
+int direct_jk_device(Handle *h, const double *dP, double *dJ, double *dK, cudaStream_t st)
+{
+    if (!h->use_graph) {
+        CK(h, cudaEventRecord(h->ev0, st));
+        int s = jk_body(h, dP, dJ, dK, st);
+        if (s) return s;
+        CK(h, cudaEventRecord(h->ev1, st));
+        return TCE_OK;
+    }
+    const bool same = h->jk_exec && h->g_P == dP && h->g_J == dJ && h->g_K == dK && h->g_st == st &&
+                      h->g_method == h->method && h->g_version == h->work_version;
+    if (!same) {
+        drop_graph(h);
+        cudaGraph_t g = nullptr;
+        CK(h, cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+        int s = jk_body(h, dP, dJ, dK, st);
+        cudaError_t e = cudaStreamEndCapture(st, &g);
+        if (s) {
+            if (g) cudaGraphDestroy(g);
+            return s;
+        }
+        if (e != cudaSuccess) return fail(h, TCE_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&h->jk_exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            h->jk_exec = nullptr;
+            return fail(h, TCE_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+        }
+        h->g_P = dP;
+        h->g_J = dJ;
+        h->g_K = dK;
+        h->g_st = st;
+        h->g_method = h->method;
+        h->g_version = h->work_version;
+    }
+    CK(h, cudaEventRecord(h->ev0, st));
+    CK(h, cudaGraphLaunch(h->jk_exec, st));
     CK(h, cudaEventRecord(h->ev1, st));
     return TCE_OK;
 }
@@ -663,6 +708,7 @@ int tce_destroy(void *handle)
     Handle *h = static_cast<Handle *>(handle);
     if (!h) return TCE_OK;
     if (h->st) cudaStreamSynchronize(h->st);
+    drop_graph(h);
     for (void *p : h->allocs) cudaFree(p);
     if (h->st) cudaStreamDestroy(h->st);
     if (h->ev0) cudaEventDestroy(h->ev0);
@@ -727,6 +773,15 @@ int tce_set_shard(void *handle, int32_t rank, int32_t nranks)
     return TCE_OK;
 }
 
+int tce_set_graph(void *handle, int32_t on)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h) return fail(h, TCE_ERR_ARG, "NULL handle");
+    h->use_graph = on ? 1 : 0;
+    if (!on) drop_graph(h);
+    return TCE_OK;
+}
+
 int tce_fp64_peak(double *tflops)
 {
     if (!tflops) return fail(nullptr, TCE_ERR_ARG, "NULL argument");
@@ -779,6 +834,49 @@ int tce_schwarz(void *handle, double *Q)
     Handle *h = static_cast<Handle *>(handle);
     if (!h || !Q) return fail(h, TCE_ERR_ARG, "NULL argument");
     std::memcpy(Q, h->Q.data(), h->Q.size() * sizeof(double));
+    return TCE_OK;
+}
+
+// Start-up accuracy gate of the fixed rule (fast_quad_self_check,
+// fast_quad_self_check.f90:30-233, ERI part): the on-site quartets
+// (SI SI|SI SI) of the unit cell plus 50 pseudo-random quartets drawn with the
+// reference's generator (seed 12345, x <- (1103515245 x + 12345) mod 2^31,
+// value x/16), each evaluated with the prefactor screens only on `fast` (the
+// 32/40-node rule) and on `full` (the 64/128-point table) of the same system.
+int tce_quad_self_check(void *fast, void *full, double *dmax, int32_t *nsample)
+{
+    Handle *hf = static_cast<Handle *>(fast), *hF = static_cast<Handle *>(full);
+    if (!hf || !hF || !dmax) return fail(hf, TCE_ERR_ARG, "NULL argument");
+    if (hf->nsh != hF->nsh || hf->nshuc != hF->nshuc || hf->nbas != hF->nbas)
+        return fail(hf, TCE_ERR_ARG, "the two handles describe different systems");
+    const int nshuc = std::max(hf->nshuc, 1), nsh = hf->nsh, nrand = 50;
+    long long seed = 12345;
+    auto next = [&]() {
+        seed = (seed * 1103515245LL + 12345LL) % 2147483648LL;
+        return seed / 16;
+    };
+    std::vector<int4> items;
+    for (int it = 0; it < nshuc + nrand; ++it) {
+        if (it < nshuc) {
+            items.push_back(make_int4(it, it, it, it));
+        } else {
+            const int a = (int)(next() % nshuc);
+            const int b = (int)(next() % nsh);
+            const int c = (int)(next() % nsh);
+            const int d = (int)(next() % nsh);
+            items.push_back(make_int4(a, b, c, d));
+        }
+    }
+    std::vector<double> b1, b2;
+    std::vector<long long> o1, o2;
+    int s = run_blocks(hf, items, nullptr, TCE_MODE_BLOCK, 0, &b1, &o1);
+    if (s) return s;
+    s = run_blocks(hF, items, nullptr, TCE_MODE_BLOCK, 0, &b2, &o2);
+    if (s) return fail(hf, s, "full-table blocks: " + hF->err);
+    double m = 0.0;
+    for (size_t i = 0; i < b1.size() && i < b2.size(); ++i) m = std::max(m, std::fabs(b1[i] - b2[i]));
+    *dmax = m;
+    if (nsample) *nsample = (int32_t)items.size();
     return TCE_OK;
 }
 

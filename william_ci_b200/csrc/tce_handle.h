@@ -77,9 +77,11 @@ struct Handle {
     // learned-grid work, one list per kernel and rule size: kind 0 generic
     // (k_quartets), 1 all-s (k_quartets_s), 2 one-periodic-direction s/p class
     // `cls` (k_quartets_r1); nq = 32 or 64 padded rule nodes
-    struct LgList { int kind, cls, nq; int4 *d = nullptr; int *rule = nullptr; long long n = 0; };
+    struct LgList { int kind, cls, nq, fp32; int4 *d = nullptr; int *rule = nullptr; long long n = 0; };
     std::vector<LgList> lg_lists;
-    long long n_lg = 0;
+    long long n_lg = 0, n_fp32 = 0;
+    double fp32_thr = 0.0;               // FP32 node sums below this Schwarz product (0: off)
+    float *d_rule_T32 = nullptr;         // FP32 copy of the rule T tables
     int4 *d_plain_items = nullptr;
     long long n_plain_direct = 0;
     int4 *d_fb_items = nullptr;
@@ -93,6 +95,15 @@ struct Handle {
     unsigned long long *d_node_evals = nullptr;
     unsigned int *d_next2 = nullptr;     // work counter of the second kernel of a pass
     unsigned int *d_next3 = nullptr;
+    // CUDA graph of the J/K pass (tce_set_graph); rebuilt when any key changes
+    int use_graph = 0;
+    long long work_version = 0;          // bumped whenever work lists are rebuilt
+    cudaGraphExec_t jk_exec = nullptr;
+    const double *g_P = nullptr;
+    double *g_J = nullptr, *g_K = nullptr;
+    cudaStream_t g_st = nullptr;
+    int g_method = -1;
+    long long g_version = -1;
 };
 
 extern thread_local std::string g_err;
@@ -149,6 +160,7 @@ int shift_to(const Handle *h, int idx, int refcell, int nblk);
 int ncomb_of(const Handle *h, int SI, int SJ, int SK, int SL);
 int make_lists(Handle *h, const std::vector<int4> &items);
 int direct_jk_device(Handle *h, const double *dP, double *dJ, double *dK, cudaStream_t st);
+void drop_graph(Handle *h);
 // learned-grid / plain passes of direct_jk_device (tce_lg.cu)
 int lg_jk_passes(Handle *h, const double *dP, double *dJ, double *dK, cudaStream_t st);
 int lg_rebuild_lists(Handle *h);

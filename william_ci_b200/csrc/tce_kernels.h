@@ -71,6 +71,7 @@ struct SArgsHost {
     const int *item_rule = nullptr;
     const RuleDev *rules = nullptr;
     const double *rule_T = nullptr, *rule_t = nullptr, *rule_wk = nullptr, *rule_wg = nullptr;
+    const float *rule_T32 = nullptr;
     double judge_tol = 1e-10;
     int4 *fb_items = nullptr;
     unsigned int *fb_count = nullptr;
@@ -78,9 +79,10 @@ struct SArgsHost {
 int tce_launch_quartets_s(const DevSys &S, const SArgsHost &h, cudaStream_t st);
 // 1D s/p classes (k_quartets_r1); cls bit i = angular momentum (0/1) of shell i
 int tce_launch_quartets_r1(const DevSys &S, int cls, const SArgsHost &h, cudaStream_t st);
-// the same kernels with per-item learned-grid rules of nq = 32 or 64 padded nodes
-int tce_launch_quartets_s_lg(const DevSys &S, const SArgsHost &h, int nq, cudaStream_t st);
-int tce_launch_quartets_r1_lg(const DevSys &S, int cls, const SArgsHost &h, int nq, cudaStream_t st);
+// the same kernels with per-item learned-grid rules of nq = 32 or 64 padded
+// nodes; fp32: FP32 node sums (one periodic direction only)
+int tce_launch_quartets_s_lg(const DevSys &S, const SArgsHost &h, int nq, bool fp32, cudaStream_t st);
+int tce_launch_quartets_r1_lg(const DevSys &S, int cls, const SArgsHost &h, int nq, bool fp32, cudaStream_t st);
 inline bool tce_r1_supported(int ndp, int nq, int cls)
 {
     return ndp == 1 && nq == 32 && cls >= 0 && cls < 16 && __builtin_popcount(cls) == 1;

@@ -32,12 +32,12 @@ int tce_launch_quartets_r1(const DevSys &S, int cls, const SArgsHost &h, cudaStr
     int nsm = h.num_sms > 0 ? h.num_sms : 148;
 #define TCE_R1(NQv, a, b, c, d)                                                                                   \
     do {                                                                                                          \
-        cudaFuncSetAttribute(k_quartets_r1<NQv, a, b, c, d, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,      \
+        cudaFuncSetAttribute(k_quartets_r1<NQv, a, b, c, d, false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,      \
                              (int)smem);                                                                          \
         int per = 0;                                                                                              \
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_quartets_r1<NQv, a, b, c, d, false>, 256, smem);    \
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_quartets_r1<NQv, a, b, c, d, false, double>, 256, smem);    \
         if (per < 1) per = 1;                                                                                     \
-        k_quartets_r1<NQv, a, b, c, d, false><<<nsm * per, 256, smem, st>>>(S, A);                                \
+        k_quartets_r1<NQv, a, b, c, d, false, double><<<nsm * per, 256, smem, st>>>(S, A);                                \
     } while (0)
 #define TCE_R1_CLS(NQv)                                                                                            \
     switch (cls) {                                                                                                 \
@@ -80,12 +80,12 @@ int tce_launch_quartets_s(const DevSys &S, const SArgsHost &h, cudaStream_t st)
     int nsm = h.num_sms > 0 ? h.num_sms : 148;
 #define TCE_LAUNCH_S(NQv, NDPv)                                                                             \
     do {                                                                                                    \
-        cudaFuncSetAttribute(k_quartets_s<NQv, NDPv, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+        cudaFuncSetAttribute(k_quartets_s<NQv, NDPv, false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
                              (int)smem);                                                                    \
         int per = 0;                                                                                        \
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_quartets_s<NQv, NDPv, false>, 256, smem);     \
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_quartets_s<NQv, NDPv, false, double>, 256, smem);     \
         if (per < 1) per = 1;                                                                               \
-        k_quartets_s<NQv, NDPv, false><<<nsm * per, 256, smem, st>>>(S, A);                                 \
+        k_quartets_s<NQv, NDPv, false, double><<<nsm * per, 256, smem, st>>>(S, A);                                 \
     } while (0)
     if (S.nq == 32) {
         if (S.ndp == 1) TCE_LAUNCH_S(32, 1);

@@ -10,8 +10,14 @@
 // estimate, as block_judge of the generic kernel) either scatters the block or
 // queues the quartet for the plain method.
 // Instantiated in tce_kernels_s.cu (system rule) and tce_kernels_slg.cu
-// (learned grid).
+// (learned grid).  AT = float gives the FP32-panel variant: the node sums of
+// the periodic direction (the F_n x T[n][k] accumulation) in FP32 with an FP32
+// copy of the rule's T table; phases, Bessel vectors, the real directions,
+// the weights and the J/K accumulation stay FP64.  It is used for quartets
+// whose Schwarz bound is below the FP32 threshold.
 #pragma once
+#include <type_traits>
+
 #include "tce_device.cuh"
 #include "tce_kernels.h"
 
@@ -50,6 +56,7 @@ struct SArgs {
     const int *item_rule;
     const RuleDev *rules;
     const double *rule_T, *rule_t, *rule_wk, *rule_wg;
+    const float *rule_T32;    // FP32 copy of rule_T (FP32-panel instantiations)
     double judge_tol;
     int4 *fb_items;
     unsigned int *fb_count;
@@ -62,8 +69,8 @@ __device__ __forceinline__ void tce_queue_fallback(const SArgs &A, int4 q)
     A.fb_items[slot] = q;
 }
 
-template <int NQ, int NDP, bool LG>
-__global__ void __launch_bounds__(256, (NQ == 32 && NDP == 1) ? 2 : 1) k_quartets_s(DevSys S, SArgs A)
+template <int NQ, int NDP, bool LG, typename AT>
+__global__ void __launch_bounds__(256, NDP == 1 ? 2 : 1) k_quartets_s(DevSys S, SArgs A)
 {
     constexpr int NG = NQ / 8;
     extern __shared__ double smem[];
@@ -93,10 +100,12 @@ __global__ void __launch_bounds__(256, (NQ == 32 && NDP == 1) ? 2 : 1) k_quartet
         const int4 q = A.items[it];
         // the quadrature rule of this quartet
         const double *Tg = nullptr, *tn = S.tnode, *wk = S.tweight, *wg = nullptr;
+        const float *Tg32 = nullptr;
         const int *gm = nullptr;
         if (LG) {
             const RuleDev *D = A.rules + A.item_rule[it];
             Tg = A.rule_T + D->T_off;
+            if (std::is_same<AT, float>::value) Tg32 = A.rule_T32 + D->T_off;
             gm = D->gmax;
             tn = A.rule_t + D->node_off;
             wk = A.rule_wk + D->node_off;
@@ -164,17 +173,23 @@ __global__ void __launch_bounds__(256, (NQ == 32 && NDP == 1) ? 2 : 1) k_quartet
                             const int nm = Pb.N[d] < Pk.N[d] ? Pb.N[d] : Pk.N[d];
                             const double phi = S.a[d] * (Pb.cen[d] - (Pk.cen[d] + Tsh[d]));
                             const double cphi = cos(phi), two_c = 2.0 * cphi;
-                            double acc[NQ];
+                            double R2 = 0.0;   // NDP == 1: both real directions at once
+                            if (NDP == 1) {
 #pragma unroll
-                            for (int k = 0; k < NQ; ++k) acc[k] = 0.0;
-                            double cn = 1.0, cprev = cphi;        // cos(n phi), cos((n-1) phi) at n = 0
-                            double gN = __ldg(G), hN = __ldg(H);  // values of row n (prefetched)
-                            int n = 0;
+                                for (int dd = 1; dd < 3; ++dd) {
+                                    double R = Pb.cen[dd] - (Pk.cen[dd] + Tsh[dd]);
+                                    R2 += R * R;
+                                }
+                            }
+                            // node passes of up to 32 nodes: 32 accumulators, folded at the end of each pass
 #pragma unroll
                             for (int g0 = 0; g0 < NG; g0 += 4) {
-                                if (g0 > 0) {   // second pass over nodes (NQ > 32): restart n
-                                    n = 0; cn = 1.0; cprev = cphi; gN = __ldg(G); hN = __ldg(H);
-                                }
+                                AT acc[32];
+#pragma unroll
+                                for (int k = 0; k < 32; ++k) acc[k] = (AT)0;
+                                double cn = 1.0, cprev = cphi;        // cos(n phi), cos((n-1) phi) at n = 0
+                                double gN = __ldg(G), hN = __ldg(H);  // values of row n (prefetched)
+                                int n = 0;
 #pragma unroll
                                 for (int sgm = 0; sgm < 4; ++sgm) {
                                     if (g0 + sgm >= NG) break;
@@ -195,51 +210,58 @@ __global__ void __launch_bounds__(256, (NQ == 32 && NDP == 1) ? 2 : 1) k_quartet
 #pragma unroll
                                         for (int g = 0; g < 4; ++g) {
                                             if (g >= sgm && g0 + g < NG) {
-                                                const double *Tr =
-                                                    LG ? Tg + ((size_t)d * (S.ncap + 1) + n) * NQ + 8 * (g0 + g)
-                                                       : (A.t_smem ? Tsm + A.tsoff[d][g0 + g] + 8 * n
-                                                                   : S.Tt + ((size_t)d * (S.ncap + 1) + n) * NQ + 8 * (g0 + g));
-                                                const double2 *T2 = reinterpret_cast<const double2 *>(Tr);
+                                                if constexpr (std::is_same<AT, float>::value) {
+                                                    const float4 *T4 = reinterpret_cast<const float4 *>(
+                                                        Tg32 + ((size_t)d * (S.ncap + 1) + n) * NQ + 8 * (g0 + g));
+                                                    const float Ff = (float)F;
 #pragma unroll
-                                                for (int kk = 0; kk < 4; ++kk) {
-                                                    const double2 t = T2[kk];
-                                                    acc[8 * (g0 + g) + 2 * kk] = fma(F, t.x, acc[8 * (g0 + g) + 2 * kk]);
-                                                    acc[8 * (g0 + g) + 2 * kk + 1] = fma(F, t.y, acc[8 * (g0 + g) + 2 * kk + 1]);
+                                                    for (int kk = 0; kk < 2; ++kk) {
+                                                        const float4 t = T4[kk];
+                                                        acc[8 * g + 4 * kk] = fmaf(Ff, t.x, acc[8 * g + 4 * kk]);
+                                                        acc[8 * g + 4 * kk + 1] = fmaf(Ff, t.y, acc[8 * g + 4 * kk + 1]);
+                                                        acc[8 * g + 4 * kk + 2] = fmaf(Ff, t.z, acc[8 * g + 4 * kk + 2]);
+                                                        acc[8 * g + 4 * kk + 3] = fmaf(Ff, t.w, acc[8 * g + 4 * kk + 3]);
+                                                    }
+                                                } else {
+                                                    const double *Tr =
+                                                        LG ? Tg + ((size_t)d * (S.ncap + 1) + n) * NQ + 8 * (g0 + g)
+                                                           : (A.t_smem ? Tsm + A.tsoff[d][g0 + g] + 8 * n
+                                                                       : S.Tt + ((size_t)d * (S.ncap + 1) + n) * NQ + 8 * (g0 + g));
+                                                    const double2 *T2 = reinterpret_cast<const double2 *>(Tr);
+#pragma unroll
+                                                    for (int kk = 0; kk < 4; ++kk) {
+                                                        const double2 t = T2[kk];
+                                                        acc[8 * g + 2 * kk] = fma(F, t.x, acc[8 * g + 2 * kk]);
+                                                        acc[8 * g + 2 * kk + 1] = fma(F, t.y, acc[8 * g + 2 * kk + 1]);
+                                                    }
                                                 }
                                             }
                                         }
                                     }
                                 }
-                            }
-                            if (NDP == 1) {
-                                // one periodic direction: weights and both real directions at once
-                                const double p = Pb.esum, qq = Pk.esum, pq_ = p * qq, ps = p + qq;
-                                double R2 = 0.0;
+                                // fold the pass's nodes k = 8 g0 + x
 #pragma unroll
-                                for (int dd = 1; dd < 3; ++dd) {
-                                    double R = Pb.cen[dd] - (Pk.cen[dd] + Tsh[dd]);
-                                    R2 += R * R;
-                                }
-#pragma unroll
-                                for (int k = 0; k < NQ; ++k) {
-                                    const double t2 = tn[k] * tn[k];
-                                    const double D2 = 1.0 / (pq_ + ps * t2);
-                                    const double e = (R2 == 0.0) ? 1.0 : exp(-(pq_ * t2 * D2) * R2);
-                                    if (LG) {
-                                        const double base = acc[k] * (PI2 * D2 * e);
-                                        val = fma(base, wk[k], val);
-                                        valG = fma(base, wg[k], valG);
+                                for (int x = 0; x < 32; ++x) {
+                                    const int k = 8 * g0 + x;
+                                    if (k >= NQ) break;
+                                    if (NDP == 1) {
+                                        const double p = Pb.esum, qq = Pk.esum, pq_ = p * qq, ps = p + qq;
+                                        const double t2 = tn[k] * tn[k];
+                                        const double D2 = 1.0 / (pq_ + ps * t2);
+                                        const double e = (R2 == 0.0) ? 1.0 : exp(-(pq_ * t2 * D2) * R2);
+                                        if (LG) {
+                                            const double base = (double)acc[x] * (PI2 * D2 * e);
+                                            val = fma(base, wk[k], val);
+                                            valG = fma(base, wg[k], valG);
+                                        } else {
+                                            val = fma((double)acc[x], S.tweight[k] * PI2 * D2 * e, val);
+                                        }
+                                    } else if (d == 0) {
+                                        prod[k < (NDP > 1 ? NQ : 1) ? k : 0] = LG ? (double)acc[x] : (double)acc[x] * S.tweight[k];
                                     } else {
-                                        val = fma(acc[k], S.tweight[k] * PI2 * D2 * e, val);
+                                        prod[k < (NDP > 1 ? NQ : 1) ? k : 0] *= (double)acc[x];
                                     }
                                 }
-                            } else if (d == 0) {
-#pragma unroll
-                                for (int k = 0; k < NQ; ++k)
-                                    prod[k < (NDP > 1 ? NQ : 1) ? k : 0] = LG ? acc[k] : acc[k] * S.tweight[k];
-                            } else {
-#pragma unroll
-                                for (int k = 0; k < NQ; ++k) prod[k < (NDP > 1 ? NQ : 1) ? k : 0] *= acc[k];
                             }
                         }
                         if (NDP == 2) {
@@ -321,8 +343,8 @@ __host__ __device__ constexpr int tce_eoff(int LJ, int i, int j)
 }
 __host__ __device__ constexpr int tce_ecount(int LI, int LJ) { return tce_eoff(LJ, LI, LJ) + LI + LJ + 1; }
 
-template <int NQ, int LA, int LB, int LC, int LD, bool LG>
-__global__ void __launch_bounds__(256, 1) k_quartets_r1(DevSys S, SArgs A)
+template <int NQ, int LA, int LB, int LC, int LD, bool LG, typename AT>
+__global__ void __launch_bounds__(256, LG ? 2 : 1) k_quartets_r1(DevSys S, SArgs A)
 {
     constexpr int NG = NQ / 8;
     constexpr int NA = LA == 0 ? 1 : 3, NB = LB == 0 ? 1 : 3, NC = LC == 0 ? 1 : 3, ND = LD == 0 ? 1 : 3;
@@ -352,10 +374,12 @@ __global__ void __launch_bounds__(256, 1) k_quartets_r1(DevSys S, SArgs A)
         if (it >= A.nitems) break;
         const int4 q = A.items[it];
         const double *Tg = nullptr, *tn = S.tnode, *wk = S.tweight, *wg = nullptr;
+        const float *Tg32 = nullptr;
         const int *gm = nullptr;
         if (LG) {
             const RuleDev *D = A.rules + A.item_rule[it];
             Tg = A.rule_T + D->T_off;
+            if (std::is_same<AT, float>::value) Tg32 = A.rule_T32 + D->T_off;
             gm = D->gmax;
             tn = A.rule_t + D->node_off;
             wk = A.rule_wk + D->node_off;
@@ -445,10 +469,11 @@ __global__ void __launch_bounds__(256, 1) k_quartets_r1(DevSys S, SArgs A)
                         for (int c = 0; c < NCQ; ++c) val[c] = 0.0;
 #pragma unroll
                         for (int c = 0; c < (LG ? NCQ : 1); ++c) valG[c] = 0.0;
+                        // node passes of up to 32 nodes (32 accumulators per power combination)
+#pragma unroll
+                        for (int g0 = 0; g0 < NG; g0 += 4) {
 #pragma unroll
                         for (int cmb = 0; cmb < NCOMB; ++cmb) {
-                            constexpr int dummy = 0;
-                            (void)dummy;
                             const int ia = cmb % (LA + 1), ib = (cmb / (LA + 1)) % (LB + 1);
                             const int ic = (cmb / ((LA + 1) * (LB + 1))) % (LC + 1);
                             const int id = cmb / ((LA + 1) * (LB + 1) * (LC + 1));
@@ -457,15 +482,16 @@ __global__ void __launch_bounds__(256, 1) k_quartets_r1(DevSys S, SArgs A)
                                                ((((long long)0 * (LA + 1) + ia) * (LB + 1) + ib) * 2 + 0) * Ub.Nlen * nppb + pq.x;
                             const double2 *H = S.vec + Uk.vec_off +
                                                ((((long long)0 * (LC + 1) + ic) * (LD + 1) + id) * 2 + 1) * Uk.Nlen * nppk + pq.y;
-                            double acc[NQ];
+                            AT acc[32];
 #pragma unroll
-                            for (int k = 0; k < NQ; ++k) acc[k] = 0.0;
+                            for (int k = 0; k < 32; ++k) acc[k] = (AT)0;
                             double cn = 1.0, sn = 0.0;
                             double2 gN = __ldg(G), hN = __ldg(H);
                             int n = 0;
 #pragma unroll
-                            for (int sgm = 0; sgm < NG; ++sgm) {
-                                int nend = LG ? gm[sgm] : S.gmax[0][sgm];
+                            for (int sgm = 0; sgm < 4; ++sgm) {
+                                if (g0 + sgm >= NG) break;
+                                int nend = LG ? gm[g0 + sgm] : S.gmax[0][g0 + sgm];
                                 nend = nend < nm ? nend : nm;
                                 for (; n <= nend; ++n) {
                                     const double2 gv = gN, hv = hN;
@@ -488,25 +514,42 @@ __global__ void __launch_bounds__(256, 1) k_quartets_r1(DevSys S, SArgs A)
                                         cn = t;
                                     }
 #pragma unroll
-                                    for (int g = 0; g < NG; ++g) {
-                                        if (g >= sgm) {
-                                            const double2 *T2 = reinterpret_cast<const double2 *>(
-                                                LG ? Tg + (size_t)n * NQ + 8 * g
-                                                   : (A.t_smem ? Tsm + A.tsoff[0][g] + 8 * n : S.Tt + (size_t)n * NQ + 8 * g));
+                                    for (int g = 0; g < 4; ++g) {
+                                        if (g >= sgm && g0 + g < NG) {
+                                            if constexpr (std::is_same<AT, float>::value) {
+                                                const float4 *T4 =
+                                                    reinterpret_cast<const float4 *>(Tg32 + (size_t)n * NQ + 8 * (g0 + g));
+                                                const float Ff = (float)F;
 #pragma unroll
-                                            for (int kk = 0; kk < 4; ++kk) {
-                                                const double2 t = T2[kk];
-                                                acc[8 * g + 2 * kk] = fma(F, t.x, acc[8 * g + 2 * kk]);
-                                                acc[8 * g + 2 * kk + 1] = fma(F, t.y, acc[8 * g + 2 * kk + 1]);
+                                                for (int kk = 0; kk < 2; ++kk) {
+                                                    const float4 t = T4[kk];
+                                                    acc[8 * g + 4 * kk] = fmaf(Ff, t.x, acc[8 * g + 4 * kk]);
+                                                    acc[8 * g + 4 * kk + 1] = fmaf(Ff, t.y, acc[8 * g + 4 * kk + 1]);
+                                                    acc[8 * g + 4 * kk + 2] = fmaf(Ff, t.z, acc[8 * g + 4 * kk + 2]);
+                                                    acc[8 * g + 4 * kk + 3] = fmaf(Ff, t.w, acc[8 * g + 4 * kk + 3]);
+                                                }
+                                            } else {
+                                                const double2 *T2 = reinterpret_cast<const double2 *>(
+                                                    LG ? Tg + (size_t)n * NQ + 8 * (g0 + g)
+                                                       : (A.t_smem ? Tsm + A.tsoff[0][g0 + g] + 8 * n
+                                                                   : S.Tt + (size_t)n * NQ + 8 * (g0 + g)));
+#pragma unroll
+                                                for (int kk = 0; kk < 4; ++kk) {
+                                                    const double2 t = T2[kk];
+                                                    acc[8 * g + 2 * kk] = fma(F, t.x, acc[8 * g + 2 * kk]);
+                                                    acc[8 * g + 2 * kk + 1] = fma(F, t.y, acc[8 * g + 2 * kk + 1]);
+                                                }
                                             }
                                         }
                                     }
                                 }
                             }
                             const double sgn = (ia + ib + ic + id) == 0 ? 1.0 : pow(S.a[0], -(double)(ia + ib + ic + id));
-                            // components whose x powers are this combination
+                            // components whose x powers are this combination, nodes k = 8 g0 + x
 #pragma unroll
-                            for (int k = 0; k < NQ; ++k) {
+                            for (int x = 0; x < 32; ++x) {
+                                const int k = 8 * g0 + x;
+                                if (k >= NQ) break;
                                 const double t2 = tn[k] * tn[k];
                                 const double D2 = 1.0 / (pq_ + ps * t2);
                                 const double w = pq_ * t2 * D2, rs = PI_D * sqrt(D2);
@@ -518,8 +561,8 @@ __global__ void __launch_bounds__(256, 1) k_quartets_r1(DevSys S, SArgs A)
                                     gy[m + 1] = 2.0 * w * Ry * gy[m] - (m > 0 ? 2.0 * m * w * gy[m - 1] : 0.0);
                                     gz[m + 1] = 2.0 * w * Rz * gz[m] - (m > 0 ? 2.0 * m * w * gz[m - 1] : 0.0);
                                 }
-                                const double xk = acc[k] * sgn * wk[k];
-                                const double xkG = LG ? acc[k] * sgn * wg[k] : 0.0;
+                                const double xk = (double)acc[x] * sgn * wk[k];
+                                const double xkG = LG ? (double)acc[x] * sgn * wg[k] : 0.0;
 #pragma unroll
                                 for (int c = 0; c < NCQ; ++c) {
                                     const int ca = c % NA, cb = (c / NA) % NB, cc = (c / (NA * NB)) % NC, cd = c / (NA * NB * NC);
@@ -546,6 +589,7 @@ __global__ void __launch_bounds__(256, 1) k_quartets_r1(DevSys S, SArgs A)
                                     if (LG) valG[LG ? c : 0] = fma(xkG, I[0] * I[1], valG[LG ? c : 0]);
                                 }
                             }
+                        }
                         }
                         const double fac = qfac[lane];
 #pragma unroll

@@ -21,6 +21,7 @@ static void lg_args(SArgs &A, const SArgsHost &h)
     A.rule_t = h.rule_t;
     A.rule_wk = h.rule_wk;
     A.rule_wg = h.rule_wg;
+    A.rule_T32 = h.rule_T32;
     A.judge_tol = h.judge_tol;
     A.fb_items = h.fb_items;
     A.fb_count = h.fb_count;
@@ -37,47 +38,61 @@ static void launch(Kern k, const DevSys &S, const SArgs &A, int nsm, cudaStream_
     k<<<nsm * per, 256, smem, st>>>(S, A);
 }
 
-int tce_launch_quartets_s_lg(const DevSys &S, const SArgsHost &h, int nq, cudaStream_t st)
+int tce_launch_quartets_s_lg(const DevSys &S, const SArgsHost &h, int nq, bool fp32, cudaStream_t st)
 {
     if (!h.item_rule || !h.rules || !h.rule_T || !h.fb_items || !h.fb_count) return TCE_ERR_ARG;
+    if (fp32 && (!h.rule_T32 || S.ndp != 1)) return TCE_ERR_UNSUPPORTED;
     SArgs A{};
     lg_args(A, h);
     cudaMemsetAsync(h.next, 0, sizeof(unsigned int), st);
     const int nsm = h.num_sms > 0 ? h.num_sms : 148;
-    if (nq == 32) {
-        if (S.ndp == 1) launch(k_quartets_s<32, 1, true>, S, A, nsm, st);
-        else if (S.ndp == 2) launch(k_quartets_s<32, 2, true>, S, A, nsm, st);
-        else launch(k_quartets_s<32, 3, true>, S, A, nsm, st);
+    if (fp32) {
+        if (nq == 32) launch(k_quartets_s<32, 1, true, float>, S, A, nsm, st);
+        else if (nq == 64) launch(k_quartets_s<64, 1, true, float>, S, A, nsm, st);
+        else return TCE_ERR_UNSUPPORTED;
+    } else if (nq == 32) {
+        if (S.ndp == 1) launch(k_quartets_s<32, 1, true, double>, S, A, nsm, st);
+        else if (S.ndp == 2) launch(k_quartets_s<32, 2, true, double>, S, A, nsm, st);
+        else launch(k_quartets_s<32, 3, true, double>, S, A, nsm, st);
     } else if (nq == 64) {
-        if (S.ndp == 1) launch(k_quartets_s<64, 1, true>, S, A, nsm, st);
-        else if (S.ndp == 2) launch(k_quartets_s<64, 2, true>, S, A, nsm, st);
-        else launch(k_quartets_s<64, 3, true>, S, A, nsm, st);
+        if (S.ndp == 1) launch(k_quartets_s<64, 1, true, double>, S, A, nsm, st);
+        else if (S.ndp == 2) launch(k_quartets_s<64, 2, true, double>, S, A, nsm, st);
+        else launch(k_quartets_s<64, 3, true, double>, S, A, nsm, st);
     } else {
         return TCE_ERR_UNSUPPORTED;
     }
     return cudaGetLastError() == cudaSuccess ? TCE_OK : TCE_ERR_CUDA;
 }
 
-int tce_launch_quartets_r1_lg(const DevSys &S, int cls, const SArgsHost &h, int nq, cudaStream_t st)
+int tce_launch_quartets_r1_lg(const DevSys &S, int cls, const SArgsHost &h, int nq, bool fp32, cudaStream_t st)
 {
     if (!h.item_rule || !h.rules || !h.rule_T || !h.fb_items || !h.fb_count) return TCE_ERR_ARG;
     if (S.ndp != 1 || (nq != 32 && nq != 64)) return TCE_ERR_UNSUPPORTED;
+    if (fp32 && !h.rule_T32) return TCE_ERR_UNSUPPORTED;
     SArgs A{};
     lg_args(A, h);
     cudaMemsetAsync(h.next, 0, sizeof(unsigned int), st);
     const int nsm = h.num_sms > 0 ? h.num_sms : 148;
-#define TCE_R1_LG(NQv)                                                                              \
+#define TCE_R1_LG(NQv, AT)                                                                          \
     switch (cls) {                                                                                  \
-    case 1: launch(k_quartets_r1<NQv, 1, 0, 0, 0, true>, S, A, nsm, st); break;                     \
-    case 2: launch(k_quartets_r1<NQv, 0, 1, 0, 0, true>, S, A, nsm, st); break;                     \
-    case 4: launch(k_quartets_r1<NQv, 0, 0, 1, 0, true>, S, A, nsm, st); break;                     \
-    case 8: launch(k_quartets_r1<NQv, 0, 0, 0, 1, true>, S, A, nsm, st); break;                     \
+    case 1: launch(k_quartets_r1<NQv, 1, 0, 0, 0, true, AT>, S, A, nsm, st); break;                 \
+    case 2: launch(k_quartets_r1<NQv, 0, 1, 0, 0, true, AT>, S, A, nsm, st); break;                 \
+    case 4: launch(k_quartets_r1<NQv, 0, 0, 1, 0, true, AT>, S, A, nsm, st); break;                 \
+    case 8: launch(k_quartets_r1<NQv, 0, 0, 0, 1, true, AT>, S, A, nsm, st); break;                 \
     default: return TCE_ERR_UNSUPPORTED;                                                            \
     }
     if (nq == 32) {
-        TCE_R1_LG(32)
+        if (fp32) {
+            TCE_R1_LG(32, float)
+        } else {
+            TCE_R1_LG(32, double)
+        }
     } else {
-        TCE_R1_LG(64)
+        if (fp32) {
+            TCE_R1_LG(64, float)
+        } else {
+            TCE_R1_LG(64, double)
+        }
     }
 #undef TCE_R1_LG
     return cudaGetLastError() == cudaSuccess ? TCE_OK : TCE_ERR_CUDA;

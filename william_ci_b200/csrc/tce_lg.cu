@@ -222,6 +222,12 @@ __global__ void k_choose_rule(const float *Z, long long n, int nrules, const flo
 
 static inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
+__global__ void k_to_float(const double *x, long long n, float *y)
+{
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = (float)x[i];
+}
+
 // ============================================================================
 // MLP host object
 // ============================================================================
@@ -412,6 +418,7 @@ static void fill_common(Handle *h, QuartetHostArgs &a)
 int lg_rebuild_lists(Handle *h)
 {
     int s;
+    ++h->work_version;
     dfree(h, h->d_shard_items);
     h->d_shard_items = nullptr;
     std::vector<int4> mine;
@@ -428,32 +435,40 @@ int lg_rebuild_lists(Handle *h)
     h->d_plain_items = h->d_fb_items = nullptr;
     h->n_lg = h->n_plain_direct = 0;
     if (h->item_rule.size() != h->items_host.size() || h->lg_nrules == 0) return TCE_OK;
-    // key = (kind * 16 + cls) * 2 + (nq == 64)
-    std::vector<std::vector<int4>> lg(3 * 16 * 2);
-    std::vector<std::vector<int>> rl(3 * 16 * 2);
+    // key = ((kind * 16 + cls) * 2 + (nq == 64)) * 2 + fp32; FP32 node sums for the
+    // register kernels of one periodic direction when the shell-pair Schwarz
+    // product is below fp32_thr
+    std::vector<std::vector<int4>> lg(3 * 16 * 4);
+    std::vector<std::vector<int>> rl(3 * 16 * 4);
     std::vector<int4> pl;
+    h->n_fp32 = 0;
     for (long long i : h->shard_idx) {
         const int r = h->item_rule[(size_t)i];
         const int4 &q = h->items_host[(size_t)i];
         if (r >= 0 && r < h->lg_nrules) {
-            const int key = lg_route(h, q) * 2 + (h->rules_host[r].nq == 64 ? 1 : 0);
+            const int route = lg_route(h, q);
+            const bool f32 = h->fp32_thr > 0.0 && route >= 16 && h->ndp == 1 && h->d_rule_T32 &&
+                             h->Qsh[q.x + (size_t)h->nsh * q.y] * h->Qsh[q.z + (size_t)h->nsh * q.w] < h->fp32_thr;
+            const int key = (route * 2 + (h->rules_host[r].nq == 64 ? 1 : 0)) * 2 + (f32 ? 1 : 0);
             lg[key].push_back(q);
             rl[key].push_back(r);
         } else {
             pl.push_back(q);
         }
     }
-    for (int key = 0; key < 3 * 16 * 2; ++key) {
+    for (int key = 0; key < 3 * 16 * 4; ++key) {
         if (lg[key].empty()) continue;
         Handle::LgList w;
-        w.kind = key / 32;
-        w.cls = (key / 2) % 16;
-        w.nq = (key & 1) ? 64 : 32;
+        w.kind = key / 64;
+        w.cls = (key / 4) % 16;
+        w.nq = ((key / 2) & 1) ? 64 : 32;
+        w.fp32 = key & 1;
         w.n = (long long)lg[key].size();
         if ((s = upload(h, &w.d, lg[key]))) return s;
         if ((s = upload(h, &w.rule, rl[key]))) return s;
         h->lg_lists.push_back(w);
         h->n_lg += w.n;
+        if (w.fp32) h->n_fp32 += w.n;
     }
     if ((s = upload(h, &h->d_plain_items, pl))) return s;
     if ((s = dalloc(h, &h->d_fb_items, (size_t)std::max<long long>(h->n_lg, 1)))) return s;
@@ -516,11 +531,12 @@ int lg_jk_passes(Handle *h, const double *dP, double *dJ, double *dK, cudaStream
             b.rule_t = h->d_rule_t;
             b.rule_wk = h->d_rule_wk;
             b.rule_wg = h->d_rule_wg;
+            b.rule_T32 = h->d_rule_T32;
             b.judge_tol = h->judge_tol;
             b.fb_items = h->d_fb_items;
             b.fb_count = h->d_fb_count;
-            if (w.kind == 1) CKS(h, tce_launch_quartets_s_lg(h->S, b, w.nq, st));
-            else CKS(h, tce_launch_quartets_r1_lg(h->S, w.cls, b, w.nq, st));
+            if (w.kind == 1) CKS(h, tce_launch_quartets_s_lg(h->S, b, w.nq, w.fp32 != 0, st));
+            else CKS(h, tce_launch_quartets_r1_lg(h->S, w.cls, b, w.nq, w.fp32 != 0, st));
         }
     }
     if (h->n_plain_direct > 0) {
@@ -620,9 +636,10 @@ int tce_lg_set_rules(void *handle, int32_t nrules, const int32_t *nn, const doub
         if (nn[r] < 1 || nn[r] > 64) return fail(h, TCE_ERR_ARG, "a rule has 1..64 nodes");
     int s;
     for (void *p : {(void *)h->d_rules, (void *)h->d_rule_T, (void *)h->d_rule_t, (void *)h->d_rule_wk,
-                    (void *)h->d_rule_wg, (void *)h->d_rule_tnmax})
+                    (void *)h->d_rule_wg, (void *)h->d_rule_tnmax, (void *)h->d_rule_T32})
         dfree(h, p);
     h->d_rule_tnmax = nullptr;
+    h->d_rule_T32 = nullptr;
     h->d_rules = nullptr;
     h->d_rule_T = h->d_rule_t = h->d_rule_wk = h->d_rule_wg = nullptr;
     h->lg_nrules = 0;
@@ -672,6 +689,9 @@ int tce_lg_set_rules(void *handle, int32_t nrules, const int32_t *nn, const doub
     }
     dfree(h, tb);
     dfree(h, tn);
+    if ((s = dalloc(h, &h->d_rule_T32, (size_t)Ttot))) return s;
+    k_to_float<<<nblk(Ttot, 256), 256, 0, h->st>>>(h->d_rule_T, Ttot, h->d_rule_T32);
+    CK(h, cudaGetLastError());
     if ((s = upload(h, &h->d_rules, h->rules_host))) return s;
     if ((s = upload(h, &h->d_rule_tnmax, all_tn))) return s;
     h->lg_nrules = nrules;
@@ -720,6 +740,15 @@ int tce_lg_set_item_rules(void *handle, const int32_t *rule)
     return lg_rebuild_lists(h);
 }
 
+int tce_set_fp32_threshold(void *handle, double thr)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h) return fail(h, TCE_ERR_ARG, "NULL handle");
+    if (!(thr >= 0.0) || thr > 1e-3) return fail(h, TCE_ERR_ARG, "threshold must be in [0, 1e-3]");
+    h->fp32_thr = thr;
+    return lg_rebuild_lists(h);
+}
+
 int tce_set_method(void *handle, int32_t method)
 {
     Handle *h = static_cast<Handle *>(handle);
@@ -744,6 +773,7 @@ int tce_set_tolerances(void *handle, double judge_tol, double plain_tol, int32_t
     h->judge_tol = judge_tol;
     h->plain_tol = plain_tol;
     h->plain_max_panels = plain_max_panels;
+    ++h->work_version;
     return TCE_OK;
 }
 
@@ -760,6 +790,7 @@ int tce_lg_stats(void *handle, int64_t *stats)
     stats[1] = fb;
     stats[2] = h->n_plain_direct;
     stats[3] = (int64_t)ev;
+    stats[4] = h->n_fp32;
     return TCE_OK;
 }
 

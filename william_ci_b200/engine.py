@@ -41,7 +41,8 @@ EXPORTS = ["tce_create", "tce_destroy", "tce_last_error", "tce_get_info", "tce_s
            "tce_lg_set_item_rules", "tce_lg_item_rules", "tce_set_method", "tce_set_tolerances", "tce_lg_stats",
            "tce_rule_blocks", "tce_mlp_create", "tce_mlp_destroy", "tce_mlp_last_error", "tce_mlp_nparams",
            "tce_mlp_get_params", "tce_mlp_set_params", "tce_mlp_loss_grad", "tce_mlp_train", "tce_mlp_predict",
-           "tce_lg_predict_rules", "tce_lg_work"]
+           "tce_lg_predict_rules", "tce_lg_work", "tce_quad_self_check", "tce_set_graph",
+           "tce_set_fp32_threshold"]
 
 TCE_METHOD_FIXED, TCE_METHOD_LEARNED, TCE_METHOD_PLAIN = 0, 1, 2
 TCE_NFEAT = 12
@@ -124,6 +125,9 @@ def lib():
         L.tce_mlp_predict.argtypes = [C.c_void_p, C.c_int64, _fp, _fp]
         L.tce_lg_predict_rules.argtypes = [C.c_void_p, C.c_void_p, C.c_double]
         L.tce_lg_work.argtypes = [C.c_void_p, _dp, _lp]
+        L.tce_quad_self_check.argtypes = [C.c_void_p, C.c_void_p, _dp, _ip]
+        L.tce_set_graph.argtypes = [C.c_void_p, C.c_int32]
+        L.tce_set_fp32_threshold.argtypes = [C.c_void_p, C.c_double]
         _lib = L
     return _lib
 
@@ -338,6 +342,10 @@ class Engine:
         _check(lib().tce_lg_work(self.h, C.byref(f), C.byref(n)), self.h)
         return f.value, n.value
 
+    def set_graph(self, on: bool = True):
+        """Capture each J/K pass into a CUDA graph and replay it (tce_set_graph)."""
+        _check(lib().tce_set_graph(self.h, int(bool(on))), self.h)
+
     def set_method(self, method: int):
         _check(lib().tce_set_method(self.h, int(method)), self.h)
 
@@ -345,10 +353,14 @@ class Engine:
         _check(lib().tce_set_tolerances(self.h, float(judge_tol), float(plain_tol), int(plain_max_panels)), self.h)
 
     def lg_stats(self) -> dict:
-        st = np.zeros(4, dtype=np.int64)
+        st = np.zeros(5, dtype=np.int64)
         _check(lib().tce_lg_stats(self.h, st.ctypes.data_as(_lp)), self.h)
         return {"learned": int(st[0]), "rejected": int(st[1]), "plain_direct": int(st[2]),
-                "plain_node_evals": int(st[3])}
+                "plain_node_evals": int(st[3]), "fp32": int(st[4])}
+
+    def set_fp32_threshold(self, thr: float = 1e-6):
+        """FP32 node sums for learned-grid quartets with Schwarz product below thr (0: off)."""
+        _check(lib().tce_set_fp32_threshold(self.h, float(thr)), self.h)
 
     def rule_blocks(self, rule: int, items: np.ndarray, mode: int = 1, judge: bool = False):
         """Blocks of the given shell quartets with one quadrature (rule >= 0 dictionary,
@@ -363,6 +375,16 @@ class Engine:
                                      _d(G) if G is not None else None), self.h)
         offs = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
         return K[:tot], (G[:tot] if G is not None else None), offs
+
+
+def fast_quad_self_check(fast: Engine, full: Engine, tol: float = 1e-10):
+    """fast_quad_self_check (fast_quad_self_check.f90:30-233), ERI part: the
+    largest block difference between the fast-rule and full-table engines on the
+    reference's sample, and whether the fast rule is kept (dmax <= tol)."""
+    d = C.c_double()
+    n = C.c_int32()
+    _check(lib().tce_quad_self_check(fast.h, full.h, C.byref(d), C.byref(n)), fast.h)
+    return d.value, n.value, d.value <= tol
 
 
 def hartree_exchange_potential(n1: int, P: np.ndarray, ERI: np.ndarray, physicist: bool = False):
