@@ -44,6 +44,7 @@ SYSTEM_FIXTURE = os.path.join(ROOT, "tests", "golden", "systems", WORKLOAD + ".n
 ONEE_FIXTURE = os.path.join(ROOT, "tests", "golden", "systems", WORKLOAD + "_onee.npz")
 PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "k_quartets_h_chain64_traffic.json")
 L2_FLUSH_BYTES = 512 << 20
+FP32_THRESHOLD = 1e-6        # Schwarz product below which the node sums run in FP32
 
 
 def parse():
@@ -317,6 +318,16 @@ def main():
         return float(t[0]) / steps, float(t[1])
 
     nq_total = info["n_func_quartets"]
+    # FP32 panels (Schwarz product < 1e-6): their J/K error against the all-FP64 pass
+    eng.set_method(TCE_METHOD_LEARNED)
+    J64, K64 = eng.direct_JK(Ph)
+    eng.set_fp32_threshold(FP32_THRESHOLD)
+    J32, K32 = eng.direct_JK(Ph)
+    fp32 = {"threshold": FP32_THRESHOLD, "quartets": eng.lg_stats()["fp32"],
+            "max_abs_jk_diff_vs_fp64": float(max(np.abs(J32 - J64).max(), np.abs(K32 - K64).max())),
+            "density_abs_sum": float(np.abs(Ph).sum())}
+    # every pass is one CUDA-graph launch from here on
+    eng.set_graph(True)
     # the headline: learned-grid J/K passes, clocks sampled during them
     clocks = ClockSampler(local)
     eng.set_method(TCE_METHOD_LEARNED)
@@ -342,6 +353,9 @@ def main():
     plain_steps = max(2, min(args.steps, 3))
     plain_ms, _ = run(TCE_METHOD_PLAIN, plain_steps, 1)
     fixed_ms, fixed_kern = run(TCE_METHOD_FIXED, args.steps, args.warmup)
+    eng.set_fp32_threshold(0.0)
+    lg64_ms, _ = run(TCE_METHOD_LEARNED, args.steps, args.warmup)
+    eng.set_fp32_threshold(FP32_THRESHOLD)
     eng.set_method(TCE_METHOD_LEARNED)
 
     # ---- end to end through the public API: pinned host P in, J/K out, every step
@@ -401,7 +415,8 @@ def main():
             "config": config(sysm, {"parallelism": "quartet shards x%d + NCCL all-reduce of J/K" % world
                                     if world > 1 else "single GPU",
                                     "quadrature": "learned grid: per-quartet Gauss-Kronrod rule (K15..K61, 21 map "
-                                                  "scales) picked by the network, judge <= 1e-10, plain fallback",
+                                                  "scales) picked by the network, judge <= 1e-10, plain fallback; "
+                                                  "FP32 node sums below Schwarz 1e-6",
                                     "shell_quartets": info["n_shell_quartets"],
                                     "function_quartets": nq_total}),
             "plain": {"value": nq_total / (plain_ms * 1e-3), "ms_per_step": plain_ms, "steps": plain_steps,
@@ -409,6 +424,9 @@ def main():
             "lg_over_plain": plain_ms / ms_step,
             "fixed_rule": {"value": nq_total / (fixed_ms * 1e-3), "ms_per_step": fixed_ms,
                            "method": "the reference's 32-node mapped Gauss-Legendre rule on the same engine"},
+            "learned_grid_fp64_only": {"value": nq_total / (lg64_ms * 1e-3), "ms_per_step": lg64_ms},
+            "fp32_panels": fp32,
+            "cuda_graph": "each J/K pass replayed as one CUDA graph (tce_set_graph)",
             "learned_grid": dict(lg_info, judge_rejected_last_pass=st["rejected"]),
             "e2e": e2e, "roofline": roofline, "clocks": clk, "gpu_launches": args.steps * launches_per_step}
     if world == 1:

@@ -243,3 +243,28 @@ def test_fp32_panels_error_vs_fp64(chain16_lg):
     assert st["fp32"] > 0.2 * st["learned"]
     err = max(np.abs(J1 - J0).max(), np.abs(K1 - K0).max())
     assert err <= 1e-10 * scale, err
+
+
+def test_graph_on_the_legacy_stream(chain16_lg):
+    """tce_direct_jk_device on the legacy default stream with graphs on: the pass
+    runs on the handle's stream, ordered with the caller's stream by events."""
+    import torch
+    from william_ci_b200.engine import TCE_METHOD_LEARNED
+    sysm, eng = chain16_lg
+    n, nf = sysm.nbas, sysm.nfuc
+    P = random_density(n, 5) * 0.05
+    eng.set_method(TCE_METHOD_LEARNED)
+    eng.set_graph(False)
+    J0, K0 = eng.direct_JK(P)
+    dP = torch.from_numpy(np.asfortranarray(P).ravel(order="F").copy()).cuda()
+    dJ = torch.zeros(nf * n, dtype=torch.float64, device="cuda")
+    dK = torch.zeros(nf * n, dtype=torch.float64, device="cuda")
+    eng.set_graph(True)
+    for _ in range(2):
+        eng.direct_JK_device(dP.data_ptr(), dJ.data_ptr(), dK.data_ptr(), 0)
+        J1 = dJ.view(n, nf).T.cpu().numpy()       # device J is nfuc x nbas, column-major
+        K1 = dK.view(n, nf).T.cpu().numpy()
+        scale = np.abs(P).sum()
+        assert np.abs(J1 - J0[:nf]).max() <= 1e-13 * scale
+        assert np.abs(K1 - K0[:nf]).max() <= 1e-13 * scale
+    eng.set_graph(False)

@@ -323,6 +323,8 @@ int build(Handle *h, const tce_system *sys)
     CK(h, cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
     CK(h, cudaEventCreate(&h->ev0));
     CK(h, cudaEventCreate(&h->ev1));
+    CK(h, cudaEventCreateWithFlags(&h->ev_in, cudaEventDisableTiming));
+    CK(h, cudaEventCreateWithFlags(&h->ev_out, cudaEventDisableTiming));
     int s;
     DevSys &S = h->S;
     S.ndp = h->ndp; S.nq = h->nq; S.ncap = h->ncap; S.nbas = nbas; S.nfuc = h->nfuc;
@@ -625,8 +627,29 @@ void drop_graph(Handle *h)
 
 // One J/K pass.  With graphs on, the pass is captured once into a CUDA graph
 // (per pointer triple, stream, method and work lists) and replayed as one
-// graph launch per call; the events around it time the whole pass.
-int direct_jk_device(Handle *h, const double *dP, double *dJ, double *dK, cudaStream_t st)
+// graph launch per call; the events around it time the whole pass.  The
+// legacy default stream cannot be captured: a caller on it is ordered with the
+// handle's own stream by events, and the graph runs there.
+int direct_jk_device(Handle *h, const double *dP, double *dJ, double *dK, cudaStream_t caller)
+{
+    cudaStream_t st = caller;
+    const bool legacy =
+        h->use_graph && (caller == nullptr || caller == cudaStreamLegacy || caller == cudaStreamPerThread);
+    if (legacy) {
+        st = h->st;
+        CK(h, cudaEventRecord(h->ev_in, caller));
+        CK(h, cudaStreamWaitEvent(st, h->ev_in, 0));
+    }
+    int s = direct_jk_on(h, dP, dJ, dK, st);
+    if (s) return s;
+    if (legacy) {
+        CK(h, cudaEventRecord(h->ev_out, st));
+        CK(h, cudaStreamWaitEvent(caller, h->ev_out, 0));
+    }
+    return TCE_OK;
+}
+
+int direct_jk_on(Handle *h, const double *dP, double *dJ, double *dK, cudaStream_t st)
 {
     if (!h->use_graph) {
         CK(h, cudaEventRecord(h->ev0, st));
@@ -696,6 +719,8 @@ int tce_create(const tce_system *sys, void **handle)
         if (h->st) cudaStreamDestroy(h->st);
         if (h->ev0) cudaEventDestroy(h->ev0);
         if (h->ev1) cudaEventDestroy(h->ev1);
+        if (h->ev_in) cudaEventDestroy(h->ev_in);
+        if (h->ev_out) cudaEventDestroy(h->ev_out);
         delete h;
         return s;
     }
@@ -713,6 +738,8 @@ int tce_destroy(void *handle)
     if (h->st) cudaStreamDestroy(h->st);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->ev_in) cudaEventDestroy(h->ev_in);
+    if (h->ev_out) cudaEventDestroy(h->ev_out);
     delete h;
     return TCE_OK;
 }

@@ -31,6 +31,7 @@ struct Handle {
     // device
     cudaStream_t st = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;   // ordering with a caller on the legacy stream
     int num_sms = 148;
     std::vector<void *> allocs;
     size_t bytes = 0;
@@ -160,6 +161,7 @@ int shift_to(const Handle *h, int idx, int refcell, int nblk);
 int ncomb_of(const Handle *h, int SI, int SJ, int SK, int SL);
 int make_lists(Handle *h, const std::vector<int4> &items);
 int direct_jk_device(Handle *h, const double *dP, double *dJ, double *dK, cudaStream_t st);
+int direct_jk_on(Handle *h, const double *dP, double *dJ, double *dK, cudaStream_t st);
 void drop_graph(Handle *h);
 // learned-grid / plain passes of direct_jk_device (tce_lg.cu)
 int lg_jk_passes(Handle *h, const double *dP, double *dJ, double *dK, cudaStream_t st);
