@@ -278,6 +278,28 @@ int tce_mlp_predict(void *mlp, int64_t n, const float *X, float *prob);
  * that is cheaper).  Sets the per-item rules; nc must equal nrules. */
 int tce_lg_predict_rules(void *handle, void *mlp, double plain_factor);
 
+/* ------------------------------------------------------------------------
+ * DF-MP2 contraction and energy.  Replaces the (ov|ov) loop of df_kMO
+ * (df_toroidal.f90:1018-1035) and kMP2_calc (MP2_SAO.f90:6-151):
+ *   G(i a, j b; k1, k2, k3) = 1/N sum_Q L(i a, Q, k1, k2) L(j b, Q, k3, k4),
+ *   k4 = k1 - k2 + k3,
+ *   E2d = -sum |G(ia,jb;ki,ka,kj)|^2 / D,  E2x = -sum Re G(ia,jb;ki,ka,kj)
+ *          conj G(ib,ja;ki,kb,kj) / D,  D = e_a(ka) + e_b(kb) - e_i(ki) - e_j(kj),
+ *   E_MP2 = 2 E2d - E2x; terms with |D| < 1e-8 are left out and counted
+ *   (nzero, largest |G| in gzero).
+ * L: complex (re,im interleaved) L(p,q,Q,k1,k2), column-major, p < no
+ * (occupied band range 1..o_hi), q < nv (virtual band range v_lo..nfuc);
+ * kcoord[3k..3k+2]: cell coordinates of k (x fastest), ncl the lattice;
+ * eps_o[k*no+i], occ_o[k*no+i], eps_v[k*nv+a], occ_v[k*nv+a]: band energies
+ * and occupations (2 occupied, 0 virtual) of those ranges.
+ * mode 0: contraction in FP64; mode 1: tensor cores in split-BF16 with FP32
+ * accumulation (energy sums FP64 in both).  ms: device time of the kernels. */
+int tce_dfmp2_energy(int32_t ncell, const int32_t ncl[3], const int32_t *kcoord, int32_t no, int32_t nv,
+                     int32_t nau, const double *L, const double *eps_o, const int32_t *occ_o, const double *eps_v,
+                     const int32_t *occ_v, int32_t mode, double *e2d, double *e2x, int64_t *nzero, double *gzero,
+                     double *ms);
+const char *tce_mp2_last_error(void);
+
 /* Library build identification (sm_100a, version). */
 const char *tce_version(void);
 

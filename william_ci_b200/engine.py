@@ -42,7 +42,7 @@ EXPORTS = ["tce_create", "tce_destroy", "tce_last_error", "tce_get_info", "tce_s
            "tce_rule_blocks", "tce_mlp_create", "tce_mlp_destroy", "tce_mlp_last_error", "tce_mlp_nparams",
            "tce_mlp_get_params", "tce_mlp_set_params", "tce_mlp_loss_grad", "tce_mlp_train", "tce_mlp_predict",
            "tce_lg_predict_rules", "tce_lg_work", "tce_quad_self_check", "tce_set_graph",
-           "tce_set_fp32_threshold"]
+           "tce_set_fp32_threshold", "tce_dfmp2_energy", "tce_mp2_last_error"]
 
 TCE_METHOD_FIXED, TCE_METHOD_LEARNED, TCE_METHOD_PLAIN = 0, 1, 2
 TCE_NFEAT = 12
@@ -128,6 +128,9 @@ def lib():
         L.tce_quad_self_check.argtypes = [C.c_void_p, C.c_void_p, _dp, _ip]
         L.tce_set_graph.argtypes = [C.c_void_p, C.c_int32]
         L.tce_set_fp32_threshold.argtypes = [C.c_void_p, C.c_double]
+        L.tce_dfmp2_energy.argtypes = [C.c_int32, _ip, _ip, C.c_int32, C.c_int32, C.c_int32, _dp, _dp, _ip, _dp,
+                                       _ip, C.c_int32, _dp, _dp, _lp, _dp, _dp]
+        L.tce_mp2_last_error.restype = C.c_char_p
         _lib = L
     return _lib
 
@@ -385,6 +388,32 @@ def fast_quad_self_check(fast: Engine, full: Engine, tol: float = 1e-10):
     n = C.c_int32()
     _check(lib().tce_quad_self_check(fast.h, full.h, C.byref(d), C.byref(n)), fast.h)
     return d.value, n.value, d.value <= tol
+
+
+def dfmp2_energy(ncl, L, eps_o, occ_o, eps_v, occ_v, mode: int = 1):
+    """DF-MP2 contraction and energy on the device (tce_dfmp2_energy).
+
+    L: complex array (no, nv, nau, N, N) = L(p, q, Q, k1, k2); eps_*/occ_*: (N, no) and (N, nv).
+    Returns dict(e2d, e2x, emp2 = 2 e2d - e2x, nzero, gzero, ms)."""
+    ncl = np.array([int(x) for x in ncl], dtype=np.int32)
+    N = int(np.prod(ncl))
+    no, nv, nau = L.shape[0], L.shape[1], L.shape[2]
+    assert L.shape == (no, nv, nau, N, N)
+    Lf = np.ascontiguousarray(np.asfortranarray(L, dtype=np.complex128).ravel(order="F")).view(np.float64).copy()
+    crd = np.array([[k % ncl[0], (k // ncl[0]) % ncl[1], k // (ncl[0] * ncl[1])] for k in range(N)],
+                   dtype=np.int32).ravel()
+    eo = np.ascontiguousarray(eps_o, dtype=np.float64).ravel()
+    ev = np.ascontiguousarray(eps_v, dtype=np.float64).ravel()
+    oo = np.ascontiguousarray(occ_o, dtype=np.int32).ravel()
+    ovv = np.ascontiguousarray(occ_v, dtype=np.int32).ravel()
+    e2d, e2x, gz, ms = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+    nz = C.c_int64()
+    code = lib().tce_dfmp2_energy(N, _i(ncl), _i(crd), no, nv, nau, _d(Lf), _d(eo), _i(oo), _d(ev), _i(ovv),
+                                  int(mode), C.byref(e2d), C.byref(e2x), C.byref(nz), C.byref(gz), C.byref(ms))
+    if code != TCE_OK:
+        raise TCEError(code, lib().tce_mp2_last_error().decode())
+    return {"e2d": e2d.value, "e2x": e2x.value, "emp2": 2 * e2d.value - e2x.value, "nzero": nz.value,
+            "gzero": gz.value, "ms": ms.value}
 
 
 def hartree_exchange_potential(n1: int, P: np.ndarray, ERI: np.ndarray, physicist: bool = False):
