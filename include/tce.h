@@ -85,6 +85,16 @@ typedef struct {
 int tce_create(const tce_system *sys, void **handle);
 int tce_destroy(void *handle);
 const char *tce_last_error(void *handle);   /* handle may be NULL */
+
+/* A handle for shell blocks only (tce_shell_block, tce_rule_blocks): t-tables,
+ * shells and pair data, but no Schwarz pass, primitive table or quartet
+ * list, so J/K are not available.  Used for density fitting (df_init,
+ * df_toroidal.f90:352-701): the system then holds the orbital functions, the
+ * auxiliary functions and constant dummies (one s function of exponent 0 and
+ * coefficient 1 next to the auxiliary functions of each atom), and
+ * (mu nu|P) = (mu nu|P 1), (P|Q) = (P 1|Q 1) are ordinary blocks.  Pairs of two
+ * exponent-0 functions have zero weight. */
+int tce_create_blocks(const tce_system *sys, void **handle);
 int tce_get_info(void *handle, tce_info *info);
 
 /* One shell quartet block (S1 S2|S3 S4), blk column-major (n1,n2,n3,n4).

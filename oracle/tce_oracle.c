@@ -599,7 +599,11 @@ static void shell_block(const orc_ctx *c, const shellv *SA, const shellv *SB, co
     double ket_max = 0.0;
     for (int k = 0; k < n3; ++k)
         for (int l = 0; l < n4; ++l, ++kl) {
-            double e1 = SC->e[k], e2 = SD->e[l], esum = e1 + e2, mu = e1 * e2 / esum;
+            double e1 = SC->e[k], e2 = SD->e[l], esum = e1 + e2;
+            /* two exponent-0 functions (density-fitting dummies, df_toroidal.f90:837)
+               are never paired by the reference: zero weight, no division by 0 */
+            int nil = !(esum > 0.0);
+            double mu = nil ? 0.0 : e1 * e2 / esum;
             k_q[kl] = esum;
             double cf = 1.0, pe, cen;
             for (int d = 0; d < 3; ++d) {
@@ -612,14 +616,20 @@ static void shell_block(const orc_ctx *c, const shellv *SA, const shellv *SB, co
                     k_off[d + 3 * kl] = off;
                     off += (k_N[d + 3 * kl] + 1) * (lsC + 1) * (lsD + 1);
                 } else {
-                    cen = (e1 * rC[d] + e2 * rD[d]) / esum;
+                    cen = nil ? rC[d] : (e1 * rC[d] + e2 * rD[d]) / esum;
                     k_cen[d + 3 * kl] = cen;
                     cf *= exp(-mu * (rC[d] - rD[d]) * (rC[d] - rD[d]));
                     for (int ic = 0; ic <= lsC; ++ic)
-                        for (int id = 0; id <= lsD; ++id)
-                            orc_hermite_E_1D(ic, id, esum, cen - rC[d], cen - rD[d], &KE(0, ic, id, d, kl));
+                        for (int id = 0; id <= lsD; ++id) {
+                            if (nil) {
+                                for (int t = 0; t <= 16; ++t) (&KE(0, ic, id, d, kl))[t] = 0.0;
+                            } else {
+                                orc_hermite_E_1D(ic, id, esum, cen - rC[d], cen - rD[d], &KE(0, ic, id, d, kl));
+                            }
+                        }
                 }
             }
+            if (nil) cf = 0.0;
             k_fac[kl] = cf;
             double mc = 0.0, md = 0.0;
             for (int x = 0; x < nC; ++x) if (fabs(SC->c[x][k]) > mc) mc = fabs(SC->c[x][k]);
@@ -634,7 +644,9 @@ static void shell_block(const orc_ctx *c, const shellv *SA, const shellv *SB, co
     /* ---------------- bra pairs / quartets (:170-364) ---------------- */
     for (int i = 0; i < n1; ++i)
         for (int j = 0; j < n2; ++j) {
-            double e1 = SA->e[i], e2 = SB->e[j], esum = e1 + e2, mu = e1 * e2 / esum, p = esum;
+            double e1 = SA->e[i], e2 = SB->e[j], esum = e1 + e2, p = esum;
+            int bnil = !(esum > 0.0);                  /* two exponent-0 dummies: never paired */
+            double mu = bnil ? 0.0 : e1 * e2 / esum;
             double cAmax = 0.0, cBmax = 0.0;
             for (int x = 0; x < nA; ++x) if (fabs(SA->c[x][i]) > cAmax) cAmax = fabs(SA->c[x][i]);
             for (int x = 0; x < nB; ++x) if (fabs(SB->c[x][j]) > cBmax) cBmax = fabs(SB->c[x][j]);
@@ -648,11 +660,12 @@ static void shell_block(const orc_ctx *c, const shellv *SA, const shellv *SB, co
                     int est = orc_bessel_nmax_estimate(Aarg);
                     b_N[d] = est < nw - ME - 2 ? est : nw - ME - 2;
                 } else {
-                    cen = (e1 * rA[d] + e2 * rB[d]) / esum;
+                    cen = bnil ? rA[d] : (e1 * rA[d] + e2 * rB[d]) / esum;
                     b_cen[d] = cen;
                     bra_fac *= exp(-mu * (rA[d] - rB[d]) * (rA[d] - rB[d]));
                 }
             }
+            if (bnil) continue;
             if (!ps_noscreen && fabs(bra_fac) * cAmax * cBmax * ket_max <= screen_tol) continue;
 
             for (int d = 0; d < 3; ++d) {

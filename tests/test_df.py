@@ -1,0 +1,86 @@
+"""Density fitting for k-MP2 on the CPU: the product's k-space algebra
+(william_ci_b200/df.py: fit_B, L_vectors, chol_factor) against the literal
+restatement of df_init / df_L_kap (oracle/df_ref.py), both fed the C oracle's
+3- and 2-index integrals on the orbital + auxiliary + dummy system; MP2 from
+the L vectors with the numpy restatement of kMP2_calc."""
+import numpy as np
+import pytest
+
+import df_ref
+import mp2_ref
+import pyoracle as po
+from test_scf import dimer_chain, rhf_inputs
+
+
+@pytest.fixture(scope="module")
+def dimer_df():
+    from william_ci_b200 import df, scf
+    from william_ci_b200 import system as S
+    ao = dimer_chain(4)
+    cell = S.Cell("Tori1D", (4, 1, 1), 4.0, (16.0, 0.0, 0.0), [("H", (0.0, 0.0, 0.0)), ("H", (1.4, 0.0, 0.0))])
+    aux = S.build_system(cell, df.even_tempered_aux(ao.charges))
+    po.normalize(aux)
+    dfs = df.df_system(ao, aux)
+    orc = po.Oracle(dfs.sys)
+    sh, nshuc, _ = orc.shells()
+    Vm, T3 = df_ref.integrals(orc, dfs, sh, nshuc)
+    o, St, Tt, Vt, en, nO = rhf_inputs(ao)
+    r = scf.rhf_sao(St, Tt, Vt, en, nO, ao.nfuc, ao.ncell, lambda P: o.direct_jk(P)[:2])
+    assert r.converged
+    return dfs, Vm, T3, r
+
+
+def test_chol_factor_whitens_the_metric():
+    from william_ci_b200 import df
+    rng = np.random.default_rng(1)
+    A = rng.standard_normal((9, 6)) + 1j * rng.standard_normal((9, 6))
+    V = A @ A.conj().T                                   # rank 6
+    f, nd = df.chol_factor(V, 1e-10)
+    assert nd == 3
+    P = f.conj().T @ V @ f
+    np.testing.assert_allclose(P[:6, :6], np.eye(6), atol=1e-10)
+    np.testing.assert_allclose(f, df_ref.chol_f(V, 1e-10), atol=1e-12)
+
+
+def test_fitted_vectors_and_L_match_the_restatement(dimer_df):
+    from william_ci_b200 import df
+    dfs, Vm, T3, r = dimer_df
+    ncl = dfs.sys.ncell
+    B, _ = df.fit_B(Vm, T3, ncl, dfs.nau)
+    Bref = df_ref.fitted(Vm, T3, ncl, dfs.nau)
+    # the inverse Cholesky factor of the metric amplifies the rounding of the two
+    # summation orders (metric entries up to ~1e2, smallest pivots ~1e-6)
+    assert np.abs(B - Bref).max() < 1e-9
+    (p0, p1), (q0, q1) = df.band_ranges(r.occ_k)
+    L = df.L_vectors(B, r.C_k, ncl, dfs.nfuc_ao, dfs.nau, (p0, p1), (q0, q1))
+    Lref = df_ref.L_vectors(Bref, r.C_k, ncl, dfs.nfuc_ao, dfs.nau, p0, p1, q0, q1)
+    assert np.abs(L - Lref).max() < 1e-9
+
+
+def test_fit_reproduces_four_index_integrals(dimer_df):
+    """sum_Q B B approximates (mu0 nu|la si) (the fitting error of this minimal
+    auxiliary set), checked on the diagonal (mu0 nu|mu0 nu) = Q(mu,nu)^2."""
+    from william_ci_b200 import df
+    dfs, Vm, T3, r = dimer_df
+    B, _ = df.fit_B(Vm, T3, dfs.sys.ncell, dfs.nau)
+    o = po.Oracle(dimer_chain(4))
+    Q = o.schwarz()
+    nf, nb = B.shape[0], B.shape[1]
+    fit = np.einsum("abq,abq->ab", B, B)
+    exact = Q[:nf, :nb] ** 2
+    big = exact > 1e-3
+    assert np.all(fit[big] <= exact[big] * (1 + 1e-8))      # the fit never exceeds the exact value
+    assert np.max(np.abs(fit[big] - exact[big]) / exact[big]) < 0.05
+
+
+def test_mp2_energy_restatement_is_consistent(dimer_df):
+    from william_ci_b200 import df
+    dfs, Vm, T3, r = dimer_df
+    ncl = dfs.sys.ncell
+    Bref = df_ref.fitted(Vm, T3, ncl, dfs.nau)
+    (p0, p1), (q0, q1) = df.band_ranges(r.occ_k)
+    L = df_ref.L_vectors(Bref, r.C_k, ncl, dfs.nfuc_ao, dfs.nau, p0, p1, q0, q1)
+    G = mp2_ref.ovov(L, ncl)
+    e = mp2_ref.kmp2(G, ncl, r.eps_k[:, p0:p1], r.occ_k[:, p0:p1], r.eps_k[:, q0:q1], r.occ_k[:, q0:q1])
+    assert e["nzero"] == 0
+    assert -0.1 < e["emp2"] < 0.0                        # a small negative correlation energy per supercell

@@ -438,6 +438,26 @@ int build(Handle *h, const tce_system *sys)
         dfree(h, scr);
     }
 
+    // a handle for shell blocks only (tce_create_blocks): no Schwarz pass, no
+    // primitive table, no quartet list; blocks are evaluated with the prefactor
+    // screens of the kernel only
+    if (h->blocks_only) {
+        h->Q.assign((size_t)nbas * nbas, 1.0);
+        h->Qsh.assign((size_t)h->nsh * h->nsh, 1.0);
+        h->Qmax = 1.0;
+        h->prim_screen = 0;
+        double *dQ;
+        if ((s = upload(h, &dQ, h->Q))) return s;
+        S.Q = dQ;
+        if ((s = upload(h, &h->d_Qsh, h->Qsh))) return s;
+        if ((s = dalloc(h, &h->d_P, (size_t)nbas * nbas))) return s;
+        if ((s = dalloc(h, &h->d_J, (size_t)h->nfuc * nbas))) return s;
+        if ((s = dalloc(h, &h->d_K, (size_t)h->nfuc * nbas))) return s;
+        h->shard_idx.clear();
+        CK(h, cudaStreamSynchronize(h->st));
+        return TCE_OK;
+    }
+
     // ---------------- Schwarz: diagonal blocks, SI in the unit cell (ERI_toroidal.f90:200-236) ----------
     {
         std::vector<int4> items;
@@ -707,11 +727,12 @@ const char *tce_last_error(void *handle)
     return g_err.c_str();
 }
 
-int tce_create(const tce_system *sys, void **handle)
+static int create_impl(const tce_system *sys, void **handle, bool blocks_only)
 {
     if (!handle) return fail(nullptr, TCE_ERR_ARG, "handle is NULL");
     *handle = nullptr;
     Handle *h = new Handle();
+    h->blocks_only = blocks_only ? 1 : 0;
     int s = build(h, sys);
     if (s != TCE_OK) {
         g_err = h->err;
@@ -727,6 +748,10 @@ int tce_create(const tce_system *sys, void **handle)
     *handle = h;
     return TCE_OK;
 }
+
+int tce_create(const tce_system *sys, void **handle) { return create_impl(sys, handle, false); }
+
+int tce_create_blocks(const tce_system *sys, void **handle) { return create_impl(sys, handle, true); }
 
 int tce_destroy(void *handle)
 {

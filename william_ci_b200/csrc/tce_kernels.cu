@@ -88,7 +88,10 @@ __global__ void k_pair_scalars(DevSys S, long long npp_tot, const int *pp_unit, 
     int i = loc / U.np2, j = loc % U.np2;
     int S1 = U.S1, S2 = U.S2;
     double e1 = S.sh_exp[S.sh_eoff[S1] + i], e2 = S.sh_exp[S.sh_eoff[S2] + j];
-    double esum = e1 + e2, mu = e1 * e2 / esum;
+    // a pair of two exponent-0 functions (the constant dummies next to auxiliary
+    // functions in density fitting) is never evaluated: zero prefactor, no NaN
+    const bool nil = !(e1 + e2 > 0.0);
+    double esum = e1 + e2, mu = nil ? 0.0 : e1 * e2 / esum;
     PairPrim P;
     P.esum = esum;
     P.cmax12 = S.sh_cmax[S.sh_eoff[S1] + i] * S.sh_cmax[S.sh_eoff[S2] + j];
@@ -109,7 +112,7 @@ __global__ void k_pair_scalars(DevSys S, long long npp_tot, const int *pp_unit, 
             P.A[d] = A;
             P.N[d] = est < S.ncap ? est : S.ncap;
         } else {
-            double cen = (e1 * r1[d] + e2 * r2[d]) / esum;
+            double cen = nil ? r1[d] : (e1 * r1[d] + e2 * r2[d]) / esum;
             P.cen[d] = cen;
             pf *= exp(-mu * (r1[d] - r2[d]) * (r1[d] - r2[d]));
             // Hermite E for every (ia, ib) of this pair, real direction dr
@@ -118,11 +121,16 @@ __global__ void k_pair_scalars(DevSys S, long long npp_tot, const int *pp_unit, 
                 for (int ib = 0; ib <= U.l2; ++ib) {
                     double *E = ecoef + U.e_off +
                                 ((((long long)loc * nreal + dr) * (U.l1 + 1) + ia) * (U.l2 + 1) + ib) * TCE_ECO;
-                    tce_hermite_E(ia, ib, esum, cen - r1[d], cen - r2[d], E);
+                    if (nil) {
+                        for (int t = 0; t < TCE_ECO; ++t) E[t] = 0.0;
+                    } else {
+                        tce_hermite_E(ia, ib, esum, cen - r1[d], cen - r2[d], E);
+                    }
                 }
         }
     }
-    P.pfac = pf;
+    P.pfac = nil ? 0.0 : pf;
+    if (nil) P.cmax12 = 0.0;
     pp[id] = P;
 }
 

@@ -807,8 +807,11 @@ int tce_rule_blocks(void *handle, int32_t rule, int32_t mode, int64_t n, const i
     std::vector<int4> v;
     if ((s = translate_items(h, n, items, v))) return s;
     std::vector<long long> off(v.size() + 1, 0);
-    for (size_t i = 0; i < v.size(); ++i)
+    int mxc = 1;
+    for (size_t i = 0; i < v.size(); ++i) {
         off[i + 1] = off[i] + (long long)h->sh_n[v[i].x] * h->sh_n[v[i].y] * h->sh_n[v[i].z] * h->sh_n[v[i].w];
+        mxc = std::max(mxc, ncomb_of(h, v[i].x, v[i].y, v[i].z, v[i].w));
+    }
     int4 *d_it = nullptr;
     long long *d_off = nullptr;
     double *d_K = nullptr, *d_G = nullptr;
@@ -820,6 +823,7 @@ int tce_rule_blocks(void *handle, int32_t rule, int32_t mode, int64_t n, const i
     fill_common(h, a);
     a.items = d_it;
     a.nitems = (int)n;
+    a.max_ncomb = mxc;          // the largest class among these items (not only the engine's)
     a.mode = mode == 2 ? TCE_MODE_NOSCREEN : TCE_MODE_BLOCK;
     a.prim_screen = mode == 1;
     a.next = h->d_next;

@@ -42,7 +42,7 @@ EXPORTS = ["tce_create", "tce_destroy", "tce_last_error", "tce_get_info", "tce_s
            "tce_rule_blocks", "tce_mlp_create", "tce_mlp_destroy", "tce_mlp_last_error", "tce_mlp_nparams",
            "tce_mlp_get_params", "tce_mlp_set_params", "tce_mlp_loss_grad", "tce_mlp_train", "tce_mlp_predict",
            "tce_lg_predict_rules", "tce_lg_work", "tce_quad_self_check", "tce_set_graph",
-           "tce_set_fp32_threshold", "tce_dfmp2_energy", "tce_mp2_last_error"]
+           "tce_set_fp32_threshold", "tce_dfmp2_energy", "tce_mp2_last_error", "tce_create_blocks"]
 
 TCE_METHOD_FIXED, TCE_METHOD_LEARNED, TCE_METHOD_PLAIN = 0, 1, 2
 TCE_NFEAT = 12
@@ -83,6 +83,7 @@ def lib():
             raise TCEError(TCE_ERR_CUDA, "libtce.so is not built (run william_ci_b200.build.build())")
         L = C.CDLL(LIB_PATH)
         L.tce_create.argtypes = [C.POINTER(TceSystem), C.POINTER(C.c_void_p)]
+        L.tce_create_blocks.argtypes = [C.POINTER(TceSystem), C.POINTER(C.c_void_p)]
         L.tce_destroy.argtypes = [C.c_void_p]
         L.tce_last_error.restype = C.c_char_p
         L.tce_last_error.argtypes = [C.c_void_p]
@@ -153,7 +154,7 @@ class Engine:
     """Device engine for one supercell basis (normalised coefficients)."""
 
     def __init__(self, system: AOSystem, nquad: int = 32, t_nodes=None, t_weights=None, physicist=False,
-                 sao=True, prim_screen=True, schwarz_thr=1e-13, prim_thr=1e-14):
+                 sao=True, prim_screen=True, schwarz_thr=1e-13, prim_thr=1e-14, blocks_only=False):
         self.sys = system
         self.physicist = bool(physicist)
         self.sao = bool(sao)
@@ -182,7 +183,8 @@ class Engine:
         s.schwarz_thr, s.prim_thr = schwarz_thr, prim_thr
         self._s = s
         h = C.c_void_p()
-        code = lib().tce_create(C.byref(s), C.byref(h))
+        create = lib().tce_create_blocks if blocks_only else lib().tce_create
+        code = create(C.byref(s), C.byref(h))
         if code != TCE_OK:
             msg = lib().tce_last_error(None)
             raise TCEError(code, msg.decode() if msg else "")

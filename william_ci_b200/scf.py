@@ -177,6 +177,12 @@ class RHFResult:
     history: List[Dict[str, float]]
     jk_seconds: List[float]
     iter_seconds: List[float]
+    # the last diagonalisation: per k block the orbitals (SAO basis, columns by
+    # ascending energy), their energies and occupations (2 or 0), as the
+    # reference's blk(k) and coeff_SAO blocks
+    C_k: Optional[np.ndarray] = None          # (Nc, nfuc, nfuc) complex
+    eps_k: Optional[np.ndarray] = None        # (Nc, nfuc)
+    occ_k: Optional[np.ndarray] = None        # (Nc, nfuc) int
 
 
 def rhf_sao(S: np.ndarray, T: np.ndarray, V: np.ndarray, enuc: float, nO: int, nfuc: int, ncell,
@@ -211,6 +217,7 @@ def rhf_sao(S: np.ndarray, T: np.ndarray, V: np.ndarray, enuc: float, nO: int, n
     n_stable = 0
     conv_hist = np.full(5, np.inf)
     eps = np.zeros(nbas)
+    C_k = occ_k = None
     nscf = 0
     while nscf < max_scf:
         t_it = time.perf_counter()
@@ -256,15 +263,18 @@ def rhf_sao(S: np.ndarray, T: np.ndarray, V: np.ndarray, enuc: float, nO: int, n
             C_k[k] = X_k[k] @ Ck
         idx = reference_sort(eps) if nbas <= 512 else np.argsort(eps, kind="stable")
         P_k = np.zeros_like(F_k)
+        occ_k = np.zeros((Nc, nfuc), dtype=np.int32)
         for i in range(nO):
             o = idx[i]
             kb, col = divmod(int(o), nfuc)
+            occ_k[kb, col] = 2
             c = C_k[kb][:, col]
             P_k[kb] += 2.0 * np.outer(c, c.conj())
         P = sao.to_ao(P_k)
         it_t.append(time.perf_counter() - t_it)
     return RHFResult(energy=ehf + enuc, e_electronic=ehf, converged=converged, stalled=stalled, iterations=nscf,
-                     orbital_energies=np.sort(eps), history=hist, jk_seconds=jk_t, iter_seconds=it_t)
+                     orbital_energies=np.sort(eps), history=hist, jk_seconds=jk_t, iter_seconds=it_t,
+                     C_k=C_k, eps_k=eps.reshape(Nc, nfuc).copy(), occ_k=occ_k)
 
 
 def fill_with_symmetry(rows: np.ndarray, nfuc: int, ncell) -> np.ndarray:
