@@ -20,7 +20,8 @@ import pyoracle  # noqa: E402
 from william_ci_b200 import system as S  # noqa: E402
 
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "systems")
-ONE_ELECTRON = ("h2_ring", "h_chain64")   # RHF inputs stored for the SCF timing
+ONE_ELECTRON = ("h2_ring", "h_chain64", "h_chain128")   # RHF inputs stored for the SCF / DF-MP2 timing
+AUX = ("h_chain128",)   # even-tempered auxiliary basis of the DF-MP2 configuration
 
 
 def main():
@@ -31,6 +32,13 @@ def main():
         path = os.path.join(OUT, name + ".npz")
         sysm.save(path)
         print("%-11s nbas %5d nfuc %3d  max|<phi|phi>-1| %.1e  -> %s" % (name, sysm.nbas, sysm.nfuc, dev, path))
+        if name in AUX:
+            from william_ci_b200 import df
+            cell, _ = S.workload(name)
+            aux = S.build_system(cell, df.even_tempered_aux(sysm.charges))
+            dev_a = pyoracle.normalize(aux)
+            aux.save(os.path.join(OUT, name + "_aux.npz"))
+            print("%-11s auxiliary nbas %5d  max|<P|P>-1| %.1e" % (name, aux.nbas, dev_a))
         if name in ONE_ELECTRON:
             # S, T, V rows of the unit cell (the others follow by translation) and E_nuc,
             # the inputs RHF_SAO receives (main.f90:379-500)
