@@ -458,6 +458,28 @@ int lg_rebuild_lists(Handle *h)
     }
     for (int key = 0; key < 3 * 16 * 4; ++key) {
         if (lg[key].empty()) continue;
+        // quartets of one rule next to each other, so that the warps working at
+        // the same time on an SM read the same T table (L1 reuse); rules with
+        // more nodes first, each rule's quartets in the original (dearest
+        // first) order
+        {
+            std::vector<size_t> ord(lg[key].size());
+            std::iota(ord.begin(), ord.end(), 0);
+            const std::vector<int> &rk = rl[key];
+            std::stable_sort(ord.begin(), ord.end(), [&](size_t x, size_t y) {
+                const int nx = h->rules_host[rk[x]].nn, ny = h->rules_host[rk[y]].nn;
+                if (nx != ny) return nx > ny;
+                return rk[x] < rk[y];
+            });
+            std::vector<int4> li(ord.size());
+            std::vector<int> lr(ord.size());
+            for (size_t i = 0; i < ord.size(); ++i) {
+                li[i] = lg[key][ord[i]];
+                lr[i] = rk[ord[i]];
+            }
+            lg[key].swap(li);
+            rl[key].swap(lr);
+        }
         Handle::LgList w;
         w.kind = key / 64;
         w.cls = (key / 4) % 16;
