@@ -389,12 +389,9 @@ def main():
     ms_step, lg_kern = float(t[0]) / args.steps, float(t[1])
     value = nq_total / (ms_step * 1e-3)
     st = eng.lg_stats()
-    from william_ci_b200 import learned_grid as LG
-    _, meta = LG.dictionary()
-    used = set(int(r) for r in eng.lg_item_rules() if r < eng.nrules)
-    classes = {2 * meta[r][1] + 1 <= 32 for r in used}
-    # learned-grid launches (one per node-count class), the fallback launch, the plain-direct launch
-    launches_per_step = len(classes) + int(len(used) > 0) + int(st["plain_direct"] > 0)
+    # kernels of one learned-grid pass: one per work list (kernel class, rule size,
+    # FP32 panels), the plain list on the side stream, the judge's fallback launch
+    launches_per_step = eng.pass_kernels()
     # comparison arms on the same device: the plain adaptive method and the system's 32-node rule
     plain_steps = max(2, min(args.steps, 3))
     plain_ms, _ = run(TCE_METHOD_PLAIN, plain_steps, 1)
@@ -473,7 +470,8 @@ def main():
             "learned_grid_fp64_only": {"value": nq_total / (lg64_ms * 1e-3), "ms_per_step": lg64_ms},
             "fp32_panels": fp32,
             "cuda_graph": "each J/K pass replayed as one CUDA graph (tce_set_graph)",
-            "learned_grid": dict(lg_info, judge_rejected_last_pass=st["rejected"]),
+            "learned_grid": dict(lg_info, judge_rejected_last_pass=st["rejected"],
+                                 plain_list_last_pass=st["plain_direct"]),
             "e2e": e2e, "roofline": roofline, "clocks": clk, "gpu_launches": args.steps * launches_per_step}
     if world == 1:
         line["rhf_scf"] = scf_iterations(eng, sysm)

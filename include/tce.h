@@ -237,8 +237,18 @@ int tce_lg_item_rules(void *handle, int32_t *rule);
  * accumulation stay FP64.  thr = 0 (default) turns it off; at most 1e-3. */
 int tce_set_fp32_threshold(void *handle, double thr);
 
-/* Quadrature method of tce_direct_jk[_device] (TCE_METHOD_*). */
+/* Quadrature method of tce_direct_jk[_device] (TCE_METHOD_*).  With
+ * TCE_METHOD_LEARNED the quartets the judge rejected in a pass (their count
+ * is read back asynchronously after the pass) are sent straight to the plain
+ * method from the next pass on (up to 4096 of them; the work lists change
+ * once, and tce_lg_item_rules then reports them as plain); the plain list
+ * runs on a second stream of the handle next to the learned-grid kernels.
+ * No reference counterpart: the reference has one quadrature. */
 int tce_set_method(void *handle, int32_t method);
+
+/* Kernels one J/K pass launches with the current method and work lists
+ * (memsets and copies not counted).  No reference counterpart. */
+int tce_pass_kernels(void *handle, int32_t *n);
 
 /* Judge tolerance on max |K - G| of a block (default 1e-10), plain-method
  * tolerance on the summed panel estimates (default 1e-11) and its panel

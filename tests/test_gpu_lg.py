@@ -206,12 +206,12 @@ def chain16_lg(systems):
     eng = _lg_engine(sysm)
     net, _, _ = _trained(eng, sysm)
     eng.lg_predict_rules(net)
-    return sysm, eng
+    return sysm, eng, net
 
 
 def test_graph_replay_matches_direct_launches(chain16_lg):
     from william_ci_b200.engine import TCE_METHOD_FIXED, TCE_METHOD_LEARNED
-    sysm, eng = chain16_lg
+    sysm, eng, net = chain16_lg
     P = random_density(sysm.nbas, 3) * 0.05
     scale = np.abs(P).sum()
     for method in (TCE_METHOD_LEARNED, TCE_METHOD_FIXED):
@@ -230,7 +230,7 @@ def test_fp32_panels_error_vs_fp64(chain16_lg):
     """FP32 node sums for quartets with Schwarz product below 1e-6: the J/K
     difference from the all-FP64 pass stays below 1e-10 per unit density."""
     from william_ci_b200.engine import TCE_METHOD_LEARNED
-    sysm, eng = chain16_lg
+    sysm, eng, net = chain16_lg
     P = random_density(sysm.nbas, 4) * 0.05
     scale = np.abs(P).sum()
     eng.set_method(TCE_METHOD_LEARNED)
@@ -250,7 +250,7 @@ def test_graph_on_the_legacy_stream(chain16_lg):
     runs on the handle's stream, ordered with the caller's stream by events."""
     import torch
     from william_ci_b200.engine import TCE_METHOD_LEARNED
-    sysm, eng = chain16_lg
+    sysm, eng, net = chain16_lg
     n, nf = sysm.nbas, sysm.nfuc
     P = random_density(n, 5) * 0.05
     eng.set_method(TCE_METHOD_LEARNED)
@@ -268,3 +268,34 @@ def test_graph_on_the_legacy_stream(chain16_lg):
         assert np.abs(J1 - J0[:nf]).max() <= 1e-13 * scale
         assert np.abs(K1 - K0[:nf]).max() <= 1e-13 * scale
     eng.set_graph(False)
+
+
+def test_rejects_move_to_the_plain_list(chain16_lg):
+    """The judge's rejects of one pass go to the plain list (side stream) from
+    the next pass on: the judge then rejects nothing, the plain list grows by
+    the reject count, the item rules report them as plain, and J/K stay the
+    same (the same plain method evaluates those quartets in both passes)."""
+    from william_ci_b200.engine import TCE_METHOD_LEARNED
+    sysm, eng, net = chain16_lg
+    P = random_density(sysm.nbas, 6) * 0.05
+    scale = np.abs(P).sum()
+    eng.set_method(TCE_METHOD_LEARNED)
+    eng.set_graph(False)
+    eng.lg_predict_rules(net)                 # the network's rules again (earlier passes moved rejects)
+    try:
+        J1, K1 = eng.direct_JK(P)
+        s1 = eng.lg_stats()
+        plain1 = int(np.sum(eng.lg_item_rules() == eng.nrules))
+        assert 0 < s1["rejected"] <= 4096, s1
+        for graph in (False, True):
+            eng.set_graph(graph)
+            J2, K2 = eng.direct_JK(P)
+            s2 = eng.lg_stats()
+            assert s2["rejected"] == 0, s2
+            assert s2["plain_direct"] == s1["plain_direct"] + s1["rejected"], (s1, s2)
+            assert s2["learned"] == s1["learned"] - s1["rejected"]
+            assert int(np.sum(eng.lg_item_rules() == eng.nrules)) == plain1 + s1["rejected"]
+            assert np.abs(J2 - J1).max() <= 1e-13 * scale and np.abs(K2 - K1).max() <= 1e-13 * scale
+            assert eng.pass_kernels() >= 2      # at least the plain list and the judge's fallback
+    finally:
+        eng.set_graph(False)

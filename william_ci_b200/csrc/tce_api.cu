@@ -325,6 +325,10 @@ int build(Handle *h, const tce_system *sys)
     CK(h, cudaEventCreate(&h->ev1));
     CK(h, cudaEventCreateWithFlags(&h->ev_in, cudaEventDisableTiming));
     CK(h, cudaEventCreateWithFlags(&h->ev_out, cudaEventDisableTiming));
+    CK(h, cudaStreamCreateWithFlags(&h->st2, cudaStreamNonBlocking));
+    CK(h, cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+    CK(h, cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+    CK(h, cudaEventCreateWithFlags(&h->ev_fb, cudaEventDisableTiming));
     int s;
     DevSys &S = h->S;
     S.ndp = h->ndp; S.nq = h->nq; S.ncap = h->ncap; S.nbas = nbas; S.nfuc = h->nfuc;
@@ -639,6 +643,19 @@ static int jk_body(Handle *h, const double *dP, double *dJ, double *dK, cudaStre
     return TCE_OK;
 }
 
+// streams, events and pinned host memory of a handle
+void release_streams(Handle *h)
+{
+    if (h->st) cudaStreamDestroy(h->st);
+    if (h->st2) cudaStreamDestroy(h->st2);
+    for (cudaEvent_t e : {h->ev0, h->ev1, h->ev_in, h->ev_out, h->ev_fork, h->ev_join, h->ev_fb})
+        if (e) cudaEventDestroy(e);
+    if (h->h_fb) cudaFreeHost(h->h_fb);
+    h->st = h->st2 = nullptr;
+    h->ev0 = h->ev1 = h->ev_in = h->ev_out = h->ev_fork = h->ev_join = h->ev_fb = nullptr;
+    h->h_fb = nullptr;
+}
+
 void drop_graph(Handle *h)
 {
     if (h->jk_exec) cudaGraphExecDestroy(h->jk_exec);
@@ -671,12 +688,17 @@ int direct_jk_device(Handle *h, const double *dP, double *dJ, double *dK, cudaSt
 
 int direct_jk_on(Handle *h, const double *dP, double *dJ, double *dK, cudaStream_t st)
 {
+    const bool lg = h->method == TCE_METHOD_LEARNED;
+    if (lg) {   // the last pass's rejects join the plain list (the work lists change once)
+        int s = lg_absorb_rejects(h);
+        if (s) return s;
+    }
     if (!h->use_graph) {
         CK(h, cudaEventRecord(h->ev0, st));
         int s = jk_body(h, dP, dJ, dK, st);
         if (s) return s;
         CK(h, cudaEventRecord(h->ev1, st));
-        return TCE_OK;
+        return lg ? lg_read_rejects(h, st) : TCE_OK;
     }
     const bool same = h->jk_exec && h->g_P == dP && h->g_J == dJ && h->g_K == dK && h->g_st == st &&
                       h->g_method == h->method && h->g_version == h->work_version;
@@ -707,7 +729,7 @@ int direct_jk_on(Handle *h, const double *dP, double *dJ, double *dK, cudaStream
     CK(h, cudaEventRecord(h->ev0, st));
     CK(h, cudaGraphLaunch(h->jk_exec, st));
     CK(h, cudaEventRecord(h->ev1, st));
-    return TCE_OK;
+    return lg ? lg_read_rejects(h, st) : TCE_OK;
 }
 
 }  // namespace tcehost
@@ -737,11 +759,7 @@ static int create_impl(const tce_system *sys, void **handle, bool blocks_only)
     if (s != TCE_OK) {
         g_err = h->err;
         for (void *p : h->allocs) cudaFree(p);
-        if (h->st) cudaStreamDestroy(h->st);
-        if (h->ev0) cudaEventDestroy(h->ev0);
-        if (h->ev1) cudaEventDestroy(h->ev1);
-        if (h->ev_in) cudaEventDestroy(h->ev_in);
-        if (h->ev_out) cudaEventDestroy(h->ev_out);
+        release_streams(h);
         delete h;
         return s;
     }
@@ -759,13 +777,26 @@ int tce_destroy(void *handle)
     if (!h) return TCE_OK;
     if (h->st) cudaStreamSynchronize(h->st);
     drop_graph(h);
+    if (h->st2) cudaStreamSynchronize(h->st2);
     for (void *p : h->allocs) cudaFree(p);
-    if (h->st) cudaStreamDestroy(h->st);
-    if (h->ev0) cudaEventDestroy(h->ev0);
-    if (h->ev1) cudaEventDestroy(h->ev1);
-    if (h->ev_in) cudaEventDestroy(h->ev_in);
-    if (h->ev_out) cudaEventDestroy(h->ev_out);
+    release_streams(h);
     delete h;
+    return TCE_OK;
+}
+
+int tce_pass_kernels(void *handle, int32_t *n)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !n) return fail(h, TCE_ERR_ARG, "NULL argument");
+    int k = 0;
+    if (h->method == TCE_METHOD_FIXED) {
+        for (const auto &w : h->lists) k += w.n > 0 ? 1 : 0;
+    } else if (h->method == TCE_METHOD_PLAIN) {
+        k = h->shard_idx.empty() ? 0 : 1;
+    } else {
+        k = (int)h->lg_lists.size() + (h->n_plain_direct > 0 ? 1 : 0) + (h->n_lg > 0 ? 1 : 0);
+    }
+    *n = k;
     return TCE_OK;
 }
 

@@ -87,6 +87,18 @@ struct Handle {
     long long n_plain_direct = 0;
     int4 *d_fb_items = nullptr;
     unsigned int *d_fb_count = nullptr;
+    // The judge's rejects depend on the integrals only, so they repeat every
+    // pass: after a pass their count and the first fb_cap of them are copied to
+    // pinned host memory (event ev_fb); the next call moves them to the plain
+    // list, which runs on the side stream st2 while the learned-grid kernels run.
+    cudaStream_t st2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_fb = nullptr;
+    unsigned int *h_fb = nullptr;        // pinned: [0] count, items from word 4
+    int fb_cap = 4096;
+    int fb_pending = 0;
+    long long fb_version = -1;           // work_version of the pass the copy came from
+    int route_rejects = 1;
+    std::vector<long long> item_order;   // items_host indices in quartet order (lookup)
     double judge_tol = 1e-10, plain_tol = 1e-11;
     int plain_max_panels = 24;
     double plain_scale = 0.6;
@@ -167,5 +179,8 @@ void drop_graph(Handle *h);
 // learned-grid / plain passes of direct_jk_device (tce_lg.cu)
 int lg_jk_passes(Handle *h, const double *dP, double *dJ, double *dK, cudaStream_t st);
 int lg_rebuild_lists(Handle *h);
+int lg_read_rejects(Handle *h, cudaStream_t st);
+int lg_absorb_rejects(Handle *h);
+void release_streams(Handle *h);
 
 }  // namespace tcehost

@@ -4,6 +4,7 @@
 // the plain adaptive method.  No counterpart in the reference: its t-integral
 // uses one fixed rule per run (fast_quad or the 64/128 tables,
 // precompute_t.f90:5-14, 906-942).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -500,6 +501,69 @@ int lg_rebuild_lists(Handle *h)
     return TCE_OK;
 }
 
+// After a learned-grid pass (on the pass's stream): the reject count and the
+// first fb_cap rejects to pinned host memory.
+int lg_read_rejects(Handle *h, cudaStream_t st)
+{
+    if (!h->route_rejects || h->n_lg == 0 || !h->d_fb_count || !h->d_fb_items) return TCE_OK;
+    if (!h->h_fb) CK(h, cudaHostAlloc(reinterpret_cast<void **>(&h->h_fb), 16 + sizeof(int4) * (size_t)h->fb_cap,
+                                      cudaHostAllocDefault));
+    const long long n = std::min<long long>(h->n_lg, h->fb_cap);
+    CK(h, cudaMemcpyAsync(h->h_fb, h->d_fb_count, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+    CK(h, cudaMemcpyAsync(h->h_fb + 4, h->d_fb_items, sizeof(int4) * (size_t)n, cudaMemcpyDeviceToHost, st));
+    CK(h, cudaEventRecord(h->ev_fb, st));
+    h->fb_pending = 1;
+    h->fb_version = h->work_version;
+    return TCE_OK;
+}
+
+static bool quartet_less(const int4 &a, const int4 &b)
+{
+    if (a.x != b.x) return a.x < b.x;
+    if (a.y != b.y) return a.y < b.y;
+    if (a.z != b.z) return a.z < b.z;
+    return a.w < b.w;
+}
+
+// Before a learned-grid pass: if the last pass has finished (its copy is in)
+// and its work lists are still the current ones, its rejects get the plain
+// method (item rule = lg_nrules) and the lists are rebuilt.  Up to fb_cap
+// rejects are moved; with more, the judge's fallback keeps them.
+int lg_absorb_rejects(Handle *h)
+{
+    if (!h->fb_pending) return TCE_OK;
+    const cudaError_t q = cudaEventQuery(h->ev_fb);
+    if (q == cudaErrorNotReady) return TCE_OK;
+    h->fb_pending = 0;
+    CK(h, q);
+    const unsigned int n = h->h_fb[0];
+    if (n == 0 || n > (unsigned int)h->fb_cap || h->fb_version != h->work_version) return TCE_OK;
+    if (h->item_rule.size() != h->items_host.size()) return TCE_OK;
+    if (h->item_order.size() != h->items_host.size()) {
+        h->item_order.resize(h->items_host.size());
+        std::iota(h->item_order.begin(), h->item_order.end(), 0LL);
+        std::sort(h->item_order.begin(), h->item_order.end(), [&](long long x, long long y) {
+            return quartet_less(h->items_host[(size_t)x], h->items_host[(size_t)y]);
+        });
+    }
+    const int4 *rej = reinterpret_cast<const int4 *>(h->h_fb + 4);
+    long long moved = 0;
+    for (unsigned int i = 0; i < n; ++i) {
+        auto it = std::lower_bound(h->item_order.begin(), h->item_order.end(), rej[i], [&](long long x, const int4 &v) {
+            return quartet_less(h->items_host[(size_t)x], v);
+        });
+        if (it == h->item_order.end()) continue;
+        const int4 &f = h->items_host[(size_t)*it];
+        if (f.x != rej[i].x || f.y != rej[i].y || f.z != rej[i].z || f.w != rej[i].w) continue;
+        int &r = h->item_rule[(size_t)*it];
+        if (r >= 0 && r < h->lg_nrules) {
+            r = h->lg_nrules;
+            ++moved;
+        }
+    }
+    return moved > 0 ? lg_rebuild_lists(h) : TCE_OK;
+}
+
 int lg_jk_passes(Handle *h, const double *dP, double *dJ, double *dK, cudaStream_t st)
 {
     int s;
@@ -525,6 +589,20 @@ int lg_jk_passes(Handle *h, const double *dP, double *dJ, double *dK, cudaStream
     if (!h->d_rules || h->item_rule.size() != h->items_host.size())
         return fail(h, TCE_ERR_STATE, "learned grid needs rules and per-item rules");
     CK(h, cudaMemsetAsync(h->d_fb_count, 0, sizeof(unsigned int), st));
+    // the plain list first, on the side stream: its few dear quartets run next
+    // to the learned-grid kernels instead of after them
+    const bool side = h->n_plain_direct > 0;
+    if (side) {
+        CK(h, cudaEventRecord(h->ev_fork, st));
+        CK(h, cudaStreamWaitEvent(h->st2, h->ev_fork, 0));
+        QuartetHostArgs b = a;
+        b.method = TCE_METHOD_PLAIN;
+        b.items = h->d_plain_items;
+        b.nitems = (int)h->n_plain_direct;
+        b.next = h->d_next2;
+        CKS(h, tce_launch_quartets(h->S, b, h->st2));
+        CK(h, cudaEventRecord(h->ev_join, h->st2));
+    }
     for (const auto &w : h->lg_lists) {
         if (w.kind == 0) {
             QuartetHostArgs b = a;
@@ -561,14 +639,8 @@ int lg_jk_passes(Handle *h, const double *dP, double *dJ, double *dK, cudaStream
             else CKS(h, tce_launch_quartets_r1_lg(h->S, w.cls, b, w.nq, w.fp32 != 0, st));
         }
     }
-    if (h->n_plain_direct > 0) {
-        QuartetHostArgs b = a;
-        b.method = TCE_METHOD_PLAIN;
-        b.items = h->d_plain_items;
-        b.nitems = (int)h->n_plain_direct;
-        b.next = h->d_next2;
-        CKS(h, tce_launch_quartets(h->S, b, st));
-    }
+    // join before the judge's fallback: both plain launches use the same per-warp scratch
+    if (side) CK(h, cudaStreamWaitEvent(st, h->ev_join, 0));
     if (h->n_lg > 0) {   // the judge's rejects, count read on the device
         QuartetHostArgs b = a;
         b.method = TCE_METHOD_PLAIN;
