@@ -23,7 +23,7 @@ int tce_launch_quartets_r1(const DevSys &S, int cls, const SArgsHost &h, cudaStr
                 tot += (S.gmax[d][g] + 1) * 8;
             }
         }
-    size_t qbytes = 8 * 64 * sizeof(int2);
+    size_t qbytes = 8 * (size_t)TCE_POOL_BYTES;     // per-warp primitive pools
     size_t tbytes = (size_t)tot * sizeof(double);
     A.t_smem = (tbytes + qbytes <= 100 * 1024) ? 1 : 0;
     A.ts_doubles = A.t_smem ? tot : 0;
@@ -71,7 +71,7 @@ int tce_launch_quartets_s(const DevSys &S, const SArgsHost &h, cudaStream_t st)
                 tot += (S.gmax[d][g] + 1) * 8;
             }
         }
-    size_t qbytes = 8 * 64 * sizeof(int2);          // per-warp batch lists
+    size_t qbytes = 8 * (size_t)TCE_POOL_BYTES;     // per-warp primitive pools
     size_t tbytes = (size_t)tot * sizeof(double);
     A.t_smem = (tbytes + qbytes <= 200 * 1024) ? 1 : 0;
     A.ts_doubles = A.t_smem ? tot : 0;

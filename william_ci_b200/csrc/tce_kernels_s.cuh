@@ -40,7 +40,9 @@ __device__ __forceinline__ bool tce_judge_accepts(double e, double M, double tol
 //   real d    : closed form for s functions, pi sqrt(D) exp(-w R^2) per direction
 //   value     : sum_k w_k prod_d I_d(t_k), contracted over the primitives.
 // The T table sits in shared memory (only rows n <= t_nmax of each 8-node
-// group), the block reduces over the warp, lane 0 scatters into J and K.
+// group), kept primitive quartets are pooled and sorted by truncation order
+// before they are cut into batches of 32, the block reduces over the warp,
+// lane 0 scatters into J and K.
 // ============================================================================
 struct SArgs {
     const int4 *items;
@@ -62,6 +64,76 @@ struct SArgs {
     unsigned int *fb_count;
 };
 
+// Per-warp pool of kept primitive quartets (shared memory): pair indices,
+// factor and sort key (the Bessel truncation order min(N_bra, N_ket), summed
+// over the periodic directions).  A full pool is sorted by key, largest
+// first, before it is cut into batches of 32 lanes, so that the lanes of a
+// batch run the n loop for about the same number of orders.
+constexpr int TCE_POOL = 128;
+constexpr int TCE_POOL_BYTES = 20 * TCE_POOL;   // int2 + double + int per entry
+struct PrimPool {
+    int2 *pq;
+    double *fac;
+    int *key;
+};
+__device__ __forceinline__ PrimPool tce_pool(void *base, int wib)
+{
+    char *p = reinterpret_cast<char *>(base) + (size_t)wib * TCE_POOL_BYTES;
+    return {reinterpret_cast<int2 *>(p), reinterpret_cast<double *>(p + 8 * TCE_POOL),
+            reinterpret_cast<int *>(p + 16 * TCE_POOL)};
+}
+
+// bitonic sort of entries [0, n) by key, descending (entries [n, m) padded
+// with key -1, m the power of two >= n); every lane owns indices lane + 32 j
+__device__ __forceinline__ void tce_pool_sort(const PrimPool &P, int n, int lane)
+{
+    int m = 64;
+    while (m < n) m <<= 1;
+    for (int i = n + lane; i < m; i += 32) P.key[i] = -1;
+    __syncwarp();
+    for (int k = 2; k <= m; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = lane; i < m; i += 32) {
+                const int x = i ^ j;
+                if (x > i) {
+                    const int a = P.key[i], b = P.key[x];
+                    const bool down = (i & k) == 0;
+                    if (down ? (a < b) : (a > b)) {
+                        P.key[i] = b;
+                        P.key[x] = a;
+                        const int2 t = P.pq[i];
+                        P.pq[i] = P.pq[x];
+                        P.pq[x] = t;
+                        const double f = P.fac[i];
+                        P.fac[i] = P.fac[x];
+                        P.fac[x] = f;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+}
+
+// move the entries [from, from + rest) of the pool to its front (rest < 32)
+__device__ __forceinline__ void tce_pool_carry(const PrimPool &P, int from, int rest, int lane)
+{
+    int2 q = make_int2(0, 0);
+    double f = 0.0;
+    int k = 0;
+    if (lane < rest) {
+        q = P.pq[from + lane];
+        f = P.fac[from + lane];
+        k = P.key[from + lane];
+    }
+    __syncwarp();
+    if (lane < rest) {
+        P.pq[lane] = q;
+        P.fac[lane] = f;
+        P.key[lane] = k;
+    }
+    __syncwarp();
+}
+
 // queue a quartet the judge rejected (lane 0)
 __device__ __forceinline__ void tce_queue_fallback(const SArgs &A, int4 q)
 {
@@ -76,8 +148,7 @@ __global__ void __launch_bounds__(256, NDP == 1 ? 2 : 1) k_quartets_s(DevSys S, 
     extern __shared__ double smem[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     double *Tsm = smem;
-    int2 *qlist = reinterpret_cast<int2 *>(smem + A.ts_doubles) + wib * 64;
-    double *qfac = reinterpret_cast<double *>(qlist + 32);
+    const PrimPool Pool = tce_pool(smem + A.ts_doubles, wib);
     // T rows n <= gmax of each group, 8 nodes per row (compact, copied once per CTA)
     if (!LG && A.t_smem) {
         for (int d = 0; d < NDP; ++d)
@@ -122,11 +193,11 @@ __global__ void __launch_bounds__(256, NDP == 1 ? 2 : 1) k_quartets_s(DevSys S, 
         const int nppb = Ub.npp, nppk = Uk.npp;
         const long long total = (long long)nppb * nppk;
         double blk = 0.0, blkG = 0.0;
-        int nb = 0;
+        int np = 0;
         for (long long base = 0; base < total; base += 32) {
             long long idx = base + lane;
             bool keep = idx < total;
-            int ipb = 0, ipk = 0;
+            int ipb = 0, ipk = 0, key = 0;
             double fac = 0.0;
             if (keep) {
                 ipb = (int)(idx / nppk);
@@ -141,27 +212,28 @@ __global__ void __launch_bounds__(256, NDP == 1 ? 2 : 1) k_quartets_s(DevSys S, 
                 if (keep) {   // fold the four contraction coefficients into the factor
                     fac *= S.sh_coef[S.sh_coff[q.x] + ipb / Ub.np2] * S.sh_coef[S.sh_coff[q.y] + ipb % Ub.np2] *
                            S.sh_coef[S.sh_coff[q.z] + ipk / Uk.np2] * S.sh_coef[S.sh_coff[q.w] + ipk % Uk.np2];
+#pragma unroll
+                    for (int d = 0; d < NDP; ++d) key += Pb.N[d] < Pk.N[d] ? Pb.N[d] : Pk.N[d];
                 }
             }
             const unsigned msk = __ballot_sync(0xffffffffu, keep);
             const int pos = __popc(msk & ((1u << lane) - 1u));
-            const int cnt = __popc(msk);
-            int done = 0;
-            while (done < cnt) {
-                int take = 32 - nb;
-                if (take > cnt - done) take = cnt - done;
-                if (keep && pos >= done && pos < done + take) {
-                    qlist[nb + pos - done] = make_int2(ipb, ipk);
-                    qfac[nb + pos - done] = fac;
-                }
-                nb += take;
-                done += take;
-                __syncwarp();
-                bool flush = (nb == 32) || (base + 32 >= total && done == cnt);
-                if (flush) {
+            if (keep) {
+                Pool.pq[np + pos] = make_int2(ipb, ipk);
+                Pool.fac[np + pos] = fac;
+                Pool.key[np + pos] = key;
+            }
+            np += __popc(msk);
+            __syncwarp();
+            const bool last = base + 32 >= total;
+            if (np > TCE_POOL - 32 || (last && np > 0)) {
+                if (np > 32) tce_pool_sort(Pool, np, lane);
+                const int nproc = last ? np : (np & ~31);
+                for (int b0 = 0; b0 < nproc; b0 += 32) {
+                    const int nb = nproc - b0 < 32 ? nproc - b0 : 32;
                     if (lane < nb) {
-                        const int2 pq = qlist[lane];
-                        const double f = qfac[lane];
+                        const int2 pq = Pool.pq[b0 + lane];
+                        const double f = Pool.fac[b0 + lane];
                         const PairPrim &Pb = S.pp[Ub.pp_off + pq.x];
                         const PairPrim &Pk = S.pp[Uk.pp_off + pq.y];
                         double prod[NDP > 1 ? NQ : 1];
@@ -295,9 +367,10 @@ __global__ void __launch_bounds__(256, NDP == 1 ? 2 : 1) k_quartets_s(DevSys S, 
                         blk = fma(f, val, blk);
                         if (LG) blkG = fma(f, valG, blkG);
                     }
-                    nb = 0;
-                    __syncwarp();
                 }
+                __syncwarp();
+                if (np > nproc) tce_pool_carry(Pool, nproc, np - nproc, lane);
+                np -= nproc;
             }
         }
         blk = tce_warp_sum(blk);
@@ -355,8 +428,7 @@ __global__ void __launch_bounds__(256, LG ? 2 : 1) k_quartets_r1(DevSys S, SArgs
     extern __shared__ double smem[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     double *Tsm = smem;
-    int2 *qlist = reinterpret_cast<int2 *>(smem + A.ts_doubles) + wib * 64;
-    double *qfac = reinterpret_cast<double *>(qlist + 32);
+    const PrimPool Pool = tce_pool(smem + A.ts_doubles, wib);
     if (!LG && A.t_smem) {
         for (int g = 0; g < NG; ++g) {
             int rows = S.gmax[0][g] + 1;
@@ -399,11 +471,11 @@ __global__ void __launch_bounds__(256, LG ? 2 : 1) k_quartets_r1(DevSys S, SArgs
         for (int c = 0; c < NCQ; ++c) blk[c] = 0.0;
 #pragma unroll
         for (int c = 0; c < (LG ? NCQ : 1); ++c) blkG[c] = 0.0;
-        int nb = 0;
+        int np = 0;
         for (long long base = 0; base < total; base += 32) {
             long long idx = base + lane;
             bool keep = idx < total;
-            int ipb = 0, ipk = 0;
+            int ipb = 0, ipk = 0, key = 0;
             double fac = 0.0;
             if (keep) {
                 ipb = (int)(idx / nppk);
@@ -415,24 +487,25 @@ __global__ void __launch_bounds__(256, LG ? 2 : 1) k_quartets_r1(DevSys S, SArgs
                 if (bra * Uk.ket_max <= 2.22e-16) keep = false;
                 else if (fabs(fac) * Pb.cmax12 * Pk.cmax12 <= 2.22e-16) keep = false;
                 else if (A.prim_screen && Pb.ps * Pk.ps < S.prim_thr) keep = false;
+                key = Pb.N[0] < Pk.N[0] ? Pb.N[0] : Pk.N[0];
             }
             const unsigned msk = __ballot_sync(0xffffffffu, keep);
             const int pos = __popc(msk & ((1u << lane) - 1u));
-            const int cnt = __popc(msk);
-            int done = 0;
-            while (done < cnt) {
-                int take = 32 - nb;
-                if (take > cnt - done) take = cnt - done;
-                if (keep && pos >= done && pos < done + take) {
-                    qlist[nb + pos - done] = make_int2(ipb, ipk);
-                    qfac[nb + pos - done] = fac;
-                }
-                nb += take;
-                done += take;
-                __syncwarp();
-                if ((nb == 32) || (base + 32 >= total && done == cnt)) {
+            if (keep) {
+                Pool.pq[np + pos] = make_int2(ipb, ipk);
+                Pool.fac[np + pos] = fac;
+                Pool.key[np + pos] = key;
+            }
+            np += __popc(msk);
+            __syncwarp();
+            const bool last = base + 32 >= total;
+            if (np > TCE_POOL - 32 || (last && np > 0)) {
+                if (np > 32) tce_pool_sort(Pool, np, lane);
+                const int nproc = last ? np : (np & ~31);
+                for (int b0 = 0; b0 < nproc; b0 += 32) {
+                    const int nb = nproc - b0 < 32 ? nproc - b0 : 32;
                     if (lane < nb) {
-                        const int2 pq = qlist[lane];
+                        const int2 pq = Pool.pq[b0 + lane];
                         const PairPrim &Pb = S.pp[Ub.pp_off + pq.x];
                         const PairPrim &Pk = S.pp[Uk.pp_off + pq.y];
                         const int i = pq.x / Ub.np2, j = pq.x - i * Ub.np2;
@@ -591,7 +664,7 @@ __global__ void __launch_bounds__(256, LG ? 2 : 1) k_quartets_r1(DevSys S, SArgs
                             }
                         }
                         }
-                        const double fac = qfac[lane];
+                        const double fac = Pool.fac[b0 + lane];
 #pragma unroll
                         for (int c = 0; c < NCQ; ++c) {
                             const int ca = c % NA, cb = (c / NA) % NB, cc = (c / (NA * NB)) % NC, cd = c / (NA * NB * NC);
@@ -601,9 +674,10 @@ __global__ void __launch_bounds__(256, LG ? 2 : 1) k_quartets_r1(DevSys S, SArgs
                             if (LG) blkG[LG ? c : 0] = fma(fac * cf, valG[LG ? c : 0], blkG[LG ? c : 0]);
                         }
                     }
-                    nb = 0;
-                    __syncwarp();
                 }
+                __syncwarp();
+                if (np > nproc) tce_pool_carry(Pool, nproc, np - nproc, lane);
+                np -= nproc;
             }
         }
         const int fI = S.sh_first[q.x], fJ = S.sh_first[q.y], fK = S.sh_first[q.z], fL = S.sh_first[q.w];

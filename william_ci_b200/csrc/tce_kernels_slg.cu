@@ -30,7 +30,7 @@ static void lg_args(SArgs &A, const SArgsHost &h)
 template <class Kern>
 static void launch(Kern k, const DevSys &S, const SArgs &A, int nsm, cudaStream_t st)
 {
-    const size_t smem = 8 * 64 * sizeof(int2);   // per-warp batch lists
+    const size_t smem = 8 * (size_t)TCE_POOL_BYTES;   // per-warp primitive pools
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, 256, smem);
