@@ -15,6 +15,7 @@
 // Consumers of a block: Schwarz / parity blocks, the primitive Schwarz table,
 // the J/K scatter (direct_JK, eri_direct.f90:331-357) and the stored-ERI
 // scatter (ERI_toroidal.f90:416-454).
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -442,7 +443,7 @@ __device__ __forceinline__ int item_count(const QuartetArgs &A)
 // method 0: one fixed rule for every item (the system's rule, or dictionary rule
 // rule_override, judged when blk_out2 is set); method 1: the learned grid.
 template <int NQ>
-__global__ void __launch_bounds__(128) k_quartets(DevSys S, QuartetArgs A)
+__global__ void __launch_bounds__(256) k_quartets(DevSys S, QuartetArgs A)
 {
     extern __shared__ double smem[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -698,14 +699,38 @@ __global__ void __launch_bounds__(128) k_plain(DevSys S, QuartetArgs A)
 // ---------------------------------------------------------------------------
 // launch
 // ---------------------------------------------------------------------------
+// Warps per block and blocks per SM of k_quartets<NQ> for a per-warp buffer of
+// wbytes: the shape with the most warps resident on an SM (shared memory and
+// registers decide), found once per (NQ, wbytes) with the occupancy calculator.
 template <int NQ>
-static cudaError_t launch_nq(const DevSys &S, const QuartetArgs &A, size_t smem, int warps, int nsm, cudaStream_t st)
+static int2 quartet_shape(size_t wbytes)
 {
+    static std::mutex mu;
+    static std::map<size_t, int2> known;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = known.find(wbytes);
+    if (it != known.end()) return it->second;
+    int2 best = make_int2(0, 0);   // (warps, blocks per SM)
+    for (int w = 8; w >= 1; --w) {
+        const size_t smem = wbytes * (size_t)w;
+        if (smem > 220 * 1024) continue;
+        cudaFuncSetAttribute(k_quartets<NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        int per = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_quartets<NQ>, 32 * w, smem) != cudaSuccess) per = 0;
+        if (per * w > best.x * best.y) best = make_int2(w, per);
+    }
+    known[wbytes] = best;
+    return best;
+}
+
+template <int NQ>
+static cudaError_t launch_nq(const DevSys &S, const QuartetArgs &A, size_t wbytes, int nsm, cudaStream_t st)
+{
+    const int2 sh = quartet_shape<NQ>(wbytes);
+    if (sh.x < 1 || sh.y < 1) return cudaErrorInvalidConfiguration;
+    const size_t smem = wbytes * (size_t)sh.x;
     cudaFuncSetAttribute(k_quartets<NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int per = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_quartets<NQ>, 32 * warps, smem);
-    if (per < 1) per = 1;
-    k_quartets<NQ><<<nsm * per, 32 * warps, smem, st>>>(S, A);
+    k_quartets<NQ><<<nsm * sh.y, 32 * sh.x, smem, st>>>(S, A);
     return cudaGetLastError();
 }
 
@@ -833,10 +858,10 @@ int tce_launch_quartets(const DevSys &S, const QuartetHostArgs &h, cudaStream_t 
         if (grid < 1) return TCE_ERR_NOMEM;
         k_plain<<<(unsigned)grid, 32 * warps, smem, st>>>(S, A);
         e = cudaGetLastError();
-    } else if (nq == 32) e = launch_nq<32>(S, A, smem, warps, nsm, st);
-    else if (nq == 40) e = launch_nq<40>(S, A, smem, warps, nsm, st);
-    else if (nq == 64) e = launch_nq<64>(S, A, smem, warps, nsm, st);
-    else if (nq == 128) e = launch_nq<128>(S, A, smem, warps, nsm, st);
+    } else if (nq == 32) e = launch_nq<32>(S, A, wbytes, nsm, st);
+    else if (nq == 40) e = launch_nq<40>(S, A, wbytes, nsm, st);
+    else if (nq == 64) e = launch_nq<64>(S, A, wbytes, nsm, st);
+    else if (nq == 128) e = launch_nq<128>(S, A, wbytes, nsm, st);
     else return TCE_ERR_UNSUPPORTED;
     return e == cudaSuccess ? TCE_OK : TCE_ERR_CUDA;
 }
