@@ -169,6 +169,13 @@ int tce_last_kernel_ms(void *handle, double *ms);
  * lists change.  Default off. */
 int tce_set_graph(void *handle, int32_t on);
 
+/* Node sums of the learned-grid pass on the FP64 tensor cores (mma.sync
+ * m8n8k4, FP64 in and out) where a kernel has that form: the all-s quartets
+ * of one periodic direction (FP64 quartets; the FP32-panel quartets keep
+ * their kernel).  Default on; off gives the FP64 CUDA-core kernels.  Same
+ * arithmetic type, different summation order.  No reference counterpart. */
+int tce_set_tensor_cores(void *handle, int32_t on);
+
 /* Multi-GPU: restrict tce_direct_jk[_device] on this handle to shard `rank`
  * of `nranks` (cost-balanced partition of the unique shell quartets, the same
  * partition on every rank).  The partial J/K of the ranks sum to the full J/K;

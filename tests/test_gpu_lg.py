@@ -299,3 +299,28 @@ def test_rejects_move_to_the_plain_list(chain16_lg):
             assert eng.pass_kernels() >= 2      # at least the plain list and the judge's fallback
     finally:
         eng.set_graph(False)
+
+
+def test_tensor_core_node_sums_match_cuda_cores(chain16_lg):
+    """All-s learned-grid quartets with the node sums on the FP64 tensor cores
+    (mma.sync m8n8k4) against the FP64 CUDA-core kernel: same J/K up to the
+    summation order."""
+    from william_ci_b200.engine import TCE_METHOD_LEARNED
+    sysm, eng, net = chain16_lg
+    P = random_density(sysm.nbas, 7) * 0.05
+    scale = np.abs(P).sum()
+    eng.set_method(TCE_METHOD_LEARNED)
+    eng.set_fp32_threshold(0.0)
+    eng.set_graph(False)
+    try:
+        out = {}
+        for tc in (False, True):
+            eng.set_tensor_cores(tc)
+            for _ in range(2):                 # the second pass: the judge's rejects routed
+                J, K = eng.direct_JK(P)
+            out[tc] = (J, K, eng.lg_stats())
+        assert out[False][2]["rejected"] == 0 and out[True][2]["rejected"] == 0
+        for a, b in zip(out[False][:2], out[True][:2]):
+            assert np.abs(a - b).max() <= 1e-12 * scale, np.abs(a - b).max() / scale
+    finally:
+        eng.set_tensor_cores(True)

@@ -865,6 +865,15 @@ int tce_set_graph(void *handle, int32_t on)
     return TCE_OK;
 }
 
+int tce_set_tensor_cores(void *handle, int32_t on)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h) return fail(h, TCE_ERR_ARG, "NULL handle");
+    h->use_tc = on ? 1 : 0;
+    ++h->work_version;   // a captured pass is re-captured
+    return TCE_OK;
+}
+
 int tce_fp64_peak(double *tflops)
 {
     if (!tflops) return fail(nullptr, TCE_ERR_ARG, "NULL argument");

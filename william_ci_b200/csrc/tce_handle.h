@@ -110,6 +110,7 @@ struct Handle {
     unsigned int *d_next3 = nullptr;
     // CUDA graph of the J/K pass (tce_set_graph); rebuilt when any key changes
     int use_graph = 0;
+    int use_tc = 1;                      // FP64 tensor-core node sums where a kernel has them
     int blocks_only = 0;                 // tce_create_blocks: no Schwarz, primitive table or quartet list
     long long work_version = 0;          // bumped whenever work lists are rebuilt
     cudaGraphExec_t jk_exec = nullptr;

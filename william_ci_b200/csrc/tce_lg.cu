@@ -635,7 +635,8 @@ int lg_jk_passes(Handle *h, const double *dP, double *dJ, double *dK, cudaStream
             b.judge_tol = h->judge_tol;
             b.fb_items = h->d_fb_items;
             b.fb_count = h->d_fb_count;
-            if (w.kind == 1) CKS(h, tce_launch_quartets_s_lg(h->S, b, w.nq, w.fp32 != 0, st));
+            if (w.kind == 1 && h->use_tc && h->ndp == 1 && !w.fp32) CKS(h, tce_launch_quartets_s_tc(h->S, b, w.nq, st));
+            else if (w.kind == 1) CKS(h, tce_launch_quartets_s_lg(h->S, b, w.nq, w.fp32 != 0, st));
             else CKS(h, tce_launch_quartets_r1_lg(h->S, w.cls, b, w.nq, w.fp32 != 0, st));
         }
     }
