@@ -86,6 +86,9 @@ int tce_launch_quartets_r1_lg(const DevSys &S, int cls, const SArgsHost &h, int 
 // all-s quartets of one periodic direction, learned grid, node sums on the FP64
 // tensor cores (k_quartets_s_tc, mma.sync m8n8k4)
 int tce_launch_quartets_s_tc(const DevSys &S, const SArgsHost &h, int nq, cudaStream_t st);
+// one-p s/p classes of one periodic direction, learned grid, tensor-core node
+// sums (k_quartets_r1_tc); cls as tce_launch_quartets_r1
+int tce_launch_quartets_r1_tc(const DevSys &S, int cls, const SArgsHost &h, int nq, cudaStream_t st);
 inline bool tce_r1_supported(int ndp, int nq, int cls)
 {
     return ndp == 1 && nq == 32 && cls >= 0 && cls < 16 && __builtin_popcount(cls) == 1;

@@ -637,6 +637,9 @@ int lg_jk_passes(Handle *h, const double *dP, double *dJ, double *dK, cudaStream
             b.fb_count = h->d_fb_count;
             if (w.kind == 1 && h->use_tc && h->ndp == 1 && !w.fp32) CKS(h, tce_launch_quartets_s_tc(h->S, b, w.nq, st));
             else if (w.kind == 1) CKS(h, tce_launch_quartets_s_lg(h->S, b, w.nq, w.fp32 != 0, st));
+            // one-p classes: the tensor-core kernel for 32-node rules (measured faster there;
+            // with 64-node rules the CUDA-core kernel is faster)
+            else if (h->use_tc && !w.fp32 && w.nq == 32) CKS(h, tce_launch_quartets_r1_tc(h->S, w.cls, b, w.nq, st));
             else CKS(h, tce_launch_quartets_r1_lg(h->S, w.cls, b, w.nq, w.fp32 != 0, st));
         }
     }
