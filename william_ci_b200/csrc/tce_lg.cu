@@ -396,6 +396,7 @@ static void fill_common(Handle *h, QuartetHostArgs &a)
     a.max_ncq = h->max_ncq;
     a.fixed_gmax = h->d_gmax;
     a.num_sms = h->num_sms;
+    a.use_tc = h->use_tc;
     a.rules = h->d_rules;
     a.rule_T = h->d_rule_T;
     a.rule_t = h->d_rule_t;

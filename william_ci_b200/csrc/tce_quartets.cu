@@ -48,6 +48,7 @@ struct QuartetArgs {
     int eri_size, physicist;
     PairPrim *pp_rw;
     int rowcap, cstride, blkcap, warp_smem_doubles;
+    int use_tc;
     const int *fixed_gmax;
     // learned grid
     const RuleDev *rules;
@@ -153,17 +154,168 @@ __device__ __forceinline__ WarpBuf warp_buf(const QuartetArgs &A, double *ws, in
     return b;
 }
 
+__device__ __forceinline__ void tce_dmma(double &d0, double &d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// The rows of row_dot for a batch, one periodic direction, on the FP64
+// tensor cores: the batch's nb * R rows (primitive quartet x power
+// combination) in chunks of 32 are the A operand (32 x N, F = Re[G_n H_n
+// e^{i n phi}]), the rule's T table the B operand (N x 32 nodes per pass);
+// mma.sync.m8n8k4 per 8 x 8 tile and step of four orders.  Lane l builds the
+// A fragments of rows 8 m + l/4 (m = 0..3) at order 4 s + l%4, cos and sin
+// of n phi by the three-term recurrence in steps of four (re-seeded every 32
+// orders), and loads the next step's G, H and T before the current step's
+// mma instructions.  Output as row_dot: rows[r * (NQ + 1) + k] = sgn I_r(t_k).
+template <int NQ>
+__device__ void tc_rows(const DevSys &S, const RuleView &Rv, const QCtx &Q, int nb, const WarpBuf &b, int lane)
+{
+    constexpr int RS = NQ + 1;
+    const int rq = lane >> 2, cq = lane & 3;
+    const int lsA = Q.lsA, lsB = Q.lsB, lsC = Q.lsC, lsD = Q.lsD, R = Q.R;
+    const int nppb = Q.Ub.npp, nppk = Q.Uk.npp;
+    const int nrows = nb * R;
+    const double *T = Rv.T;
+    const int *gm = Rv.gmax;
+    for (int r0 = 0; r0 < nrows; r0 += 32) {
+        int goff[4], hoff[4], nmr[4];
+        double sg[4];
+        int nmax = -1;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const int r = r0 + 8 * m + rq;
+            nmr[m] = -1;
+            goff[m] = hoff[m] = 0;
+            sg[m] = 0.0;
+            if (r < nrows) {
+                const int p = r / R, cmb = r - p * R;
+                const int ia = cmb % (lsA + 1), t1 = cmb / (lsA + 1);
+                const int ib = t1 % (lsB + 1), t2 = t1 / (lsB + 1);
+                const int ic = t2 % (lsC + 1), id = t2 / (lsC + 1);
+                const int2 pq = b.qlist[p];
+                const PairPrim &Pb = S.pp[Q.Ub.pp_off + pq.x];
+                const PairPrim &Pk = S.pp[Q.Uk.pp_off + pq.y];
+                nmr[m] = Pb.N[0] < Pk.N[0] ? Pb.N[0] : Pk.N[0];
+                goff[m] = (int)((((long long)ia * (lsB + 1) + ib) * 2 + 0) * Q.Ub.Nlen * nppb + pq.x);
+                hoff[m] = (int)((((long long)ic * (lsD + 1) + id) * 2 + 1) * Q.Uk.Nlen * nppk + pq.y);
+                sg[m] = pow(S.a[0], -(double)(ia + ib + ic + id));
+                nmax = nmr[m] > nmax ? nmr[m] : nmax;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
+        auto phase = [&](int m) {
+            const int r = r0 + 8 * m + rq;
+            if (r >= nrows) return 0.0;
+            const int2 pq = b.qlist[r / R];
+            return S.a[0] * (S.pp[Q.Ub.pp_off + pq.x].cen[0] - (S.pp[Q.Uk.pp_off + pq.y].cen[0] + Q.Tsh[0]));
+        };
+        const double2 *Gv = S.vec + Q.Ub.vec_off, *Hv = S.vec + Q.Uk.vec_off;
+#pragma unroll 1
+        for (int g0 = 0; g0 < NQ / 8; g0 += 4) {
+            int gmb[4], nend = -1;
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                gmb[t] = gm[g0 + t];
+                nend = gmb[t] > nend ? gmb[t] : nend;
+            }
+            nend = nend < nmax ? nend : nmax;
+            double acc[32];
+#pragma unroll
+            for (int x = 0; x < 32; ++x) acc[x] = 0.0;
+            double cc[4], cp[4], sc[4], sp[4], c4[4];
+            double2 gN[4], hN[4];
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                const double ph = phase(m);
+                sincos((double)cq * ph, &sc[m], &cc[m]);
+                sincos((double)(cq - 4) * ph, &sp[m], &cp[m]);
+                c4[m] = 2.0 * cos(4.0 * ph);
+                const bool ok = cq <= nmr[m];
+                gN[m] = ok ? __ldg(Gv + goff[m] + (size_t)cq * nppb) : make_double2(0.0, 0.0);
+                hN[m] = ok ? __ldg(Hv + hoff[m] + (size_t)cq * nppk) : make_double2(0.0, 0.0);
+            }
+            double tN[4];
+#pragma unroll
+            for (int t = 0; t < 4; ++t)
+                tN[t] = (0 <= gmb[t] && cq <= S.ncap) ? __ldg(T + (size_t)cq * NQ + 8 * (g0 + t) + rq) : 0.0;
+            for (int s4 = 0; s4 <= nend; s4 += 4) {
+                const int n = s4 + cq, n1 = n + 4;
+                double F[4], Tb[4];
+#pragma unroll
+                for (int m = 0; m < 4; ++m) {
+                    const double2 gv = gN[m], hv = hN[m];
+                    const double ar = gv.x * hv.x - gv.y * hv.y, ai = gv.x * hv.y + gv.y * hv.x;
+                    F[m] = ar * cc[m] - ai * sc[m];
+                    const bool ok = n1 <= nmr[m];
+                    gN[m] = ok ? __ldg(Gv + goff[m] + (size_t)n1 * nppb) : make_double2(0.0, 0.0);
+                    hN[m] = ok ? __ldg(Hv + hoff[m] + (size_t)n1 * nppk) : make_double2(0.0, 0.0);
+                }
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    Tb[t] = tN[t];
+                    tN[t] = (s4 + 4 <= gmb[t] && n1 <= S.ncap) ? __ldg(T + (size_t)n1 * NQ + 8 * (g0 + t) + rq) : 0.0;
+                }
+                if (((s4 + 4) & 31) == 0) {
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) {
+                        const double ph = phase(m);
+                        sincos((double)n * ph, &sp[m], &cp[m]);
+                        sincos((double)n1 * ph, &sc[m], &cc[m]);
+                    }
+                } else {
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) {
+                        const double tc_ = c4[m] * cc[m] - cp[m], ts_ = c4[m] * sc[m] - sp[m];
+                        cp[m] = cc[m];
+                        cc[m] = tc_;
+                        sp[m] = sc[m];
+                        sc[m] = ts_;
+                    }
+                }
+#pragma unroll
+                for (int t = 0; t < 4; ++t)
+                    if (s4 <= gmb[t]) {
+#pragma unroll
+                        for (int m = 0; m < 4; ++m) tce_dmma(acc[8 * m + 2 * t], acc[8 * m + 2 * t + 1], F[m], Tb[t]);
+                    }
+            }
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                const int r = r0 + 8 * m + rq;
+                if (r >= nrows) continue;
+#pragma unroll
+                for (int t = 0; t < 4; ++t)
+#pragma unroll
+                    for (int i = 0; i < 2; ++i) b.rows[(size_t)r * RS + 8 * (g0 + t) + 2 * cq + i] = acc[8 * m + 2 * t + i] * sg[m];
+            }
+        }
+    }
+}
+
 // Phases 1+2 for a batch of nb primitive quartets, accumulating into blkK (and blkG)
 template <int NQ, bool RO>
 __device__ void process_batch(const DevSys &S, const RuleView &Rv, const QCtx &Q, int nb, const WarpBuf &b, int lane,
-                              int cstride)
+                              int cstride, bool tc)
 {
     constexpr int RS = NQ + 1;
     const int ndp = S.ndp, nreal = 3 - ndp;
     const int lsA = Q.lsA, lsB = Q.lsB, lsC = Q.lsC, lsD = Q.lsD, ncomb = Q.ncomb, R = Q.R;
     const int nppb = Q.Ub.npp, nppk = Q.Uk.npp;
     const int nrows = nb * R;
-    for (int r = lane; r < nrows; r += 32) {
+    bool rows_done = false;
+    // tensor-core rows for 64-node rules (measured faster there; with 32-node
+    // rules the lane-per-row loop below is faster)
+    if constexpr (RO && NQ == 64) {
+        if (tc && ndp == 1) {
+            tc_rows<NQ>(S, Rv, Q, nb, b, lane);
+            rows_done = true;
+        }
+    }
+    for (int r = lane; r < (rows_done ? 0 : nrows); r += 32) {
         int p = r / R, rem = r - p * R;
         int d = rem / ncomb, cmb = rem - d * ncomb;
         int ia = cmb % (lsA + 1), t1 = cmb / (lsA + 1);
@@ -336,13 +488,13 @@ __device__ void eval_block(const DevSys &S, const QuartetArgs &A, const RuleView
             done += take;
             __syncwarp();
             if (nb == B) {
-                process_batch<NQ, RO>(S, Rv, Q, nb, b, lane, A.cstride);
+                process_batch<NQ, RO>(S, Rv, Q, nb, b, lane, A.cstride, A.use_tc != 0);
                 nb = 0;
                 __syncwarp();
             }
         }
     }
-    if (nb > 0) process_batch<NQ, RO>(S, Rv, Q, nb, b, lane, A.cstride);
+    if (nb > 0) process_batch<NQ, RO>(S, Rv, Q, nb, b, lane, A.cstride, A.use_tc != 0);
     __syncwarp();
 }
 
@@ -798,6 +950,7 @@ int tce_launch_quartets(const DevSys &S, const QuartetHostArgs &h, cudaStream_t 
     A.eri_size = h.eri_size;
     A.physicist = h.physicist;
     A.pp_rw = h.pp_rw;
+    A.use_tc = h.use_tc;
     A.fixed_gmax = h.fixed_gmax;
     A.rules = h.rules;
     A.rule_T = h.rule_T;
