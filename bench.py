@@ -42,7 +42,7 @@ METRIC = "toroidal ERI quartets/s at ≤1e-10 err, learned-grid vs plain; RHF SC
 WORKLOAD = "h_chain64"
 SYSTEM_FIXTURE = os.path.join(ROOT, "tests", "golden", "systems", WORKLOAD + ".npz")
 ONEE_FIXTURE = os.path.join(ROOT, "tests", "golden", "systems", WORKLOAD + "_onee.npz")
-PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "k_quartets_h_chain64_traffic.json")
+PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "jk_pass_learned_grid_h_chain64_traffic.json")
 L2_FLUSH_BYTES = 512 << 20
 FP32_THRESHOLD = 1e-6        # Schwarz product below which the node sums run in FP32
 
@@ -442,11 +442,12 @@ def main():
     traffic = None
     if os.path.exists(PROFILE_TRAFFIC):
         try:
-            traffic = json.load(open(PROFILE_TRAFFIC)).get("dram_bytes_per_launch")
+            traffic = json.load(open(PROFILE_TRAFFIC)).get("dram_bytes_per_pass")
         except Exception:
             traffic = None
-    roofline = {"bound": "fp64", "kernel": "k_quartets<32|64> learned grid (per-quartet rule, judge, fused J/K "
-                                           "scatter) + the plain fallback launch",
+    roofline = {"bound": "fp64", "kernel": "the learned-grid J/K pass, one CUDA graph: k_quartets<32|64>, "
+                                           "k_quartets_s[_tc], k_quartets_r1[_tc] (per-quartet rule, judge, fused "
+                                           "J/K scatter) and the plain launches",
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if (achieved and peak) else None, "traffic": traffic,
                 "peak_source": "measured FP64 FMA throughput of this GPU (tce_fp64_peak probe); MEASURED_PEAKS.json "
