@@ -178,6 +178,16 @@ int tce_set_graph(void *handle, int32_t on);
  * arithmetic type, different summation order.  No reference counterpart. */
 int tce_set_tensor_cores(void *handle, int32_t on);
 
+/* Nuclear attraction matrix of the handle's system (replaces
+ * nuclear_attraction_matrix_toroidal_{1,2,3}D, 1D_Nuclear_attraction_toroidal.f90
+ * :169-276 / 3D_Nuclear_attraction_toroidal.f90:113-196, with the per-pair
+ * integral of :26-163 / :18-111): V (nbas x nbas, column-major) with the rows
+ * of the unit cell computed on the device (|V| < 1e-14 set to zero) and the
+ * other rows by translation, as the reference's fill_with_symmetry.  geometry
+ * is the reference's geometry(natoms, 3), column-major (x of every atom, then
+ * y, then z); Z the nuclear charges.  Uses the handle's t-rule and tables. */
+int tce_nuclear_attraction(void *handle, int32_t natoms, const double *geometry, const int32_t *Z, double *V);
+
 /* Multi-GPU: restrict tce_direct_jk[_device] on this handle to shard `rank`
  * of `nranks` (cost-balanced partition of the unique shell quartets, the same
  * partition on every rank).  The partial J/K of the ranks sum to the full J/K;

@@ -1,0 +1,265 @@
+// tce_onee.cu -- nuclear attraction matrix on the device.
+//
+// NA(i, j) = -sum_atoms Z_C <i| 1/|r - C| |j> for i in the unit cell, j in
+// the supercell: nuclear_attraction_integral_toroidal_{1,2,3}D
+// (1D_Nuclear_attraction_toroidal.f90:26-163, 3D_Nuclear_attraction_toroidal.f90
+// :18-111) with the handle's t-rule and T table, then |NA| < 1e-14 set to
+// zero and the other cells' rows by translation (nuclear_attraction_matrix_
+// toroidal_1D, :169-276; fill_with_symmetry, symmetric_matrix.f90:1-52).
+//
+// Per primitive pair the integral is
+//   (2/sqrt(pi)) c1 c2 prod_periodic[e^{-2(p - pe)/a^2} L / a^M] prod_real e^{-mu R^2}
+//   x sum_k w_k prod_d X_d(t_k),
+// periodic d: X_d = sum_n F_n T[n][k], F_n = Re[(G_n) e^{i n phi_C}], G_n the
+// pair's Fourier-Bessel vector sum_j d_j e^{-A} I_{|n+j|}(A), phi_C = a (P - C);
+// real d: X_d = e^{-p eta (P - C)^2} S_1D(l1, l2, p + t^2, PA - eta PC, PB - eta PC),
+// eta = t^2 / (p + t^2).
+//
+// One warp per function pair (i, j).  Lane 0 runs the Miller recurrence of
+// e^{-A} I_n(A) (bessel_scaled_vector_fast, clifford_tools.f90:429-461) into
+// shared memory; the lanes build G_n over n, then per atom F_n over n (a
+// rotation by e^{32 i phi} per step of the lane's n) and finally the node
+// sums over k (lanes over nodes, F broadcast from shared memory, T rows
+// coalesced), reduced over the warp.
+#include <vector>
+
+#include "tce_handle.h"
+
+namespace {
+
+constexpr double PI_D = 3.14159265358979323846;
+constexpr int NA_WARPS_MAX = 8;
+constexpr int NA_MEXTRA = 4 * TCE_LMAX + 4;   // Bessel orders past N for the Fourier product
+
+// 1D overlap of x^j e^{-p (x - PA')...}: sum_k sum_q C(j,k) C(m,q) pa^{j-k} pb^{m-q}
+// <x^{k+q}>, moments (n-1)!! / (2p)^{n/2} sqrt(pi/p) (overlap_1D_real, :336-361)
+__device__ double na_overlap_1d(int j, int m, double p, double pa, double pb)
+{
+    double mom[2 * TCE_LMAX + 1];
+    mom[0] = sqrt(PI_D / p);
+    if (j + m >= 1) mom[1] = 0.0;
+    for (int n = 2; n <= j + m; ++n) mom[n] = (n & 1) ? 0.0 : mom[n - 2] * (double)(n - 1) / (2.0 * p);
+    double acc = 0.0, bj = 1.0;
+    for (int k = 0; k <= j; ++k) {
+        double bm = 1.0;
+        for (int q = 0; q <= m; ++q) {
+            if (((k + q) & 1) == 0) acc += bj * bm * pow(pa, (double)(j - k)) * pow(pb, (double)(m - q)) * mom[k + q];
+            bm = bm * (double)(m - q) / (double)(q + 1);
+        }
+        bj = bj * (double)(j - k) / (double)(k + 1);
+    }
+    return acc;
+}
+
+struct NaArgs {
+    const int2 *fsh;     // per function: shell, component
+    int natoms;
+    const double *geo;   // [natoms + natoms * d] (Fortran geometry(natoms, 3))
+    const int *Z;
+    double *V;           // rows of the unit cell: V[i + nfuc * j]
+    int wdoubles;        // shared doubles per warp
+};
+
+__global__ void __launch_bounds__(NA_WARPS_MAX * 32) k_nuclear(DevSys S, NaArgs A)
+{
+    extern __shared__ double smem[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const long long pair = (long long)blockIdx.x * (blockDim.x >> 5) + wib;
+    if (pair >= (long long)S.nfuc * S.nbas) return;
+    const int fi = (int)(pair % S.nfuc), fj = (int)(pair / S.nfuc);
+    const int NW = S.ncap + 1;
+    double *Iv = smem + (size_t)wib * A.wdoubles;            // NW + NA_MEXTRA
+    double *Gre = Iv + NW + NA_MEXTRA;                        // [ndp][NW] each
+    double *Gim = Gre + 3 * NW;
+    double *F = Gim + 3 * NW;
+    const int2 a1 = A.fsh[fi], a2 = A.fsh[fj];
+    const int S1 = a1.x, S2 = a2.x;
+    int l1[3], l2[3], M[3];
+    for (int d = 0; d < 3; ++d) {
+        l1[d] = S.fn_pw[3 * fi + d];
+        l2[d] = S.fn_pw[3 * fj + d];
+        M[d] = l1[d] + l2[d];
+    }
+    const double *r1 = S.sh_r + 3 * S1, *r2 = S.sh_r + 3 * S2;
+    const int n1 = S.sh_np[S1], n2 = S.sh_np[S2];
+    double V = 0.0;
+    for (int pi = 0; pi < n1; ++pi)
+        for (int pj = 0; pj < n2; ++pj) {
+            const double al = S.sh_exp[S.sh_eoff[S1] + pi], be = S.sh_exp[S.sh_eoff[S2] + pj];
+            const double es = al + be, mu = al * be / es;
+            double pref = S.sh_coef[S.sh_coff[S1] + a1.y * n1 + pi] * S.sh_coef[S.sh_coff[S2] + a2.y * n2 + pj] * 2.0 /
+                          sqrt(PI_D);
+            double cen[3];
+            int Np[3] = {0, 0, 0};
+            for (int d = 0; d < 3; ++d) {
+                if (d < S.ndp) {
+                    const double a = S.a[d];
+                    double pe;
+                    tce_bary(al, be, r1[d], r2[d], S.L[d], a, pe, cen[d]);
+                    const double Aa = 2.0 * pe / (a * a);
+                    pref *= exp(-2.0 * (es - pe) / (a * a)) * S.L[d] / pow(a, (double)M[d]);
+                    const int est = tce_nmax_estimate(Aa);
+                    Np[d] = est < S.ncap ? est : S.ncap;
+                    const int N = Np[d] + M[d];
+                    if (lane == 0) {   // e^{-A} I_n(A), n = 0..N, Miller from N
+                        if (Aa < 1e-10) {
+                            for (int k = 0; k <= N; ++k) Iv[k] = 0.0;
+                            Iv[0] = 1.0;
+                        } else if (N < 2) {
+                            for (int k = 0; k <= N; ++k) Iv[k] = 0.0;
+                            Iv[0] = tce_iv0_scaled(Aa);
+                        } else {
+                            const double inv_A2 = 2.0 / Aa;
+                            Iv[N] = 1e-280;
+                            Iv[N - 1] = Iv[N] * (double)N * inv_A2;
+                            for (int k = N - 1; k >= 1; --k) {
+                                Iv[k - 1] = Iv[k + 1] + (double)k * inv_A2 * Iv[k];
+                                if (Iv[k - 1] > 1e250)
+                                    for (int m = k - 1; m <= N; ++m) Iv[m] *= 1e-250;
+                            }
+                            const double s = tce_iv0_scaled(Aa) / Iv[0];
+                            for (int k = 0; k <= N; ++k) Iv[k] *= s;
+                        }
+                    }
+                    __syncwarp();
+                    double dre[4 * TCE_LMAX + 1], dim[4 * TCE_LMAX + 1];
+                    if (M[d] > 0) tce_fourier_sin(l1[d], l2[d], a * (cen[d] - r1[d]), a * (cen[d] - r2[d]), dre, dim);
+                    for (int n = lane; n <= Np[d]; n += 32) {
+                        double gr = 0.0, gi = 0.0;
+                        if (M[d] == 0) {
+                            gr = Iv[n];
+                        } else {
+                            for (int kk = -M[d]; kk <= M[d]; ++kk) {
+                                const int idx = n + kk;
+                                const double b = Iv[idx < 0 ? -idx : idx];
+                                gr += dre[kk + M[d]] * b;
+                                gi += dim[kk + M[d]] * b;
+                            }
+                        }
+                        Gre[d * NW + n] = gr;
+                        Gim[d * NW + n] = gi;
+                    }
+                    __syncwarp();
+                } else {
+                    cen[d] = (al * r1[d] + be * r2[d]) / es;
+                    pref *= exp(-mu * (r1[d] - r2[d]) * (r1[d] - r2[d]));
+                }
+            }
+            for (int at = 0; at < A.natoms; ++at) {
+                double Cc[3];
+                for (int d = 0; d < 3; ++d) Cc[d] = A.geo[at + (size_t)A.natoms * d];
+                for (int d = 0; d < S.ndp; ++d) {
+                    const double phi = S.a[d] * (cen[d] - Cc[d]);
+                    double sn, cn, s32, c32;
+                    sincos((double)lane * phi, &sn, &cn);
+                    sincos(32.0 * phi, &s32, &c32);
+                    for (int n = lane; n <= Np[d]; n += 32) {
+                        F[d * NW + n] = Gre[d * NW + n] * cn - Gim[d * NW + n] * sn;
+                        const double t = cn * c32 - sn * s32;
+                        sn = sn * c32 + cn * s32;
+                        cn = t;
+                    }
+                }
+                __syncwarp();
+                double res = 0.0;
+                for (int k = lane; k < S.nq; k += 32) {
+                    const double t2 = S.tnode[k] * S.tnode[k];
+                    double prod = 1.0;
+                    for (int d = 0; d < 3; ++d) {
+                        if (d < S.ndp) {
+                            const double *Tk = S.Tt + (size_t)d * NW * S.nq + k;
+                            const double *Fd = F + d * NW;
+                            double dot = 0.0;
+                            for (int n = 0; n <= Np[d]; ++n) dot = fma(Fd[n], Tk[(size_t)n * S.nq], dot);
+                            prod *= dot;
+                        } else {
+                            const double ppt = es + t2, eta = t2 / ppt, pc = cen[d] - Cc[d];
+                            const double ed = exp(-es * eta * pc * pc);
+                            prod *= ed * na_overlap_1d(l1[d], l2[d], ppt, (cen[d] - r1[d]) - eta * pc,
+                                                        (cen[d] - r2[d]) - eta * pc);
+                        }
+                    }
+                    res = fma(S.tweight[k], prod, res);
+                }
+                res = tce_warp_sum(res);
+                V -= (double)A.Z[at] * pref * res;
+                __syncwarp();
+            }
+        }
+    if (lane == 0) A.V[fi + (size_t)S.nfuc * fj] = fabs(V) < 1e-14 ? 0.0 : V;
+}
+
+}  // namespace
+
+using namespace tcehost;
+
+extern "C" int tce_nuclear_attraction(void *handle, int32_t natoms, const double *geo, const int32_t *Z, double *V)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !geo || !Z || !V || natoms < 1) return fail(h, TCE_ERR_ARG, "bad argument");
+    const int nbas = h->nbas, nfuc = h->nfuc;
+    // per function: its shell and its component within the shell
+    std::vector<int2> fsh((size_t)nbas, make_int2(-1, 0));
+    for (int s = 0; s < (int)h->sh_first.size(); ++s)
+        for (int c = 0; c < h->sh_n[s]; ++c) fsh[(size_t)h->sh_first[s] + c] = make_int2(s, c);
+    for (int f = 0; f < nbas; ++f)
+        if (fsh[(size_t)f].x < 0) return fail(h, TCE_ERR_STATE, "function without a shell");
+    std::vector<double> g((size_t)natoms * 3);
+    for (int i = 0; i < natoms * 3; ++i) g[(size_t)i] = geo[i];
+    std::vector<int> z(Z, Z + natoms);
+    int2 *d_fsh = nullptr;
+    double *d_geo = nullptr, *d_V = nullptr;
+    int *d_Z = nullptr;
+    int s;
+    auto cleanup = [&]() {
+        dfree(h, d_fsh);
+        dfree(h, d_geo);
+        dfree(h, d_Z);
+        dfree(h, d_V);
+    };
+    if ((s = upload(h, &d_fsh, fsh)) || (s = upload(h, &d_geo, g)) || (s = upload(h, &d_Z, z)) ||
+        (s = dalloc(h, &d_V, (size_t)nfuc * nbas))) {
+        cleanup();
+        return s;
+    }
+    NaArgs A;
+    A.fsh = d_fsh;
+    A.natoms = natoms;
+    A.geo = d_geo;
+    A.Z = d_Z;
+    A.V = d_V;
+    const int NW = h->ncap + 1;
+    A.wdoubles = (NW + NA_MEXTRA + 9 * NW + 31) / 32 * 32;
+    const size_t wbytes = (size_t)A.wdoubles * sizeof(double);
+    int warps = NA_WARPS_MAX;
+    while (warps > 1 && wbytes * warps > 200 * 1024) --warps;
+    if (wbytes > 200 * 1024) {
+        cleanup();
+        return fail(h, TCE_ERR_UNSUPPORTED, "truncation order too large for the nuclear-attraction kernel");
+    }
+    const long long npairs = (long long)nfuc * nbas;
+    const size_t smem = wbytes * (size_t)warps;
+    cudaFuncSetAttribute(k_nuclear, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_nuclear<<<(unsigned)((npairs + warps - 1) / warps), 32 * warps, smem, h->st>>>(h->S, A);
+    cudaError_t e = cudaGetLastError();
+    std::vector<double> rows((size_t)nfuc * nbas);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(rows.data(), d_V, sizeof(double) * rows.size(), cudaMemcpyDeviceToHost, h->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+    cleanup();
+    if (e != cudaSuccess) return fail(h, TCE_ERR_CUDA, std::string("nuclear attraction: ") + cudaGetErrorString(e));
+    // rows of the unit cell, the rest by translation (fill_with_symmetry)
+    const int nx = h->ncl[0], ny = h->ncl[1], nz = h->ncl[2];
+    for (int i = 0; i < nbas; ++i) {
+        const int Ri = i / nfuc, a = i % nfuc;
+        const int Rxi = Ri % nx, Ryi = (Ri / nx) % ny, Rzi = Ri / (nx * ny);
+        for (int j = 0; j < nbas; ++j) {
+            const int Rj = j / nfuc, b = j % nfuc;
+            const int Rxj = Rj % nx, Ryj = (Rj / nx) % ny, Rzj = Rj / (nx * ny);
+            const int dx = ((Rxj - Rxi) % nx + nx) % nx, dy = ((Ryj - Ryi) % ny + ny) % ny;
+            const int dz = ((Rzj - Rzi) % nz + nz) % nz;
+            const int src = (dz * ny + dy) * nx + dx;
+            V[i + (size_t)nbas * j] = rows[a + (size_t)nfuc * (b + (size_t)src * nfuc)];
+        }
+    }
+    return TCE_OK;
+}

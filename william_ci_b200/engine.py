@@ -43,7 +43,7 @@ EXPORTS = ["tce_create", "tce_destroy", "tce_last_error", "tce_get_info", "tce_s
            "tce_mlp_get_params", "tce_mlp_set_params", "tce_mlp_loss_grad", "tce_mlp_train", "tce_mlp_predict",
            "tce_lg_predict_rules", "tce_lg_work", "tce_quad_self_check", "tce_set_graph",
            "tce_set_fp32_threshold", "tce_dfmp2_energy", "tce_mp2_last_error", "tce_create_blocks",
-           "tce_pass_kernels", "tce_set_tensor_cores"]
+           "tce_pass_kernels", "tce_set_tensor_cores", "tce_nuclear_attraction"]
 
 TCE_METHOD_FIXED, TCE_METHOD_LEARNED, TCE_METHOD_PLAIN = 0, 1, 2
 TCE_NFEAT = 12
@@ -131,6 +131,7 @@ def lib():
         L.tce_set_graph.argtypes = [C.c_void_p, C.c_int32]
         L.tce_pass_kernels.argtypes = [C.c_void_p, _ip]
         L.tce_set_tensor_cores.argtypes = [C.c_void_p, C.c_int32]
+        L.tce_nuclear_attraction.argtypes = [C.c_void_p, C.c_int32, _dp, _ip, _dp]
         L.tce_set_fp32_threshold.argtypes = [C.c_void_p, C.c_double]
         L.tce_dfmp2_energy.argtypes = [C.c_int32, _ip, _ip, C.c_int32, C.c_int32, C.c_int32, _dp, _dp, _ip, _dp,
                                        _ip, C.c_int32, _dp, _dp, _lp, _dp, _dp]
@@ -355,6 +356,16 @@ class Engine:
         n = C.c_int32()
         _check(lib().tce_pass_kernels(self.h, C.byref(n)), self.h)
         return n.value
+
+    def nuclear_attraction(self, geometry=None, charges=None) -> np.ndarray:
+        """Nuclear attraction matrix (nbas x nbas) on the device (tce_nuclear_attraction);
+        the system's own atoms by default."""
+        geo = np.asfortranarray(self.sys.geometry if geometry is None else geometry, dtype=np.float64)
+        Z = np.ascontiguousarray(self.sys.charges if charges is None else charges, dtype=np.int32)
+        V = np.zeros(self.nbas * self.nbas)
+        g = geo.ravel(order="F").copy()
+        _check(lib().tce_nuclear_attraction(self.h, int(len(Z)), _d(g), _i(Z), _d(V)), self.h)
+        return V.reshape(self.nbas, self.nbas, order="F")
 
     def set_tensor_cores(self, on: bool = True):
         """FP64 tensor-core node sums where a kernel has them (tce_set_tensor_cores)."""
