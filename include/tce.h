@@ -125,6 +125,17 @@ int tce_shell_block_noalloc(void *handle, const int32_t sh4[4], int32_t mode, do
  * fast rule when dmax <= 1e-10, the caller does the same with its handles. */
 int tce_quad_self_check(void *fast, void *full, double *dmax, int32_t *nsample);
 
+/* The whole gate of fast_quad_self_check (fast_quad_self_check.f90:30-233):
+ * the ERI sample of tce_quad_self_check (dmax, nq elements) and then, with
+ * the same generator continuing, the nuclear-attraction sample of :135-172:
+ * V(i,i) for the first function of every unit-cell shell, 20 random pairs in
+ * the unit cell, 20 with j anywhere (nv elements), each computed with both
+ * handles; dV is the largest difference.  The reference keeps the fast rule
+ * when dmax <= 1e-10 and dV <= 1e-10.  geometry and Z as
+ * tce_nuclear_attraction. */
+int tce_quad_self_check_nuc(void *fast, void *full, int32_t natoms, const double *geometry, const int32_t *Z,
+                            double *dmax, double *dV, int32_t *nq, int32_t *nv);
+
 /* Shell list: first function and component count of each shell. */
 int tce_shells(void *handle, int32_t *first, int32_t *n);
 

@@ -117,6 +117,49 @@ def _lcg_sample(nshuc, nsh, nrand=50):
     return out
 
 
+def _lcg_v_sample(nshuc_first, nfuc, nbas, nrand=50, nv_rand=20):
+    """The nuclear-attraction sample of fast_quad_self_check.f90:135-151 (0-based):
+    the generator continues after the quartet sample's 4 nrand draws."""
+    seed = 12345
+    for _ in range(4 * nrand):
+        seed = (seed * 1103515245 + 12345) % 2147483648
+    out = [(f, f) for f in nshuc_first] or [(0, 0)]
+    for r in range(2 * nv_rand):
+        seed = (seed * 1103515245 + 12345) % 2147483648
+        i = (seed // 16) % nfuc
+        seed = (seed * 1103515245 + 12345) % 2147483648
+        j = (seed // 16) % (nfuc if r < nv_rand else nbas)
+        out.append((i, j))
+    return out
+
+
+@pytest.mark.parametrize("name,ncell", [("h_chain64", (8, 1, 1)), ("li_cube", (2, 2, 2))])
+def test_fast_quad_self_check_nuclear_vs_oracle(systems, name, ncell):
+    """Both halves of the gate: the ERI sample as in the test below, and the
+    nuclear-attraction sample against the oracle's V with both rules."""
+    import json
+    import os
+    import pyoracle
+    from william_ci_b200.engine import Engine, fast_quad_self_check, fast_quad_self_check_nuc
+    tab = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "quad_tables.json")))["128"]
+    sysm = systems(name, ncell)
+    fast = Engine(sysm)
+    full = Engine(sysm, t_nodes=tab["t_val"], t_weights=tab["w_val"])
+    d, dv, nq, nv, keep = fast_quad_self_check_nuc(fast, full)
+    d0, nq0, _ = fast_quad_self_check(fast, full)
+    assert d == d0 and nq == nq0
+    o32 = pyoracle.Oracle(sysm)
+    o128 = pyoracle.Oracle(sysm, t_nodes=tab["t_val"], t_weights=tab["w_val"])
+    sh, _, _ = o32.shells()
+    first = [f for f, _ in sh if f < sysm.nfuc]
+    sample = _lcg_v_sample(first, sysm.nfuc, sysm.nbas)
+    assert nv == len(sample)
+    V32, V128 = o32.one_electron()[2], o128.one_electron()[2]
+    dvref = max(abs(V32[i, j] - V128[i, j]) for i, j in sample)
+    assert abs(dv - dvref) <= 1e-12, (dv, dvref)
+    assert keep == (d <= 1e-10 and dvref <= 1e-10)
+
+
 @pytest.mark.parametrize("name,ncell", [("h_chain64", (8, 1, 1)), ("li_cube", (2, 2, 2))])
 def test_fast_quad_self_check_vs_oracle(systems, name, ncell):
     import json

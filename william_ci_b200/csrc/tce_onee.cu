@@ -21,6 +21,8 @@
 // rotation by e^{32 i phi} per step of the lane's n) and finally the node
 // sums over k (lanes over nodes, F broadcast from shared memory, T rows
 // coalesced), reduced over the warp.
+#include <algorithm>
+#include <cmath>
 #include <vector>
 
 #include "tce_handle.h"
@@ -53,10 +55,12 @@ __device__ double na_overlap_1d(int j, int m, double p, double pa, double pb)
 
 struct NaArgs {
     const int2 *fsh;     // per function: shell, component
+    const int2 *plist;   // (i, j) of each element, or null: every i < nfuc, j < nbas
+    long long npairs;
     int natoms;
     const double *geo;   // [natoms + natoms * d] (Fortran geometry(natoms, 3))
     const int *Z;
-    double *V;           // rows of the unit cell: V[i + nfuc * j]
+    double *V;           // rows of the unit cell V[i + nfuc * j], or V[p] for a pair list
     int wdoubles;        // shared doubles per warp
 };
 
@@ -65,8 +69,9 @@ __global__ void __launch_bounds__(NA_WARPS_MAX * 32) k_nuclear(DevSys S, NaArgs 
     extern __shared__ double smem[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const long long pair = (long long)blockIdx.x * (blockDim.x >> 5) + wib;
-    if (pair >= (long long)S.nfuc * S.nbas) return;
-    const int fi = (int)(pair % S.nfuc), fj = (int)(pair / S.nfuc);
+    if (pair >= A.npairs) return;
+    const int fi = A.plist ? A.plist[pair].x : (int)(pair % S.nfuc);
+    const int fj = A.plist ? A.plist[pair].y : (int)(pair / S.nfuc);
     const int NW = S.ncap + 1;
     double *Iv = smem + (size_t)wib * A.wdoubles;            // NW + NA_MEXTRA
     double *Gre = Iv + NW + NA_MEXTRA;                        // [ndp][NW] each
@@ -186,44 +191,49 @@ __global__ void __launch_bounds__(NA_WARPS_MAX * 32) k_nuclear(DevSys S, NaArgs 
                 __syncwarp();
             }
         }
-    if (lane == 0) A.V[fi + (size_t)S.nfuc * fj] = fabs(V) < 1e-14 ? 0.0 : V;
+    if (lane == 0) A.V[A.plist ? pair : fi + (long long)S.nfuc * fj] = fabs(V) < 1e-14 ? 0.0 : V;
 }
 
 }  // namespace
 
 using namespace tcehost;
 
-extern "C" int tce_nuclear_attraction(void *handle, int32_t natoms, const double *geo, const int32_t *Z, double *V)
+// Elements of the nuclear attraction matrix on the device: every i < nfuc,
+// j < nbas (plist empty; out[i + nfuc j]) or the listed (i, j) (out[p]).
+static int nuclear_elements(Handle *h, int natoms, const double *geo, const int32_t *Z, const std::vector<int2> &plist,
+                            std::vector<double> &out)
 {
-    Handle *h = static_cast<Handle *>(handle);
-    if (!h || !geo || !Z || !V || natoms < 1) return fail(h, TCE_ERR_ARG, "bad argument");
     const int nbas = h->nbas, nfuc = h->nfuc;
-    // per function: its shell and its component within the shell
     std::vector<int2> fsh((size_t)nbas, make_int2(-1, 0));
     for (int s = 0; s < (int)h->sh_first.size(); ++s)
         for (int c = 0; c < h->sh_n[s]; ++c) fsh[(size_t)h->sh_first[s] + c] = make_int2(s, c);
     for (int f = 0; f < nbas; ++f)
         if (fsh[(size_t)f].x < 0) return fail(h, TCE_ERR_STATE, "function without a shell");
-    std::vector<double> g((size_t)natoms * 3);
-    for (int i = 0; i < natoms * 3; ++i) g[(size_t)i] = geo[i];
+    for (const int2 &p : plist)
+        if (p.x < 0 || p.x >= nfuc || p.y < 0 || p.y >= nbas) return fail(h, TCE_ERR_ARG, "element outside the unit-cell rows");
+    const long long npairs = plist.empty() ? (long long)nfuc * nbas : (long long)plist.size();
+    std::vector<double> g(geo, geo + (size_t)natoms * 3);
     std::vector<int> z(Z, Z + natoms);
-    int2 *d_fsh = nullptr;
+    int2 *d_fsh = nullptr, *d_pl = nullptr;
     double *d_geo = nullptr, *d_V = nullptr;
     int *d_Z = nullptr;
     int s;
     auto cleanup = [&]() {
         dfree(h, d_fsh);
+        dfree(h, d_pl);
         dfree(h, d_geo);
         dfree(h, d_Z);
         dfree(h, d_V);
     };
-    if ((s = upload(h, &d_fsh, fsh)) || (s = upload(h, &d_geo, g)) || (s = upload(h, &d_Z, z)) ||
-        (s = dalloc(h, &d_V, (size_t)nfuc * nbas))) {
+    if ((s = upload(h, &d_fsh, fsh)) || (!plist.empty() && (s = upload(h, &d_pl, plist))) ||
+        (s = upload(h, &d_geo, g)) || (s = upload(h, &d_Z, z)) || (s = dalloc(h, &d_V, (size_t)npairs))) {
         cleanup();
         return s;
     }
     NaArgs A;
     A.fsh = d_fsh;
+    A.plist = plist.empty() ? nullptr : d_pl;
+    A.npairs = npairs;
     A.natoms = natoms;
     A.geo = d_geo;
     A.Z = d_Z;
@@ -237,16 +247,26 @@ extern "C" int tce_nuclear_attraction(void *handle, int32_t natoms, const double
         cleanup();
         return fail(h, TCE_ERR_UNSUPPORTED, "truncation order too large for the nuclear-attraction kernel");
     }
-    const long long npairs = (long long)nfuc * nbas;
     const size_t smem = wbytes * (size_t)warps;
     cudaFuncSetAttribute(k_nuclear, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_nuclear<<<(unsigned)((npairs + warps - 1) / warps), 32 * warps, smem, h->st>>>(h->S, A);
     cudaError_t e = cudaGetLastError();
-    std::vector<double> rows((size_t)nfuc * nbas);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(rows.data(), d_V, sizeof(double) * rows.size(), cudaMemcpyDeviceToHost, h->st);
+    out.assign((size_t)npairs, 0.0);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out.data(), d_V, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, h->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
     cleanup();
     if (e != cudaSuccess) return fail(h, TCE_ERR_CUDA, std::string("nuclear attraction: ") + cudaGetErrorString(e));
+    return TCE_OK;
+}
+
+extern "C" int tce_nuclear_attraction(void *handle, int32_t natoms, const double *geo, const int32_t *Z, double *V)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !geo || !Z || !V || natoms < 1) return fail(h, TCE_ERR_ARG, "bad argument");
+    const int nbas = h->nbas, nfuc = h->nfuc;
+    std::vector<double> rows;
+    int s = nuclear_elements(h, natoms, geo, Z, {}, rows);
+    if (s) return s;
     // rows of the unit cell, the rest by translation (fill_with_symmetry)
     const int nx = h->ncl[0], ny = h->ncl[1], nz = h->ncl[2];
     for (int i = 0; i < nbas; ++i) {
@@ -261,5 +281,45 @@ extern "C" int tce_nuclear_attraction(void *handle, int32_t natoms, const double
             V[i + (size_t)nbas * j] = rows[a + (size_t)nfuc * (b + (size_t)src * nfuc)];
         }
     }
+    return TCE_OK;
+}
+
+// The nuclear-attraction half of fast_quad_self_check (fast_quad_self_check.f90
+// :135-172, 189): after the ERI sample (tce_quad_self_check, whose 50 random
+// quartets take 200 draws of the generator next() :228-231, seed 12345), the
+// diagonal V(i,i) of the first function of every unit-cell shell, 20 random
+// pairs inside the unit cell and 20 with j anywhere, each with both handles'
+// rules; the fast rule stays when both largest differences are <= 1e-10.
+extern "C" int tce_quad_self_check_nuc(void *fast, void *full, int32_t natoms, const double *geo, const int32_t *Z,
+                                       double *dmax, double *dV, int32_t *nq, int32_t *nv)
+{
+    Handle *hf = static_cast<Handle *>(fast), *hg = static_cast<Handle *>(full);
+    if (!hf || !hg || !geo || !Z || !dmax || !dV || !nq || !nv || natoms < 1) return fail(hf, TCE_ERR_ARG, "bad argument");
+    if (hf->nbas != hg->nbas || hf->nfuc != hg->nfuc) return fail(hf, TCE_ERR_ARG, "handles of different systems");
+    int s = tce_quad_self_check(fast, full, dmax, nq);
+    if (s) return s;
+    const int nfuc = hf->nfuc, nbas = hf->nbas;
+    long long seed = 12345;
+    auto next = [&]() {
+        seed = (seed * 1103515245LL + 12345LL) % 2147483648LL;
+        return seed / 16;
+    };
+    for (int k = 0; k < 4 * 50; ++k) next();   // the ERI sample's draws
+    std::vector<int2> pl;
+    for (size_t sh = 0; sh < hf->sh_first.size(); ++sh)
+        if (hf->sh_first[sh] < nfuc) pl.push_back(make_int2(hf->sh_first[sh], hf->sh_first[sh]));
+    if (pl.empty()) pl.push_back(make_int2(0, 0));
+    for (int r = 0; r < 40; ++r) {
+        const int i = (int)(next() % nfuc);
+        const int j = (int)(next() % (r < 20 ? nfuc : nbas));
+        pl.push_back(make_int2(i, j));
+    }
+    std::vector<double> v1, v2;
+    if ((s = nuclear_elements(hf, natoms, geo, Z, pl, v1))) return s;
+    if ((s = nuclear_elements(hg, natoms, geo, Z, pl, v2))) return fail(hf, s, hg->err);
+    double m = 0.0;
+    for (size_t p = 0; p < pl.size(); ++p) m = std::max(m, std::fabs(v1[p] - v2[p]));
+    *dV = m;
+    *nv = (int32_t)pl.size();
     return TCE_OK;
 }

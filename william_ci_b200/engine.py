@@ -43,7 +43,7 @@ EXPORTS = ["tce_create", "tce_destroy", "tce_last_error", "tce_get_info", "tce_s
            "tce_mlp_get_params", "tce_mlp_set_params", "tce_mlp_loss_grad", "tce_mlp_train", "tce_mlp_predict",
            "tce_lg_predict_rules", "tce_lg_work", "tce_quad_self_check", "tce_set_graph",
            "tce_set_fp32_threshold", "tce_dfmp2_energy", "tce_mp2_last_error", "tce_create_blocks",
-           "tce_pass_kernels", "tce_set_tensor_cores", "tce_nuclear_attraction"]
+           "tce_pass_kernels", "tce_set_tensor_cores", "tce_nuclear_attraction", "tce_quad_self_check_nuc"]
 
 TCE_METHOD_FIXED, TCE_METHOD_LEARNED, TCE_METHOD_PLAIN = 0, 1, 2
 TCE_NFEAT = 12
@@ -132,6 +132,7 @@ def lib():
         L.tce_pass_kernels.argtypes = [C.c_void_p, _ip]
         L.tce_set_tensor_cores.argtypes = [C.c_void_p, C.c_int32]
         L.tce_nuclear_attraction.argtypes = [C.c_void_p, C.c_int32, _dp, _ip, _dp]
+        L.tce_quad_self_check_nuc.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, _dp, _ip, _dp, _dp, _ip, _ip]
         L.tce_set_fp32_threshold.argtypes = [C.c_void_p, C.c_double]
         L.tce_dfmp2_energy.argtypes = [C.c_int32, _ip, _ip, C.c_int32, C.c_int32, C.c_int32, _dp, _dp, _ip, _dp,
                                        _ip, C.c_int32, _dp, _dp, _lp, _dp, _dp]
@@ -414,6 +415,19 @@ def fast_quad_self_check(fast: Engine, full: Engine, tol: float = 1e-10):
     n = C.c_int32()
     _check(lib().tce_quad_self_check(fast.h, full.h, C.byref(d), C.byref(n)), fast.h)
     return d.value, n.value, d.value <= tol
+
+
+def fast_quad_self_check_nuc(fast: Engine, full: Engine, tol: float = 1e-10):
+    """The whole fast_quad_self_check (fast_quad_self_check.f90:30-233): ERI and
+    nuclear-attraction samples on the fast-rule and full-table engines; returns
+    (dmax, dV, n_eri, n_v, keep) with keep = dmax <= tol and dV <= tol."""
+    geo = np.asfortranarray(fast.sys.geometry, dtype=np.float64).ravel(order="F").copy()
+    Z = np.ascontiguousarray(fast.sys.charges, dtype=np.int32)
+    d, dv = C.c_double(), C.c_double()
+    nq, nv = C.c_int32(), C.c_int32()
+    _check(lib().tce_quad_self_check_nuc(fast.h, full.h, int(len(Z)), _d(geo), _i(Z), C.byref(d), C.byref(dv),
+                                         C.byref(nq), C.byref(nv)), fast.h)
+    return d.value, dv.value, nq.value, nv.value, (d.value <= tol and dv.value <= tol)
 
 
 def dfmp2_energy(ncl, L, eps_o, occ_o, eps_v, occ_v, mode: int = 1):
