@@ -97,11 +97,30 @@ def cpu_baseline(sysm, stride, reps=1):
                       % (stride, len(items), nf, best)}
 
 
-def scf_iterations(eng, sysm, n_iter=5):
-    """RHF SCF iteration time (RHF_SAO mirror: host linear algebra + device direct J/K)."""
+def nuclear_attraction_stage(eng, sysm):
+    """Nuclear attraction matrix on the device (tce_nuclear_attraction, every atom
+    of the 64-cell chain): wall time of the call (host output), and its unit-cell
+    rows against the oracle's committed rows."""
+    z = np.load(ONEE_FIXTURE)
+    eng.nuclear_attraction()
+    t0 = time.perf_counter()
+    V = eng.nuclear_attraction()
+    t = time.perf_counter() - t0
+    d = float(np.abs(V[:sysm.nfuc] - z["V"]).max())
+    return V, {"ms": 1e3 * t, "elements": int(sysm.nfuc * sysm.nbas), "atoms": int(len(sysm.charges)),
+               "max_abs_diff_vs_oracle_rows": d,
+               "api": "tce_nuclear_attraction (rows of the unit cell on the device, the rest by translation, "
+                      "host output)"}
+
+
+def scf_iterations(eng, sysm, n_iter=5, V=None):
+    """RHF SCF iteration time (RHF_SAO mirror: host linear algebra + device direct J/K);
+    V from the device when given."""
     from william_ci_b200 import scf
     z = np.load(ONEE_FIXTURE)
     S_, T_, V_ = (scf.fill_with_symmetry(z[k], sysm.nfuc, sysm.ncell) for k in ("S", "T", "V"))
+    if V is not None:
+        V_ = V
     r = scf.rhf_sao(S_, T_, V_, float(z["enuc"]), scf.n_occupied(sysm), sysm.nfuc, sysm.ncell, eng.direct_JK,
                     max_scf=n_iter)
     it = r.iter_seconds[1:] if len(r.iter_seconds) > 1 else r.iter_seconds
@@ -354,9 +373,9 @@ def main():
 
     def run(method, steps, warmup):
         eng.set_method(method)
-        for _ in range(warmup):
+        for _ in range(warmup):      # synchronised: one-time list changes (rejects moved) finish here
             step()
-        torch.cuda.synchronize()
+            torch.cuda.synchronize()
         tot, kern = timed_passes(eng, step, steps, flush, stream, world, dist)
         t = torch.tensor([tot, kern], dtype=torch.float64, device=dev)
         if world > 1:
@@ -372,14 +391,22 @@ def main():
     fp32 = {"threshold": FP32_THRESHOLD, "quartets": eng.lg_stats()["fp32"],
             "max_abs_jk_diff_vs_fp64": float(max(np.abs(J32 - J64).max(), np.abs(K32 - K64).max())),
             "density_abs_sum": float(np.abs(Ph).sum())}
+    # kernel form (CUDA cores or FP64 tensor cores) per work list, chosen by timing both
+    tune = eng.lg_autotune(3) if world == 1 else None
+    if tune is not None:
+        names = {0: "generic", 1: "all-s", 2: "one-p"}
+        tune["lists"] = ["%s cls%d nq%d%s: %s, %d quartets" % (names[w["kind"]], w["cls"], w["nq"],
+                                                                " fp32" if w["fp32"] else "",
+                                                                "tensor cores" if w["tc"] else "CUDA cores", w["n"])
+                         for w in eng.lg_lists()]
     # every pass is one CUDA-graph launch from here on
     eng.set_graph(True)
     # the headline: learned-grid J/K passes, clocks sampled during them
     clocks = ClockSampler(local)
     eng.set_method(TCE_METHOD_LEARNED)
-    for _ in range(args.warmup):
+    for _ in range(args.warmup):     # synchronised: one-time list changes (rejects moved) finish here
         step()
-    torch.cuda.synchronize()
+        torch.cuda.synchronize()
     clocks.start()
     tot_ms, lg_kern = timed_passes(eng, step, args.steps, flush, stream, world, dist)
     clk = clocks.stop()
@@ -471,11 +498,13 @@ def main():
             "learned_grid_fp64_only": {"value": nq_total / (lg64_ms * 1e-3), "ms_per_step": lg64_ms},
             "fp32_panels": fp32,
             "cuda_graph": "each J/K pass replayed as one CUDA graph (tce_set_graph)",
+            "autotune": tune,
             "learned_grid": dict(lg_info, judge_rejected_last_pass=st["rejected"],
                                  plain_list_last_pass=st["plain_direct"]),
             "e2e": e2e, "roofline": roofline, "clocks": clk, "gpu_launches": args.steps * launches_per_step}
     if world == 1:
-        line["rhf_scf"] = scf_iterations(eng, sysm)
+        Vdev, line["nuclear_attraction"] = nuclear_attraction_stage(eng, sysm)
+        line["rhf_scf"] = scf_iterations(eng, sysm, V=Vdev)
         line["dfmp2"] = dfmp2_timing()
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(sysm, stride=1)

@@ -189,6 +189,24 @@ int tce_set_graph(void *handle, int32_t on);
  * arithmetic type, different summation order.  No reference counterpart. */
 int tce_set_tensor_cores(void *handle, int32_t on);
 
+/* Kernel-form tuning of the learned-grid pass (after tce_lg_predict_rules /
+ * tce_lg_set_item_rules): every work list that has both a CUDA-core and an
+ * FP64 tensor-core kernel is timed with each (reps launches each, CUDA
+ * events; the fastest launch counts) and keeps the faster, also when the
+ * lists are rebuilt later (new rules, rejects moved to the plain list).
+ * ntuned: lists timed; nswitched: lists whose choice differs from the built-in
+ * default; ms_saved: estimated time per pass saved against the default.  Uses
+ * the handle's host-entry J/K buffers as scratch; results of later passes are
+ * the same up to the summation order.  No reference counterpart. */
+int tce_lg_autotune(void *handle, int32_t reps, int32_t *ntuned, int32_t *nswitched, double *ms_saved);
+
+/* The learned-grid work lists of the handle: *n lists; with info (6 int32
+ * per list, *n on entry = its capacity in lists): kind (0 generic, 1 all-s,
+ * 2 one-p), class bits, padded rule nodes (32/64), FP32 panels, kernel form in
+ * use (0 CUDA cores, 1 FP64 tensor cores), quartets.  No reference
+ * counterpart. */
+int tce_lg_lists(void *handle, int32_t *n, int32_t *info);
+
 /* Nuclear attraction matrix of the handle's system (replaces
  * nuclear_attraction_matrix_toroidal_{1,2,3}D, 1D_Nuclear_attraction_toroidal.f90
  * :169-276 / 3D_Nuclear_attraction_toroidal.f90:113-196, with the per-pair

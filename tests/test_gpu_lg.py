@@ -324,3 +324,25 @@ def test_tensor_core_node_sums_match_cuda_cores(chain16_lg):
             assert np.abs(a - b).max() <= 1e-12 * scale, np.abs(a - b).max() / scale
     finally:
         eng.set_tensor_cores(True)
+
+
+def test_autotune_keeps_the_results(chain16_lg):
+    """tce_lg_autotune times the CUDA-core and tensor-core form of every list
+    that has both and keeps the faster: J/K unchanged up to the summation order,
+    and the choice survives the rebuild that moves the judge's rejects."""
+    from william_ci_b200.engine import TCE_METHOD_LEARNED
+    sysm, eng, net = chain16_lg
+    P = random_density(sysm.nbas, 8) * 0.05
+    scale = np.abs(P).sum()
+    eng.set_method(TCE_METHOD_LEARNED)
+    eng.set_fp32_threshold(0.0)
+    eng.set_graph(False)
+    eng.lg_predict_rules(net)
+    J0, K0 = eng.direct_JK(P)
+    info = eng.lg_autotune(reps=1)
+    assert info["lists_tuned"] >= 1
+    for graph in (False, True):          # the second call also rebuilds the lists (rejects moved)
+        eng.set_graph(graph)
+        J1, K1 = eng.direct_JK(P)
+        assert np.abs(J1 - J0).max() <= 1e-12 * scale and np.abs(K1 - K0).max() <= 1e-12 * scale
+    eng.set_graph(False)

@@ -625,7 +625,7 @@ static int jk_body(Handle *h, const double *dP, double *dJ, double *dK, cudaStre
             a.max_ncq = h->max_ncq;
             a.fixed_gmax = h->d_gmax;
             a.num_sms = h->num_sms;
-            a.use_tc = h->use_tc;
+            a.use_tc = h->use_tc && h->nq == 64;   // tensor-core rows measured faster with 64 nodes only
             CKS(h, tce_launch_quartets(h->S, a, st));
         } else {             // register-resident kernels of the dominant classes
             SArgsHost b;

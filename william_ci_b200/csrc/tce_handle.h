@@ -2,6 +2,7 @@
 // host translation units share (error reporting, device allocation).
 #pragma once
 #include <algorithm>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -78,8 +79,12 @@ struct Handle {
     // learned-grid work, one list per kernel and rule size: kind 0 generic
     // (k_quartets), 1 all-s (k_quartets_s), 2 one-periodic-direction s/p class
     // `cls` (k_quartets_r1); nq = 32 or 64 padded rule nodes
-    struct LgList { int kind, cls, nq, fp32; int4 *d = nullptr; int *rule = nullptr; long long n = 0; };
+    // tc: kernel form chosen by tce_lg_autotune (-1: the default rule of
+    // lg_tc_default, 0: CUDA cores, 1: FP64 tensor cores); tc_choice keeps the
+    // choices per list key across rebuilds
+    struct LgList { int kind, cls, nq, fp32, tc = -1; int4 *d = nullptr; int *rule = nullptr; long long n = 0; };
     std::vector<LgList> lg_lists;
+    std::map<int, int> tc_choice;
     long long n_lg = 0, n_fp32 = 0;
     double fp32_thr = 0.0;               // FP32 node sums below this Schwarz product (0: off)
     float *d_rule_T32 = nullptr;         // FP32 copy of the rule T tables

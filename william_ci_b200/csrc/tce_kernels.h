@@ -35,7 +35,7 @@ struct QuartetHostArgs {
     int max_ncomb = 1;   // largest (lA+1)(lB+1)(lC+1)(lD+1) among the items
     int max_ncq = 1296;  // largest block (components) among the items
     int num_sms = 148;
-    int use_tc = 0;      // rows of one periodic direction on the FP64 tensor cores (64-node rules)
+    int use_tc = 0;      // rows of one periodic direction on the FP64 tensor cores (32/64-node rules)
     const int *fixed_gmax = nullptr;   // [3*TCE_MAXG] of the system's rule
     // learned grid
     const RuleDev *rules = nullptr;

@@ -396,7 +396,7 @@ static void fill_common(Handle *h, QuartetHostArgs &a)
     a.max_ncq = h->max_ncq;
     a.fixed_gmax = h->d_gmax;
     a.num_sms = h->num_sms;
-    a.use_tc = h->use_tc;
+    a.use_tc = 0;   // set per launch
     a.rules = h->d_rules;
     a.rule_T = h->d_rule_T;
     a.rule_t = h->d_rule_t;
@@ -487,6 +487,10 @@ int lg_rebuild_lists(Handle *h)
         w.cls = (key / 4) % 16;
         w.nq = ((key / 2) & 1) ? 64 : 32;
         w.fp32 = key & 1;
+        {
+            auto tcit = h->tc_choice.find(key);
+            if (tcit != h->tc_choice.end()) w.tc = tcit->second;
+        }
         w.n = (long long)lg[key].size();
         if ((s = upload(h, &w.d, lg[key]))) return s;
         if ((s = upload(h, &w.rule, rl[key]))) return s;
@@ -500,6 +504,73 @@ int lg_rebuild_lists(Handle *h)
     h->n_plain_direct = (long long)pl.size();
     CK(h, cudaStreamSynchronize(h->st));
     return TCE_OK;
+}
+
+// Whether a learned-grid list has a tensor-core form (one periodic direction:
+// generic rows, all-s and one-p kernels) and which form it runs by default:
+// the all-s kernel on the tensor cores for FP64 quartets, the one-p kernel for
+// FP64 quartets with 32-node rules, the generic rows with 64-node rules (the
+// forms measured faster on the 64-cell chain); FP32-panel lists keep their
+// CUDA-core kernels unless tuned otherwise.
+static bool lg_tc_available(const Handle *h, const Handle::LgList &w)
+{
+    return h->ndp == 1 && (w.nq == 32 || w.nq == 64);
+}
+
+static int lg_tc_default(const Handle *h, const Handle::LgList &w)
+{
+    if (!lg_tc_available(h, w) || w.fp32) return 0;
+    if (w.kind == 0) return w.nq == 64 ? 1 : 0;
+    if (w.kind == 1) return 1;
+    return w.nq == 32 ? 1 : 0;
+}
+
+static int lg_tc(const Handle *h, const Handle::LgList &w)
+{
+    if (!h->use_tc || !lg_tc_available(h, w)) return 0;
+    return w.tc >= 0 ? w.tc : lg_tc_default(h, w);
+}
+
+// one learned-grid list with kernel form tc (0 CUDA cores, 1 FP64 tensor cores)
+static int lg_launch_list(Handle *h, const Handle::LgList &w, const QuartetHostArgs &a, const double *dP, double *dJ,
+                          double *dK, int tc, cudaStream_t st)
+{
+    if (w.kind == 0) {
+        QuartetHostArgs b = a;
+        b.method = TCE_METHOD_LEARNED;
+        b.dict_nq = w.nq;
+        b.items = w.d;
+        b.nitems = (int)w.n;
+        b.item_rule = w.rule;
+        b.fb_items = h->d_fb_items;
+        b.fb_count = h->d_fb_count;
+        b.next = h->d_next;
+        b.use_tc = tc;
+        return tce_launch_quartets(h->S, b, st);
+    }
+    SArgsHost b;
+    b.items = w.d;
+    b.nitems = (int)w.n;
+    b.prim_screen = h->prim_screen;
+    b.next = h->d_next;
+    b.P = dP;
+    b.J = dJ;
+    b.K = dK;
+    b.num_sms = h->num_sms;
+    b.item_rule = w.rule;
+    b.rules = h->d_rules;
+    b.rule_T = h->d_rule_T;
+    b.rule_t = h->d_rule_t;
+    b.rule_wk = h->d_rule_wk;
+    b.rule_wg = h->d_rule_wg;
+    b.rule_T32 = h->d_rule_T32;
+    b.judge_tol = h->judge_tol;
+    b.fb_items = h->d_fb_items;
+    b.fb_count = h->d_fb_count;
+    if (w.kind == 1)
+        return tc ? tce_launch_quartets_s_tc(h->S, b, w.nq, st) : tce_launch_quartets_s_lg(h->S, b, w.nq, w.fp32 != 0, st);
+    return tc ? tce_launch_quartets_r1_tc(h->S, w.cls, b, w.nq, st)
+              : tce_launch_quartets_r1_lg(h->S, w.cls, b, w.nq, w.fp32 != 0, st);
 }
 
 // After a learned-grid pass (on the pass's stream): the reject count and the
@@ -604,46 +675,7 @@ int lg_jk_passes(Handle *h, const double *dP, double *dJ, double *dK, cudaStream
         CKS(h, tce_launch_quartets(h->S, b, h->st2));
         CK(h, cudaEventRecord(h->ev_join, h->st2));
     }
-    for (const auto &w : h->lg_lists) {
-        if (w.kind == 0) {
-            QuartetHostArgs b = a;
-            b.method = TCE_METHOD_LEARNED;
-            b.dict_nq = w.nq;
-            b.items = w.d;
-            b.nitems = (int)w.n;
-            b.item_rule = w.rule;
-            b.fb_items = h->d_fb_items;
-            b.fb_count = h->d_fb_count;
-            b.next = h->d_next;
-            CKS(h, tce_launch_quartets(h->S, b, st));
-        } else {
-            SArgsHost b;
-            b.items = w.d;
-            b.nitems = (int)w.n;
-            b.prim_screen = h->prim_screen;
-            b.next = h->d_next;
-            b.P = dP;
-            b.J = dJ;
-            b.K = dK;
-            b.num_sms = h->num_sms;
-            b.item_rule = w.rule;
-            b.rules = h->d_rules;
-            b.rule_T = h->d_rule_T;
-            b.rule_t = h->d_rule_t;
-            b.rule_wk = h->d_rule_wk;
-            b.rule_wg = h->d_rule_wg;
-            b.rule_T32 = h->d_rule_T32;
-            b.judge_tol = h->judge_tol;
-            b.fb_items = h->d_fb_items;
-            b.fb_count = h->d_fb_count;
-            if (w.kind == 1 && h->use_tc && h->ndp == 1 && !w.fp32) CKS(h, tce_launch_quartets_s_tc(h->S, b, w.nq, st));
-            else if (w.kind == 1) CKS(h, tce_launch_quartets_s_lg(h->S, b, w.nq, w.fp32 != 0, st));
-            // one-p classes: the tensor-core kernel for 32-node rules (measured faster there;
-            // with 64-node rules the CUDA-core kernel is faster)
-            else if (h->use_tc && !w.fp32 && w.nq == 32) CKS(h, tce_launch_quartets_r1_tc(h->S, w.cls, b, w.nq, st));
-            else CKS(h, tce_launch_quartets_r1_lg(h->S, w.cls, b, w.nq, w.fp32 != 0, st));
-        }
-    }
+    for (const auto &w : h->lg_lists) CKS(h, lg_launch_list(h, w, a, dP, dJ, dK, lg_tc(h, w), st));
     // join before the judge's fallback: both plain launches use the same per-warp scratch
     if (side) CK(h, cudaStreamWaitEvent(st, h->ev_join, 0));
     if (h->n_lg > 0) {   // the judge's rejects, count read on the device
@@ -934,6 +966,7 @@ int tce_rule_blocks(void *handle, int32_t rule, int32_t mode, int64_t n, const i
         a.dict_nq = h->rules_host[rule].nq;
     }
     if (rule == -2) a.method = TCE_METHOD_PLAIN;
+    a.use_tc = h->use_tc && ((rule >= 0 && a.dict_nq == 64) || (rule == -1 && h->nq == 64));
     CKS(h, tce_launch_quartets(h->S, a, h->st));
     CK(h, cudaMemcpyAsync(K, d_K, sizeof(double) * off.back(), cudaMemcpyDeviceToHost, h->st));
     if (d_G) CK(h, cudaMemcpyAsync(G, d_G, sizeof(double) * off.back(), cudaMemcpyDeviceToHost, h->st));
@@ -1239,6 +1272,100 @@ int tce_lg_work(void *handle, double *flops, int64_t *nprim)
     *nprim = (int64_t)np_;
     dfree(h, d_np);
     dfree(h, d_fl);
+    return TCE_OK;
+}
+
+// The learned-grid work lists: per list kind, class, padded rule nodes, FP32
+// panels, kernel form in use (0 CUDA cores, 1 tensor cores), quartets.
+int tce_lg_lists(void *handle, int32_t *n, int32_t *info)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !n) return fail(h, TCE_ERR_ARG, "NULL argument");
+    if (info) {
+        if (*n < (int32_t)h->lg_lists.size()) return fail(h, TCE_ERR_ARG, "info holds fewer lists than the handle has");
+        for (size_t i = 0; i < h->lg_lists.size(); ++i) {
+            const auto &w = h->lg_lists[i];
+            int32_t *o = info + 6 * i;
+            o[0] = w.kind;
+            o[1] = w.cls;
+            o[2] = w.nq;
+            o[3] = w.fp32;
+            o[4] = lg_tc(h, w);
+            o[5] = (int32_t)w.n;
+        }
+    }
+    *n = (int32_t)h->lg_lists.size();
+    return TCE_OK;
+}
+
+// Kernel-form tuning of the learned-grid pass: every list that has a
+// tensor-core form runs `reps` times with each form on the handle's stream
+// (CUDA events around each launch, the fastest launch of each form counts) and
+// keeps the faster form, also for later rebuilds of the lists.  The pass's
+// J/K buffers of the host entry points serve as scratch.
+int tce_lg_autotune(void *handle, int32_t reps, int32_t *ntuned, int32_t *nswitched, double *ms_saved)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !ntuned || !nswitched || !ms_saved) return fail(h, TCE_ERR_ARG, "NULL argument");
+    if (!h->d_rules || h->lg_lists.empty()) return fail(h, TCE_ERR_STATE, "no learned-grid lists");
+    if (!h->d_P || !h->d_J || !h->d_K) return fail(h, TCE_ERR_STATE, "handle without J/K buffers");
+    if (reps < 1) reps = 1;
+    int s;
+    if ((s = ensure_plain(h))) return s;
+    QuartetHostArgs a;
+    fill_common(h, a);
+    a.mode = TCE_MODE_JK;
+    a.prim_screen = h->prim_screen;
+    a.P = h->d_P;
+    a.J = h->d_J;
+    a.K = h->d_K;
+    CK(h, cudaMemsetAsync(h->d_P, 0, sizeof(double) * (size_t)h->nbas * h->nbas, h->st));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(h, cudaEventCreate(&e0));
+    CK(h, cudaEventCreate(&e1));
+    int nt = 0, nsw = 0;
+    double saved = 0.0;
+    s = TCE_OK;
+    for (auto &w : h->lg_lists) {
+        if (!lg_tc_available(h, w)) continue;
+        double best[2] = {1e300, 1e300};
+        for (int tc = 0; tc < 2 && s == TCE_OK; ++tc)
+            for (int r = 0; r < reps && s == TCE_OK; ++r) {
+                cudaMemsetAsync(h->d_fb_count, 0, sizeof(unsigned int), h->st);
+                cudaEventRecord(e0, h->st);
+                s = lg_launch_list(h, w, a, h->d_P, h->d_J, h->d_K, tc, h->st);
+                cudaEventRecord(e1, h->st);
+                if (s == TCE_OK && cudaEventSynchronize(e1) != cudaSuccess) s = TCE_ERR_CUDA;
+                float ms = 0.f;
+                if (s == TCE_OK) cudaEventElapsedTime(&ms, e0, e1);
+                best[tc] = std::min(best[tc], (double)ms);
+            }
+        if (s != TCE_OK) break;
+        // the other form only when it is clearly faster: isolated launches differ a
+        // little from launches inside the pass, so near-ties keep the default
+        const int dflt = lg_tc_default(h, w);
+        const double alt_t = best[1 - dflt], def_t = best[dflt];
+        const int choice = (alt_t < 0.97 * def_t && def_t - alt_t > 0.02) ? 1 - dflt : dflt;
+        const int key = ((w.kind * 16 + w.cls) * 2 + (w.nq == 64 ? 1 : 0)) * 2 + (w.fp32 ? 1 : 0);
+        h->tc_choice[key] = choice;
+        w.tc = choice;
+        ++nt;
+        if (choice != dflt) ++nsw;
+        saved += best[dflt] - best[choice];
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (s != TCE_OK) return fail(h, s, "autotune launch failed");
+    CK(h, cudaMemsetAsync(h->d_fb_count, 0, sizeof(unsigned int), h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    // a captured pass is re-captured with the chosen forms; the items and rules
+    // are unchanged, so rejects copied back from the last pass stay valid
+    const bool keep_fb = h->fb_version == h->work_version;
+    ++h->work_version;
+    if (keep_fb) h->fb_version = h->work_version;
+    *ntuned = nt;
+    *nswitched = nsw;
+    *ms_saved = saved;
     return TCE_OK;
 }
 

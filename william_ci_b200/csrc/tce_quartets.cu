@@ -307,9 +307,8 @@ __device__ void process_batch(const DevSys &S, const RuleView &Rv, const QCtx &Q
     const int nppb = Q.Ub.npp, nppk = Q.Uk.npp;
     const int nrows = nb * R;
     bool rows_done = false;
-    // tensor-core rows for 64-node rules (measured faster there; with 32-node
-    // rules the lane-per-row loop below is faster)
-    if constexpr (RO && NQ == 64) {
+    // tensor-core rows when the launch asks for them (32- and 64-node rules)
+    if constexpr (RO && (NQ == 32 || NQ == 64)) {
         if (tc && ndp == 1) {
             tc_rows<NQ>(S, Rv, Q, nb, b, lane);
             rows_done = true;

@@ -43,7 +43,8 @@ EXPORTS = ["tce_create", "tce_destroy", "tce_last_error", "tce_get_info", "tce_s
            "tce_mlp_get_params", "tce_mlp_set_params", "tce_mlp_loss_grad", "tce_mlp_train", "tce_mlp_predict",
            "tce_lg_predict_rules", "tce_lg_work", "tce_quad_self_check", "tce_set_graph",
            "tce_set_fp32_threshold", "tce_dfmp2_energy", "tce_mp2_last_error", "tce_create_blocks",
-           "tce_pass_kernels", "tce_set_tensor_cores", "tce_nuclear_attraction", "tce_quad_self_check_nuc"]
+           "tce_pass_kernels", "tce_set_tensor_cores", "tce_nuclear_attraction", "tce_quad_self_check_nuc",
+           "tce_lg_autotune", "tce_lg_lists"]
 
 TCE_METHOD_FIXED, TCE_METHOD_LEARNED, TCE_METHOD_PLAIN = 0, 1, 2
 TCE_NFEAT = 12
@@ -132,6 +133,8 @@ def lib():
         L.tce_pass_kernels.argtypes = [C.c_void_p, _ip]
         L.tce_set_tensor_cores.argtypes = [C.c_void_p, C.c_int32]
         L.tce_nuclear_attraction.argtypes = [C.c_void_p, C.c_int32, _dp, _ip, _dp]
+        L.tce_lg_autotune.argtypes = [C.c_void_p, C.c_int32, _ip, _ip, _dp]
+        L.tce_lg_lists.argtypes = [C.c_void_p, _ip, _ip]
         L.tce_quad_self_check_nuc.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, _dp, _ip, _dp, _dp, _ip, _ip]
         L.tce_set_fp32_threshold.argtypes = [C.c_void_p, C.c_double]
         L.tce_dfmp2_energy.argtypes = [C.c_int32, _ip, _ip, C.c_int32, C.c_int32, C.c_int32, _dp, _dp, _ip, _dp,
@@ -367,6 +370,23 @@ class Engine:
         g = geo.ravel(order="F").copy()
         _check(lib().tce_nuclear_attraction(self.h, int(len(Z)), _d(g), _i(Z), _d(V)), self.h)
         return V.reshape(self.nbas, self.nbas, order="F")
+
+    def lg_autotune(self, reps: int = 2) -> dict:
+        """Time each learned-grid list with its CUDA-core and tensor-core kernels
+        and keep the faster (tce_lg_autotune)."""
+        nt, ns = C.c_int32(), C.c_int32()
+        saved = C.c_double()
+        _check(lib().tce_lg_autotune(self.h, int(reps), C.byref(nt), C.byref(ns), C.byref(saved)), self.h)
+        return {"lists_tuned": nt.value, "lists_switched": ns.value, "ms_saved_per_pass": saved.value}
+
+    def lg_lists(self) -> list:
+        """The learned-grid work lists: dicts of kind, cls, nq, fp32, tc (kernel form in use), n."""
+        n = C.c_int32(0)
+        _check(lib().tce_lg_lists(self.h, C.byref(n), None), self.h)
+        info = np.zeros(6 * max(n.value, 1), dtype=np.int32)
+        _check(lib().tce_lg_lists(self.h, C.byref(n), _i(info)), self.h)
+        keys = ("kind", "cls", "nq", "fp32", "tc", "n")
+        return [dict(zip(keys, (int(x) for x in info[6 * i:6 * i + 6]))) for i in range(n.value)]
 
     def set_tensor_cores(self, on: bool = True):
         """FP64 tensor-core node sums where a kernel has them (tce_set_tensor_cores)."""
