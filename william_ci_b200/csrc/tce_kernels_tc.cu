@@ -74,11 +74,14 @@ __device__ __forceinline__ int tce_pool_add(const DevSys &S, const SArgs &A, con
 // the batch's 8 MT x 32 nodes of one pass (MT tiles x 4 node tiles x 2 per lane)
 constexpr int TCE_TC_MT = 2;
 constexpr int TCE_TC_BATCH = 8 * TCE_TC_MT;
+// node tiles of 8 per pass of the all-s kernel (4: 32 nodes per pass)
+constexpr int TCE_TC_NT = 4;
 
 template <int NQ>
 __global__ void __launch_bounds__(256, 2) k_quartets_s_tc(DevSys S, SArgs A)
 {
     constexpr int MT = TCE_TC_MT, BT = TCE_TC_BATCH;
+    constexpr int NT = (NQ / 8) < TCE_TC_NT ? (NQ / 8) : TCE_TC_NT;   // node tiles per pass
     extern __shared__ double smem[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int rq = lane >> 2, cq = lane & 3;   // fragment row in an 8-row tile, fragment column
@@ -140,17 +143,17 @@ __global__ void __launch_bounds__(256, 2) k_quartets_s_tc(DevSys S, SArgs A)
                     return S.a[0] * (S.pp[Ub.pp_off + pq.x].cen[0] - (S.pp[Uk.pp_off + pq.y].cen[0] + Tsh[0]));
                 };
 #pragma unroll 1
-                for (int g0 = 0; g0 < NQ / 8; g0 += 4) {
-                    int gmb[4], nend = -1;
+                for (int g0 = 0; g0 < NQ / 8; g0 += NT) {
+                    int gmb[NT], nend = -1;
 #pragma unroll
-                    for (int t = 0; t < 4; ++t) {
+                    for (int t = 0; t < NT; ++t) {
                         gmb[t] = gm[g0 + t];
                         nend = gmb[t] > nend ? gmb[t] : nend;
                     }
                     nend = nend < nmax ? nend : nmax;
-                    double acc[8 * MT];
+                    double acc[2 * MT * NT];
 #pragma unroll
-                    for (int x = 0; x < 8 * MT; ++x) acc[x] = 0.0;
+                    for (int x = 0; x < 2 * MT * NT; ++x) acc[x] = 0.0;
                     double cc[MT], cp[MT], c4[MT];   // cos(n phi), cos((n - 4) phi), 2 cos(4 phi)
                     double gN[MT], hN[MT];           // G_n, H_n of the next step (prefetched)
 #pragma unroll
@@ -163,13 +166,13 @@ __global__ void __launch_bounds__(256, 2) k_quartets_s_tc(DevSys S, SArgs A)
                         gN[m] = ok ? __ldg(Gbase + goff[m] + 2 * (size_t)cq * nppb) : 0.0;
                         hN[m] = ok ? __ldg(Hbase + hoff[m] + 2 * (size_t)cq * nppk) : 0.0;
                     }
-                    double tN[4];                    // T fragments of the next step
+                    double tN[NT];                    // T fragments of the next step
 #pragma unroll
-                    for (int t = 0; t < 4; ++t)
+                    for (int t = 0; t < NT; ++t)
                         tN[t] = (0 <= gmb[t] && cq <= S.ncap) ? __ldg(Tg + (size_t)cq * NQ + 8 * (g0 + t) + rq) : 0.0;
                     for (int s4 = 0; s4 <= nend; s4 += 4) {
                         const int n = s4 + cq, n1 = n + 4;
-                        double F[MT], Tb[4];
+                        double F[MT], Tb[NT];
 #pragma unroll
                         for (int m = 0; m < MT; ++m) {
                             F[m] = gN[m] * hN[m] * cc[m];
@@ -178,7 +181,7 @@ __global__ void __launch_bounds__(256, 2) k_quartets_s_tc(DevSys S, SArgs A)
                             hN[m] = ok ? __ldg(Hbase + hoff[m] + 2 * (size_t)n1 * nppk) : 0.0;
                         }
 #pragma unroll
-                        for (int t = 0; t < 4; ++t) {
+                        for (int t = 0; t < NT; ++t) {
                             Tb[t] = tN[t];
                             tN[t] = (s4 + 4 <= gmb[t] && n1 <= S.ncap)
                                         ? __ldg(Tg + (size_t)n1 * NQ + 8 * (g0 + t) + rq) : 0.0;
@@ -199,13 +202,13 @@ __global__ void __launch_bounds__(256, 2) k_quartets_s_tc(DevSys S, SArgs A)
                             }
                         }
 #pragma unroll
-                        for (int t = 0; t < 4; ++t)
+                        for (int t = 0; t < NT; ++t)
                             if (s4 <= gmb[t]) {
 #pragma unroll
-                                for (int m = 0; m < MT; ++m) tce_dmma(acc[8 * m + 2 * t], acc[8 * m + 2 * t + 1], F[m], Tb[t]);
+                                for (int m = 0; m < MT; ++m) tce_dmma(acc[(m * NT + t) * 2], acc[(m * NT + t) * 2 + 1], F[m], Tb[t]);
                             }
                     }
-                    // epilogue: acc[8 m + 2 t + i] = I[8 m + rq][8 (g0 + t) + 2 cq + i]
+                    // epilogue: acc[2 (m NT + t) + i] = I[8 m + rq][8 (g0 + t) + 2 cq + i]
 #pragma unroll
                     for (int m = 0; m < MT; ++m) {
                         const int r = 8 * m + rq;
@@ -222,7 +225,7 @@ __global__ void __launch_bounds__(256, 2) k_quartets_s_tc(DevSys S, SArgs A)
                         }
                         double vK = 0.0, vG = 0.0;
 #pragma unroll
-                        for (int t = 0; t < 4; ++t) {
+                        for (int t = 0; t < NT; ++t) {
                             if (gmb[t] < 0) continue;   // padding nodes
 #pragma unroll
                             for (int i = 0; i < 2; ++i) {
@@ -230,7 +233,7 @@ __global__ void __launch_bounds__(256, 2) k_quartets_s_tc(DevSys S, SArgs A)
                                 const double t2 = tn[k] * tn[k];
                                 const double D2 = 1.0 / (pq_ + ps * t2);
                                 const double e = (R2 == 0.0) ? 1.0 : exp(-(pq_ * t2 * D2) * R2);
-                                const double bse = acc[8 * m + 2 * t + i] * (PI2 * D2 * e);
+                                const double bse = acc[(m * NT + t) * 2 + i] * (PI2 * D2 * e);
                                 vK = fma(bse, wk[k], vK);
                                 vG = fma(bse, wg[k], vG);
                             }
