@@ -75,8 +75,8 @@ __global__ void __launch_bounds__(NA_WARPS_MAX * 32) k_nuclear(DevSys S, NaArgs 
     const int NW = S.ncap + 1;
     double *Iv = smem + (size_t)wib * A.wdoubles;            // NW + NA_MEXTRA
     double *Gre = Iv + NW + NA_MEXTRA;                        // [ndp][NW] each
-    double *Gim = Gre + 3 * NW;
-    double *F = Gim + 3 * NW;
+    double *Gim = Gre + S.ndp * NW;
+    double *F = Gim + S.ndp * NW;
     const int2 a1 = A.fsh[fi], a2 = A.fsh[fj];
     const int S1 = a1.x, S2 = a2.x;
     int l1[3], l2[3], M[3];
@@ -174,9 +174,16 @@ __global__ void __launch_bounds__(NA_WARPS_MAX * 32) k_nuclear(DevSys S, NaArgs 
                         if (d < S.ndp) {
                             const double *Tk = S.Tt + (size_t)d * NW * S.nq + k;
                             const double *Fd = F + d * NW;
-                            double dot = 0.0;
-                            for (int n = 0; n <= Np[d]; ++n) dot = fma(Fd[n], Tk[(size_t)n * S.nq], dot);
-                            prod *= dot;
+                            double d0 = 0.0, d1 = 0.0, d2 = 0.0, d3 = 0.0;   // four chains
+                            int n = 0;
+                            for (; n + 3 <= Np[d]; n += 4) {
+                                d0 = fma(Fd[n], Tk[(size_t)n * S.nq], d0);
+                                d1 = fma(Fd[n + 1], Tk[(size_t)(n + 1) * S.nq], d1);
+                                d2 = fma(Fd[n + 2], Tk[(size_t)(n + 2) * S.nq], d2);
+                                d3 = fma(Fd[n + 3], Tk[(size_t)(n + 3) * S.nq], d3);
+                            }
+                            for (; n <= Np[d]; ++n) d0 = fma(Fd[n], Tk[(size_t)n * S.nq], d0);
+                            prod *= (d0 + d1) + (d2 + d3);
                         } else {
                             const double ppt = es + t2, eta = t2 / ppt, pc = cen[d] - Cc[d];
                             const double ed = exp(-es * eta * pc * pc);
@@ -239,7 +246,7 @@ static int nuclear_elements(Handle *h, int natoms, const double *geo, const int3
     A.Z = d_Z;
     A.V = d_V;
     const int NW = h->ncap + 1;
-    A.wdoubles = (NW + NA_MEXTRA + 9 * NW + 31) / 32 * 32;
+    A.wdoubles = (NW + NA_MEXTRA + 3 * h->ndp * NW + 31) / 32 * 32;
     const size_t wbytes = (size_t)A.wdoubles * sizeof(double);
     int warps = NA_WARPS_MAX;
     while (warps > 1 && wbytes * warps > 200 * 1024) --warps;
