@@ -217,6 +217,21 @@ int tce_lg_lists(void *handle, int32_t *n, int32_t *info);
  * y, then z); Z the nuclear charges.  Uses the handle's t-rule and tables. */
 int tce_nuclear_attraction(void *handle, int32_t natoms, const double *geometry, const int32_t *Z, double *V);
 
+/* Density-fitted J and K of the SCF (replaces df_JK, df_toroidal.f90:850-956).
+ * tce_dfjk_create keeps on the device the fitted coefficients B =
+ * df_B(nfuc, nbas, naux) (column-major, naux = nau x cells) and the k-space
+ * Bh = df_Bh(nfuc, nau, nfuc, cells, nkh) of df_init (:660-678, complex as
+ * interleaved re/im, k2 over the half set of df_khalf :103-114).  tce_dfjk
+ * takes P (nbas x nbas) and returns J and K with rows > nfuc zero, as the
+ * reference.  K is contracted with the whole P(k) (the reference drops the
+ * eigen-components of P(k) below 1e-10 in magnitude).  Own error string:
+ * tce_dfjk_last_error. */
+int tce_dfjk_create(int32_t nfuc, int32_t nbas, int32_t nau, const int32_t ncl[3], const double *B, const double *Bh,
+                    void **handle);
+int tce_dfjk(void *handle, const double *P, double *J, double *K);
+int tce_dfjk_destroy(void *handle);
+const char *tce_dfjk_last_error(void *handle);
+
 /* Multi-GPU: restrict tce_direct_jk[_device] on this handle to shard `rank`
  * of `nranks` (cost-balanced partition of the unique shell quartets, the same
  * partition on every rank).  The partial J/K of the ranks sum to the full J/K;

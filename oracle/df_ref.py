@@ -11,7 +11,8 @@ the restated quartet kernel) on the same orbital + auxiliary + dummy system:
   f(-k) = conj f(k) (:575-594, 1174-1216);
 * T3(mu0, nu, P) = (mu0 nu|P 1) (:597-626);
 * df_B = T3 f in k-space, back to real space (:628-687);
-* L(p, q, Q, k1, k2) per momentum transfer (df_L_kap :1053-1104).
+* L(p, q, Q, k1, k2) per momentum transfer (df_L_kap :1053-1104);
+* df_JK (:850-956) with the k-space Bh of :660-678.
 """
 from __future__ import annotations
 
@@ -96,7 +97,27 @@ def integrals(orc, dfs, shells, nshuc):
     return Vm, T3
 
 
-def fitted(Vm, T3, ncl, nau, tol=1e-10):
+def khalf(ncl):
+    """df_khalf :103-114: position of k in the half set {k : -k >= k} (0-based), -1 otherwise."""
+    N = int(np.prod(ncl))
+    khi = -np.ones(N, dtype=np.int64)
+    n = 0
+    for k in range(N):
+        if csub(ncl, 0, k) >= k:
+            khi[k] = n
+            n += 1
+    return khi
+
+
+def cadd(ncl, r1, r2):
+    c = coords(ncl)
+    d = [(c[r1][x] + c[r2][x]) % ncl[x] for x in range(3)]
+    return d[0] + ncl[0] * (d[1] + ncl[1] * d[2])
+
+
+def fitted(Vm, T3, ncl, nau, tol=1e-10, bh=False):
+    """df_B (and with bh=True also the k-space Bh(mu, Q, nu0; k1, k) of :660-678,
+    complex (nf, nau, nf, N, nkh))."""
     N = int(np.prod(ncl))
     ph = phase(ncl)
     f = np.zeros((nau, nau, N), dtype=np.complex128)
@@ -118,16 +139,81 @@ def fitted(Vm, T3, ncl, nau, tol=1e-10):
     Sph = ph.T.imag
     Ar = T @ Cph
     Ai = T @ Sph
+    khi = khalf(ncl)
+    Bh = np.zeros((nf, nau, nf, N, int((khi >= 0).sum())), dtype=np.complex128) if bh else None
     for k in range(N):
         Zk = (Ar[:, k] + 1j * Ai[:, k]).reshape(nf * nb, nau, order="F")
         Wk = Zk @ f[:, :, k]
         Ar[:, k] = Wk.real.ravel(order="F")
         Ai[:, k] = Wk.imag.ravel(order="F")
+        if bh and khi[k] >= 0:
+            Wt = np.zeros((nf, nau, nf, N), dtype=np.complex128)
+            for r in range(N):
+                for nu0 in range(nf):
+                    for q in range(nau):
+                        Wt[:, q, nu0, r] = Wk[r * nf * nf + nu0 * nf: r * nf * nf + (nu0 + 1) * nf, q]
+            for k1 in range(N):
+                Bh[:, :, :, k1, khi[k]] = np.einsum("aqbr,r->aqb", Wt, ph[k1])
     Bf = (Ar @ Cph.T + Ai @ Sph.T) / N        # (m1, R')
     B = np.zeros((nf, nb, nau * N))
     for r in range(N):
         B[:, :, r * nau:(r + 1) * nau] = Bf[:, r].reshape(nf, nb, nau, order="F")
-    return B
+    return (B, Bh) if bh else B
+
+
+def df_jk(B, Bh, P, ncl, nf, nau):
+    """df_JK :850-956: J from the real-space B (gamma over the cells), K from the
+    k-space Bh and the eigenvectors of P(k) with |eigenvalue| > 1e-10.  Rows
+    >= nf of J and K are zero, as the reference leaves them."""
+    N = int(np.prod(ncl))
+    nbas = nf * N
+    naux = nau * N
+    ph = phase(ncl)
+    khi = khalf(ncl)
+    Bm = B.reshape(nf * nbas, naux, order="F")
+    Ps = np.zeros((nf * nbas, N))
+    for r in range(N):
+        for rs in range(N):
+            c = cadd(ncl, rs, r)
+            Ps[rs * nf * nf:(rs + 1) * nf * nf, r] = P[r * nf:(r + 1) * nf, c * nf:(c + 1) * nf].ravel(order="F")
+    G = Bm.T @ Ps
+    gam = np.zeros(naux)
+    for r in range(N):
+        for rq in range(N):
+            c = cadd(ncl, rq, r)
+            gam[c * nau:(c + 1) * nau] += G[rq * nau:(rq + 1) * nau, r]
+    J = np.zeros((nbas, nbas))
+    J[:nf, :] = (Bm @ gam).reshape(nf, nbas, order="F")
+    ck, wk = [], []
+    for ik in range(N):
+        pk = sum(P[:nf, r * nf:(r + 1) * nf] * ph[ik, r] for r in range(N))
+        pk = 0.5 * (pk + pk.conj().T)
+        ew, ev = np.linalg.eigh(pk)
+        keep = np.abs(ew) > 1e-10
+        ck.append(ev[:, keep])
+        wk.append(ew[keep])
+    Kt = np.zeros((N, nf, nf), dtype=np.complex128)
+    for kk in range(N):
+        Kloc = np.zeros((nf, nf), dtype=np.complex128)
+        for k1 in range(N):
+            no = len(wk[k1])
+            if no == 0:
+                continue
+            k2 = csub(ncl, kk, k1)
+            if khi[k2] >= 0:
+                L = Bh[:, :, :, k1, khi[k2]].reshape(nf * nau, nf, order="F") @ ck[k1]
+            else:
+                mk1 = csub(ncl, 0, k1)
+                L = np.conj(Bh[:, :, :, mk1, khi[csub(ncl, 0, k2)]].reshape(nf * nau, nf, order="F") @ np.conj(ck[k1]))
+            L = L.reshape(nf, nau * no, order="F")
+            w = np.repeat(wk[k1], nau)                      # column (q, i) -> w_i
+            Kloc += (L * w) @ L.conj().T
+        Kt[kk] = Kloc * (-0.5 / N)
+    K = np.zeros((nbas, nbas))
+    for r in range(N):
+        pk = sum(Kt[kk] * np.conj(ph[kk, r]) for kk in range(N))
+        K[:nf, r * nf:(r + 1) * nf] = pk.real / N
+    return J, K
 
 
 def L_vectors(B, C_k, ncl, nf, nau, p_lo, p_hi, q_lo, q_hi):

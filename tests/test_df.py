@@ -84,3 +84,42 @@ def test_mp2_energy_restatement_is_consistent(dimer_df):
     e = mp2_ref.kmp2(G, ncl, r.eps_k[:, p0:p1], r.occ_k[:, p0:p1], r.eps_k[:, q0:q1], r.occ_k[:, q0:q1])
     assert e["nzero"] == 0
     assert -0.1 < e["emp2"] < 0.0                        # a small negative correlation energy per supercell
+
+
+def tinv_density(nf, ncl, seed=3):
+    """A symmetric, translation-invariant real-space density (block (r, c) = D(c - r))."""
+    N = int(np.prod(ncl))
+    rng = np.random.default_rng(seed)
+    D = rng.standard_normal((N, nf, nf)) * 0.1
+    for d in range(N):
+        md = df_ref.csub(ncl, 0, d)
+        if md >= d:
+            D[d] = 0.5 * (D[d] + D[md].T)
+            D[md] = D[d].T
+    P = np.zeros((nf * N, nf * N))
+    for r in range(N):
+        for c in range(N):
+            P[r * nf:(r + 1) * nf, c * nf:(c + 1) * nf] = D[df_ref.csub(ncl, c, r)]
+    return P
+
+
+def test_k_space_B_and_df_jk_restatement(dimer_df):
+    """The product's k-space Bh (fit_B, bh=True) against the restatement of
+    df_init :660-678; the restated df_JK against the oracle's exact J/K (the
+    fitting error of this auxiliary basis, not a parity bar)."""
+    from william_ci_b200 import df
+    from test_scf import dimer_chain
+    dfs, Vm, T3, r = dimer_df
+    ncl = dfs.sys.ncell
+    B, _, Bh = df.fit_B(Vm, T3, ncl, dfs.nau, bh=True)
+    Bref, Bhref = df_ref.fitted(Vm, T3, ncl, dfs.nau, bh=True)
+    assert Bh.shape == Bhref.shape
+    assert np.abs(Bh - Bhref).max() < 1e-9
+    nf = dfs.nfuc_ao
+    P = tinv_density(nf, ncl)
+    J, K = df_ref.df_jk(Bref, Bhref, P, ncl, nf, dfs.nau)
+    ao = dimer_chain(4)
+    Je, Ke, _ = po.Oracle(ao).direct_jk(P)
+    assert np.abs(J[nf:]).max() == 0.0 and np.abs(K[nf:]).max() == 0.0
+    assert np.abs(J[:nf] - Je[:nf]).max() < 2e-2 * np.abs(Je[:nf]).max()
+    assert np.abs(K[:nf] - Ke[:nf]).max() < 2e-2 * np.abs(Ke[:nf]).max()

@@ -198,10 +198,25 @@ class DensityFitting:
         return L_vectors(B, C_k, self.ncl, self.dfs.nfuc_ao, self.dfs.nau, p_rng, q_rng)
 
 
-def fit_B(Vm: np.ndarray, T3: np.ndarray, ncl, nau: int, mtol: float = METRIC_TOL):
+def khalf(ncl) -> np.ndarray:
+    """df_khalf (df_toroidal.f90:103-114): position of k in the half set
+    {k : -k >= k}, -1 for the others."""
+    N = int(np.prod(ncl))
+    khi = -np.ones(N, dtype=np.int64)
+    n = 0
+    for k in range(N):
+        if _csub(ncl, 0, k) >= k:
+            khi[k] = n
+            n += 1
+    return khi
+
+
+def fit_B(Vm: np.ndarray, T3: np.ndarray, ncl, nau: int, mtol: float = METRIC_TOL, bh: bool = False):
     """df_B(mu0, nu, Q R) = sum (mu0 nu|P) [f](P, Q): f per k from the pivoted
     Cholesky of V(k) (chol_f, f(-k) = conj f(k)), the product in k-space,
-    back to real space.  Returns (B, largest number of dropped pivots)."""
+    back to real space.  Returns (B, largest number of dropped pivots), and with
+    bh=True also the k-space Bh(mu, Q, nu0; k1, kh) = sum_R1 W(k)(mu, nu0 R1, Q)
+    e^{i k1 R1} of df_init (:660-678), (nf, nau, nf, N, nkh), k over the half set."""
     N = int(np.prod(ncl))
     ph = _phase(ncl)
     Vr = Vm.reshape(nau, N, nau)                               # (P, R, Q)
@@ -221,7 +236,59 @@ def fit_B(Vm: np.ndarray, T3: np.ndarray, ncl, nau: int, mtol: float = METRIC_TO
     Z = np.einsum("xrp,kr->kxp", T, ph)                        # sum_R T3(R) e^{ikR}
     W = np.einsum("kxp,kpq->kxq", Z, f)
     B = np.einsum("kxq,kr->xrq", W, ph.conj()).real / N        # 1/N Re sum_k W(k) e^{-ikR}
-    return B.reshape(nfu, nb, N * nau), ndrop
+    B = B.reshape(nfu, nb, N * nau)
+    if not bh:
+        return B, ndrop
+    khi = khalf(ncl)
+    Bh = np.zeros((nfu, nau, nfu, N, int((khi >= 0).sum())), dtype=np.complex128)
+    for k in np.nonzero(khi >= 0)[0]:
+        Wr = W[k].reshape(nfu, N, nfu, nau)                     # (mu, R1, nu0, Q): nu = R1 nf + nu0
+        Bh[:, :, :, :, khi[k]] = np.einsum("arbq,kr->aqbk", Wr, ph)
+    return B, ndrop, Bh
+
+
+class DFJK:
+    """Density-fitted J and K on the device (tce_dfjk: df_JK, df_toroidal.f90
+    :850-956), from df_B and the k-space Bh of fit_B(..., bh=True)."""
+
+    def __init__(self, B: np.ndarray, Bh: np.ndarray, ncl, nf: int, nau: int):
+        import ctypes as C
+        from .engine import TCEError, lib
+        self._lib = lib()
+        self.nbas = B.shape[1]
+        Bf = np.asfortranarray(B, dtype=np.float64).ravel(order="F").copy()
+        Bhf = np.asfortranarray(Bh, dtype=np.complex128).ravel(order="F").copy().view(np.float64)
+        n3 = np.array([int(x) for x in ncl], dtype=np.int32)
+        self.h = C.c_void_p()
+        dp = C.POINTER(C.c_double)
+        code = self._lib.tce_dfjk_create(int(nf), int(self.nbas), int(nau), n3.ctypes.data_as(C.POINTER(C.c_int32)),
+                                         Bf.ctypes.data_as(dp), Bhf.ctypes.data_as(dp), C.byref(self.h))
+        if code != 0:
+            raise TCEError(code, self._lib.tce_dfjk_last_error(None).decode())
+
+    def __call__(self, P: np.ndarray):
+        import ctypes as C
+        from .engine import TCEError
+        n = self.nbas
+        Pf = np.asfortranarray(P, dtype=np.float64).ravel(order="F").copy()
+        J = np.zeros(n * n)
+        K = np.zeros(n * n)
+        dp = C.POINTER(C.c_double)
+        code = self._lib.tce_dfjk(self.h, Pf.ctypes.data_as(dp), J.ctypes.data_as(dp), K.ctypes.data_as(dp))
+        if code != 0:
+            raise TCEError(code, self._lib.tce_dfjk_last_error(self.h).decode())
+        return J.reshape(n, n, order="F"), K.reshape(n, n, order="F")
+
+    def close(self):
+        if self.h:
+            self._lib.tce_dfjk_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def L_vectors(B: np.ndarray, C_k: np.ndarray, ncl, nf: int, nau: int, p_rng: Tuple[int, int],

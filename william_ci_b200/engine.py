@@ -44,7 +44,8 @@ EXPORTS = ["tce_create", "tce_destroy", "tce_last_error", "tce_get_info", "tce_s
            "tce_lg_predict_rules", "tce_lg_work", "tce_quad_self_check", "tce_set_graph",
            "tce_set_fp32_threshold", "tce_dfmp2_energy", "tce_mp2_last_error", "tce_create_blocks",
            "tce_pass_kernels", "tce_set_tensor_cores", "tce_nuclear_attraction", "tce_quad_self_check_nuc",
-           "tce_lg_autotune", "tce_lg_lists"]
+           "tce_lg_autotune", "tce_lg_lists", "tce_dfjk_create", "tce_dfjk", "tce_dfjk_destroy",
+           "tce_dfjk_last_error"]
 
 TCE_METHOD_FIXED, TCE_METHOD_LEARNED, TCE_METHOD_PLAIN = 0, 1, 2
 TCE_NFEAT = 12
@@ -135,6 +136,11 @@ def lib():
         L.tce_nuclear_attraction.argtypes = [C.c_void_p, C.c_int32, _dp, _ip, _dp]
         L.tce_lg_autotune.argtypes = [C.c_void_p, C.c_int32, _ip, _ip, _dp]
         L.tce_lg_lists.argtypes = [C.c_void_p, _ip, _ip]
+        L.tce_dfjk_create.argtypes = [C.c_int32, C.c_int32, C.c_int32, _ip, _dp, _dp, C.POINTER(C.c_void_p)]
+        L.tce_dfjk.argtypes = [C.c_void_p, _dp, _dp, _dp]
+        L.tce_dfjk_destroy.argtypes = [C.c_void_p]
+        L.tce_dfjk_last_error.restype = C.c_char_p
+        L.tce_dfjk_last_error.argtypes = [C.c_void_p]
         L.tce_quad_self_check_nuc.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, _dp, _ip, _dp, _dp, _ip, _ip]
         L.tce_set_fp32_threshold.argtypes = [C.c_void_p, C.c_double]
         L.tce_dfmp2_energy.argtypes = [C.c_int32, _ip, _ip, C.c_int32, C.c_int32, C.c_int32, _dp, _dp, _ip, _dp,
