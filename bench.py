@@ -152,7 +152,7 @@ def dfmp2_timing(n_scf=8):
     dfit = df.DensityFitting(df.df_system(ao, aux))
     Vm, T3 = dfit.metric(), dfit.three_index()
     t2 = time.perf_counter()
-    B = dfit.fitted(Vm, T3)
+    B, dfit.ndrop, Bh = df.fit_B(Vm, T3, dfit.ncl, dfit.dfs.nau, bh=True)
     (p0, p1), (q0, q1) = df.band_ranges(r.occ_k)
     L = dfit.L(B, r.C_k, (p0, p1), (q0, q1))
     t3 = time.perf_counter()
@@ -163,6 +163,15 @@ def dfmp2_timing(n_scf=8):
     N, nau, ov = dfit.N, dfit.dfs.nau, (p1 - p0) * (q1 - q0)
     flops = 3.0 * 8.0 * N ** 3 * ov * ov * nau          # complex MACs, three split-BF16 products
     dfit.eng.close()
+    # density-fitted J/K of the SCF (df_JK) on the device, with the last RHF density
+    jk = df.DFJK(B, Bh, dfit.ncl, dfit.dfs.nfuc_ao, nau)
+    jk(r.P)
+    tj = []
+    for _ in range(5):
+        t = time.perf_counter()
+        jk(r.P)
+        tj.append(time.perf_counter() - t)
+    jk.close()
     return {"workload": "Tori1D H chain, 128 cells, L=230.4, nbas=768, aux 4s/2p/1d per H (naux %d), no=%d nv=%d"
                         % (N * nau, p1 - p0, q1 - q0),
             "rhf_iterations": r.iterations, "rhf_s": t1 - t0, "integrals_s": t2 - t1, "host_fit_s": t3 - t2,
@@ -171,6 +180,8 @@ def dfmp2_timing(n_scf=8):
             "emp2_split_bf16": e16["emp2"], "emp2_fp64": e64["emp2"],
             "split_bf16_rel_err_vs_fp64": abs(e16["emp2"] - e64["emp2"]) / max(abs(e64["emp2"]), 1e-300),
             "zero_gap_terms": e64["nzero"],
+            "df_jk_ms": 1e3 * float(np.median(tj)),
+            "df_jk_api": "tce_dfjk (host P in, J and K out; df_B and the k-space Bh resident on the device)",
             "tensor_tflops_split_bf16": flops / (e16["ms"] * 1e-3) / 1e12,
             "note": "orbitals of %d RHF iterations of a half-filled band (zero-gap terms left out as kMP2_calc does); "
                     "times the DF-MP2 stage, not a converged MP2 energy" % n_scf}

@@ -183,6 +183,7 @@ class RHFResult:
     C_k: Optional[np.ndarray] = None          # (Nc, nfuc, nfuc) complex
     eps_k: Optional[np.ndarray] = None        # (Nc, nfuc)
     occ_k: Optional[np.ndarray] = None        # (Nc, nfuc) int
+    P: Optional[np.ndarray] = None            # the density of the last diagonalisation (nbas x nbas)
 
 
 def rhf_sao(S: np.ndarray, T: np.ndarray, V: np.ndarray, enuc: float, nO: int, nfuc: int, ncell,
@@ -274,7 +275,7 @@ def rhf_sao(S: np.ndarray, T: np.ndarray, V: np.ndarray, enuc: float, nO: int, n
         it_t.append(time.perf_counter() - t_it)
     return RHFResult(energy=ehf + enuc, e_electronic=ehf, converged=converged, stalled=stalled, iterations=nscf,
                      orbital_energies=np.sort(eps), history=hist, jk_seconds=jk_t, iter_seconds=it_t,
-                     C_k=C_k, eps_k=eps.reshape(Nc, nfuc).copy(), occ_k=occ_k)
+                     C_k=C_k, eps_k=eps.reshape(Nc, nfuc).copy(), occ_k=occ_k, P=P)
 
 
 def fill_with_symmetry(rows: np.ndarray, nfuc: int, ncell) -> np.ndarray:
