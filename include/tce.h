@@ -217,6 +217,19 @@ int tce_lg_lists(void *handle, int32_t *n, int32_t *info);
  * y, then z); Z the nuclear charges.  Uses the handle's t-rule and tables. */
 int tce_nuclear_attraction(void *handle, int32_t natoms, const double *geometry, const int32_t *Z, double *V);
 
+/* k-space MO integrals from the stored SAO integrals (replaces
+ * transform_ERI_AO_to_kMO, AO_to_MO_SAO.f90:34-393, and its integral-direct
+ * twin transform_ERI_direct_kMO, AO_to_MO_SAO_direct.f90:26-176):
+ * out(p,q,r,s,k1,k2,k3) = (p k1, q k2 | r k3, s k4), k4 = k1 - k2 + k3, complex
+ * (interleaved re/im), shape (no, nv, no, nv, cells, cells, cells)
+ * column-major, no = p_hi - p_lo + 1, nv = q_hi - q_lo + 1; band indices
+ * 1-based inclusive within 1..nfuc as the reference.  coeff is coeff_SAO
+ * (nbas x nbas complex, column-major, k blocks on the diagonal).  Needs the
+ * stored integrals of tce_eri_stored (eri_size = nfuc, chemist order) on the
+ * handle. */
+int tce_ao_to_kmo(void *handle, const double *coeff, int32_t p_lo, int32_t p_hi, int32_t q_lo, int32_t q_hi,
+                  double *out);
+
 /* Density-fitted J and K of the SCF (replaces df_JK, df_toroidal.f90:850-956).
  * tce_dfjk_create keeps on the device the fitted coefficients B =
  * df_B(nfuc, nbas, naux) (column-major, naux = nau x cells) and the k-space

@@ -45,7 +45,7 @@ EXPORTS = ["tce_create", "tce_destroy", "tce_last_error", "tce_get_info", "tce_s
            "tce_set_fp32_threshold", "tce_dfmp2_energy", "tce_mp2_last_error", "tce_create_blocks",
            "tce_pass_kernels", "tce_set_tensor_cores", "tce_nuclear_attraction", "tce_quad_self_check_nuc",
            "tce_lg_autotune", "tce_lg_lists", "tce_dfjk_create", "tce_dfjk", "tce_dfjk_destroy",
-           "tce_dfjk_last_error"]
+           "tce_dfjk_last_error", "tce_ao_to_kmo"]
 
 TCE_METHOD_FIXED, TCE_METHOD_LEARNED, TCE_METHOD_PLAIN = 0, 1, 2
 TCE_NFEAT = 12
@@ -136,6 +136,7 @@ def lib():
         L.tce_nuclear_attraction.argtypes = [C.c_void_p, C.c_int32, _dp, _ip, _dp]
         L.tce_lg_autotune.argtypes = [C.c_void_p, C.c_int32, _ip, _ip, _dp]
         L.tce_lg_lists.argtypes = [C.c_void_p, _ip, _ip]
+        L.tce_ao_to_kmo.argtypes = [C.c_void_p, _dp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _dp]
         L.tce_dfjk_create.argtypes = [C.c_int32, C.c_int32, C.c_int32, _ip, _dp, _dp, C.POINTER(C.c_void_p)]
         L.tce_dfjk.argtypes = [C.c_void_p, _dp, _dp, _dp]
         L.tce_dfjk_destroy.argtypes = [C.c_void_p]
@@ -265,6 +266,22 @@ class Engine:
         eri = np.zeros(esz * n * n * n)
         _check(lib().tce_eri_stored(self.h, esz, _d(eri)), self.h)
         return eri.reshape((esz, n, n, n), order="F")
+
+    def ao_to_kmo(self, C_k: np.ndarray, p_rng, q_rng) -> np.ndarray:
+        """(p k1, q k2 | r k3, s k4) from the stored SAO integrals (tce_ao_to_kmo);
+        C_k (cells, nfuc, nfuc) the k-block orbitals, p_rng / q_rng 0-based
+        half-open band ranges.  Run ERI_integral_toroidal first (SAO, chemist)."""
+        N, nf = C_k.shape[0], C_k.shape[1]
+        n = self.nbas
+        coeff = np.zeros((n, n), dtype=np.complex128)
+        for k in range(N):
+            coeff[k * nf:(k + 1) * nf, k * nf:(k + 1) * nf] = C_k[k]
+        cf = np.asfortranarray(coeff).ravel(order="F").copy().view(np.float64)
+        (p0, p1), (q0, q1) = p_rng, q_rng
+        no, nv = p1 - p0, q1 - q0
+        out = np.zeros(2 * no * nv * no * nv * N ** 3)
+        _check(lib().tce_ao_to_kmo(self.h, _d(cf), p0 + 1, p1, q0 + 1, q1, _d(out)), self.h)
+        return out.view(np.complex128).reshape((no, nv, no, nv, N, N, N), order="F")
 
     def direct_JK(self, P: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
         n = self.nbas
