@@ -127,7 +127,23 @@ def scf_iterations(eng, sysm, n_iter=5, V=None):
     jk = r.jk_seconds[1:] if len(r.jk_seconds) > 1 else r.jk_seconds
     return {"iter_ms": 1e3 * float(np.mean(it)), "jk_ms": 1e3 * float(np.mean(jk)), "iterations_timed": len(it),
             "energy_after": r.energy, "host": "numpy (SAO transforms, per-k eigh, DIIS)",
-            "note": "64-cell H chain, half-filled band: timing of SCF iterations, not a converged energy"}
+            "note": "64-cell H chain, half-filled band: timing of SCF iterations, not a converged energy"}, r
+
+
+def ao_to_kmo_stage(eng, r):
+    """(ov|ov) k-space MO integrals of the 64-cell chain (tce_ao_to_kmo) from the
+    stored SAO integrals, with the SCF stage's orbitals: wall times of both."""
+    from william_ci_b200 import df
+    t0 = time.perf_counter()
+    eri = eng.ERI_integral_toroidal()
+    t1 = time.perf_counter()
+    gb = eri.nbytes / 1e9
+    del eri
+    pr, qr = df.band_ranges(r.occ_k)
+    out = eng.ao_to_kmo(r.C_k, pr, qr)
+    t2 = time.perf_counter()
+    return {"stored_eri_s": t1 - t0, "stored_eri_gb": gb, "ao_to_kmo_s": t2 - t1, "shape": list(out.shape),
+            "api": "tce_eri_stored then tce_ao_to_kmo (integrals resident on the device, host output)"}
 
 
 def dfmp2_timing(n_scf=8):
@@ -515,7 +531,8 @@ def main():
             "e2e": e2e, "roofline": roofline, "clocks": clk, "gpu_launches": args.steps * launches_per_step}
     if world == 1:
         Vdev, line["nuclear_attraction"] = nuclear_attraction_stage(eng, sysm)
-        line["rhf_scf"] = scf_iterations(eng, sysm, V=Vdev)
+        line["rhf_scf"], r_scf = scf_iterations(eng, sysm, V=Vdev)
+        line["ao_to_kmo"] = ao_to_kmo_stage(eng, r_scf)
         line["dfmp2"] = dfmp2_timing()
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(sysm, stride=1)
