@@ -123,3 +123,18 @@ def test_k_space_B_and_df_jk_restatement(dimer_df):
     assert np.abs(J[nf:]).max() == 0.0 and np.abs(K[nf:]).max() == 0.0
     assert np.abs(J[:nf] - Je[:nf]).max() < 2e-2 * np.abs(Je[:nf]).max()
     assert np.abs(K[:nf] - Ke[:nf]).max() < 2e-2 * np.abs(Ke[:nf]).max()
+
+
+@pytest.mark.parametrize("ncl", [(4, 1, 1), (5, 1, 1), (2, 3, 1), (2, 2, 2)])
+def test_half_k_set_matches_the_restatement(ncl):
+    """df_khalf (:103-114): the product's table against the restatement; every
+    k is in the set or its -k is, never both unless k = -k."""
+    from william_ci_b200 import df
+    khi = df.khalf(ncl)
+    assert np.array_equal(khi, df_ref.khalf(ncl))
+    N = int(np.prod(ncl))
+    for k in range(N):
+        mk = df_ref.csub(ncl, 0, k)
+        assert (khi[k] >= 0) or (khi[mk] >= 0)
+        if mk != k:
+            assert not (khi[k] >= 0 and khi[mk] >= 0)
