@@ -214,7 +214,8 @@ int tce_lg_lists(void *handle, int32_t *n, int32_t *info);
  * of the unit cell computed on the device (|V| < 1e-14 set to zero) and the
  * other rows by translation, as the reference's fill_with_symmetry.  geometry
  * is the reference's geometry(natoms, 3), column-major (x of every atom, then
- * y, then z); Z the nuclear charges.  Uses the handle's t-rule and tables. */
+ * y, then z); Z the nuclear charges.  Uses the handle's t-rule and tables (one periodic direction: node sums on the FP64 tensor cores when
+ * tce_set_tensor_cores is on). */
 int tce_nuclear_attraction(void *handle, int32_t natoms, const double *geometry, const int32_t *Z, double *V);
 
 /* k-space MO integrals from the stored SAO integrals (replaces

@@ -201,6 +201,191 @@ __global__ void __launch_bounds__(NA_WARPS_MAX * 32) k_nuclear(DevSys S, NaArgs 
     if (lane == 0) A.V[A.plist ? pair : fi + (long long)S.nfuc * fj] = fabs(V) < 1e-14 ? 0.0 : V;
 }
 
+__device__ __forceinline__ void na_dmma(double &d0, double &d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// One periodic direction, 32- or 64-node rule: per primitive pair the node
+// sums of every atom, X(atom, k) = sum_n F_n(atom) T[n][k], are an
+// (atoms x orders) x (orders x nodes) product done as FP64 mma.sync.m8n8k4
+// tiles: 16 atoms x 32 nodes per pass, lane l owns atom rows 8 m + l/4 and
+// order 4 s + l%4, cos / sin(n phi_atom) by the three-term recurrence in
+// steps of four (re-seeded every 32 orders), B fragments T[4 s + l%4][8 g + l/4].
+// The epilogue multiplies each (atom, node) by its real-direction factors,
+// weight and charge.  G vectors, prefactor and the rest as k_nuclear.
+template <int NQ>
+__global__ void __launch_bounds__(NA_WARPS_MAX * 32, 1) k_nuclear_tc(DevSys S, NaArgs A)
+{
+    extern __shared__ double smem[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int rq = lane >> 2, cq = lane & 3;
+    const long long pair = (long long)blockIdx.x * (blockDim.x >> 5) + wib;
+    if (pair >= A.npairs) return;
+    const int fi = A.plist ? A.plist[pair].x : (int)(pair % S.nfuc);
+    const int fj = A.plist ? A.plist[pair].y : (int)(pair / S.nfuc);
+    const int NW = S.ncap + 1;
+    double *Iv = smem + (size_t)wib * A.wdoubles;
+    double *Gre = Iv + NW + NA_MEXTRA;
+    double *Gim = Gre + NW;
+    const int2 a1 = A.fsh[fi], a2 = A.fsh[fj];
+    const int S1 = a1.x, S2 = a2.x;
+    int l1[3], l2[3], M[3];
+    for (int d = 0; d < 3; ++d) {
+        l1[d] = S.fn_pw[3 * fi + d];
+        l2[d] = S.fn_pw[3 * fj + d];
+        M[d] = l1[d] + l2[d];
+    }
+    const double *r1 = S.sh_r + 3 * S1, *r2 = S.sh_r + 3 * S2;
+    const int n1 = S.sh_np[S1], n2 = S.sh_np[S2];
+    const double a = S.a[0];
+    double V = 0.0;
+    for (int pi = 0; pi < n1; ++pi)
+        for (int pj = 0; pj < n2; ++pj) {
+            const double al = S.sh_exp[S.sh_eoff[S1] + pi], be = S.sh_exp[S.sh_eoff[S2] + pj];
+            const double es = al + be, mu = al * be / es;
+            double pref = S.sh_coef[S.sh_coff[S1] + a1.y * n1 + pi] * S.sh_coef[S.sh_coff[S2] + a2.y * n2 + pj] * 2.0 /
+                          sqrt(PI_D);
+            double cen[3], pe;
+            tce_bary(al, be, r1[0], r2[0], S.L[0], a, pe, cen[0]);
+            const double Aa = 2.0 * pe / (a * a);
+            pref *= exp(-2.0 * (es - pe) / (a * a)) * S.L[0] / pow(a, (double)M[0]);
+            const int est = tce_nmax_estimate(Aa);
+            const int Np = est < S.ncap ? est : S.ncap;
+            const int N = Np + M[0];
+            for (int d = 1; d < 3; ++d) {
+                cen[d] = (al * r1[d] + be * r2[d]) / es;
+                pref *= exp(-mu * (r1[d] - r2[d]) * (r1[d] - r2[d]));
+            }
+            if (lane == 0) {   // e^{-A} I_n(A), n = 0..N
+                if (Aa < 1e-10) {
+                    for (int k = 0; k <= N; ++k) Iv[k] = 0.0;
+                    Iv[0] = 1.0;
+                } else if (N < 2) {
+                    for (int k = 0; k <= N; ++k) Iv[k] = 0.0;
+                    Iv[0] = tce_iv0_scaled(Aa);
+                } else {
+                    const double inv_A2 = 2.0 / Aa;
+                    Iv[N] = 1e-280;
+                    Iv[N - 1] = Iv[N] * (double)N * inv_A2;
+                    for (int k = N - 1; k >= 1; --k) {
+                        Iv[k - 1] = Iv[k + 1] + (double)k * inv_A2 * Iv[k];
+                        if (Iv[k - 1] > 1e250)
+                            for (int m = k - 1; m <= N; ++m) Iv[m] *= 1e-250;
+                    }
+                    const double sc = tce_iv0_scaled(Aa) / Iv[0];
+                    for (int k = 0; k <= N; ++k) Iv[k] *= sc;
+                }
+            }
+            __syncwarp();
+            double dre[4 * TCE_LMAX + 1], dim[4 * TCE_LMAX + 1];
+            if (M[0] > 0) tce_fourier_sin(l1[0], l2[0], a * (cen[0] - r1[0]), a * (cen[0] - r2[0]), dre, dim);
+            for (int n = lane; n <= Np; n += 32) {
+                double gr = 0.0, gi = 0.0;
+                if (M[0] == 0) {
+                    gr = Iv[n];
+                } else {
+                    for (int kk = -M[0]; kk <= M[0]; ++kk) {
+                        const int idx = n + kk;
+                        const double bv = Iv[idx < 0 ? -idx : idx];
+                        gr += dre[kk + M[0]] * bv;
+                        gi += dim[kk + M[0]] * bv;
+                    }
+                }
+                Gre[n] = gr;
+                Gim[n] = gi;
+            }
+            __syncwarp();
+            double vsum = 0.0;
+            for (int at0 = 0; at0 < A.natoms; at0 += 16) {
+                double phr[2];
+                bool valid[2];
+#pragma unroll
+                for (int m = 0; m < 2; ++m) {
+                    const int at = at0 + 8 * m + rq;
+                    valid[m] = at < A.natoms;
+                    phr[m] = valid[m] ? a * (cen[0] - A.geo[at]) : 0.0;
+                }
+#pragma unroll 1
+                for (int g0 = 0; g0 < NQ / 8; g0 += 4) {
+                    double acc[16];
+#pragma unroll
+                    for (int x = 0; x < 16; ++x) acc[x] = 0.0;
+                    double cc[2], cp[2], sc[2], sp[2], c4[2];
+#pragma unroll
+                    for (int m = 0; m < 2; ++m) {
+                        sincos((double)cq * phr[m], &sc[m], &cc[m]);
+                        sincos((double)(cq - 4) * phr[m], &sp[m], &cp[m]);
+                        c4[m] = 2.0 * cos(4.0 * phr[m]);
+                    }
+                    for (int s4 = 0; s4 <= Np; s4 += 4) {
+                        const int n = s4 + cq, n1 = n + 4;
+                        const bool inr = n <= Np;
+                        const double gr = inr ? Gre[n] : 0.0, gi = inr ? Gim[n] : 0.0;
+                        double F[2];
+#pragma unroll
+                        for (int m = 0; m < 2; ++m) F[m] = valid[m] ? gr * cc[m] - gi * sc[m] : 0.0;
+                        double Tb[4];
+#pragma unroll
+                        for (int t = 0; t < 4; ++t)
+                            Tb[t] = (n <= S.ncap) ? __ldg(S.Tt + (size_t)n * S.nq + 8 * (g0 + t) + rq) : 0.0;
+                        if (((s4 + 4) & 31) == 0) {
+#pragma unroll
+                            for (int m = 0; m < 2; ++m) {
+                                sincos((double)n * phr[m], &sp[m], &cp[m]);
+                                sincos((double)n1 * phr[m], &sc[m], &cc[m]);
+                            }
+                        } else {
+#pragma unroll
+                            for (int m = 0; m < 2; ++m) {
+                                const double tc_ = c4[m] * cc[m] - cp[m], ts_ = c4[m] * sc[m] - sp[m];
+                                cp[m] = cc[m];
+                                cc[m] = tc_;
+                                sp[m] = sc[m];
+                                sc[m] = ts_;
+                            }
+                        }
+#pragma unroll
+                        for (int t = 0; t < 4; ++t)
+#pragma unroll
+                            for (int m = 0; m < 2; ++m) na_dmma(acc[(m * 4 + t) * 2], acc[(m * 4 + t) * 2 + 1], F[m], Tb[t]);
+                    }
+                    // epilogue: acc[(m 4 + t) 2 + i] = X(atom 8 m + rq, node 8 (g0 + t) + 2 cq + i)
+#pragma unroll
+                    for (int m = 0; m < 2; ++m) {
+                        if (!valid[m]) continue;
+                        const int at = at0 + 8 * m + rq;
+                        double Cc[3];
+                        for (int d = 1; d < 3; ++d) Cc[d] = A.geo[at + (size_t)A.natoms * d];
+                        double part = 0.0;
+#pragma unroll
+                        for (int t = 0; t < 4; ++t)
+#pragma unroll
+                            for (int i = 0; i < 2; ++i) {
+                                const int k = 8 * (g0 + t) + 2 * cq + i;
+                                const double t2 = S.tnode[k] * S.tnode[k];
+                                double prod = acc[(m * 4 + t) * 2 + i];
+                                for (int d = 1; d < 3; ++d) {
+                                    const double ppt = es + t2, eta = t2 / ppt, pc = cen[d] - Cc[d];
+                                    const double ed = exp(-es * eta * pc * pc);
+                                    prod *= ed * na_overlap_1d(l1[d], l2[d], ppt, (cen[d] - r1[d]) - eta * pc,
+                                                                (cen[d] - r2[d]) - eta * pc);
+                                }
+                                part = fma(S.tweight[k], prod, part);
+                            }
+                        vsum = fma((double)A.Z[at], part, vsum);
+                    }
+                }
+            }
+            vsum = tce_warp_sum(vsum);
+            V -= pref * vsum;
+            __syncwarp();
+        }
+    if (lane == 0) A.V[A.plist ? pair : fi + (long long)S.nfuc * fj] = fabs(V) < 1e-14 ? 0.0 : V;
+}
+
 }  // namespace
 
 using namespace tcehost;
@@ -255,8 +440,16 @@ static int nuclear_elements(Handle *h, int natoms, const double *geo, const int3
         return fail(h, TCE_ERR_UNSUPPORTED, "truncation order too large for the nuclear-attraction kernel");
     }
     const size_t smem = wbytes * (size_t)warps;
-    cudaFuncSetAttribute(k_nuclear, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_nuclear<<<(unsigned)((npairs + warps - 1) / warps), 32 * warps, smem, h->st>>>(h->S, A);
+    // one periodic direction with a 32- or 64-node rule: the tensor-core form
+    const unsigned grid = (unsigned)((npairs + warps - 1) / warps);
+    if (h->use_tc && h->ndp == 1 && (h->nq == 32 || h->nq == 64)) {
+        auto kern = h->nq == 32 ? k_nuclear_tc<32> : k_nuclear_tc<64>;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<grid, 32 * warps, smem, h->st>>>(h->S, A);
+    } else {
+        cudaFuncSetAttribute(k_nuclear, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_nuclear<<<grid, 32 * warps, smem, h->st>>>(h->S, A);
+    }
     cudaError_t e = cudaGetLastError();
     out.assign((size_t)npairs, 0.0);
     if (e == cudaSuccess) e = cudaMemcpyAsync(out.data(), d_V, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, h->st);
