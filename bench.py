@@ -2,7 +2,7 @@
 """Benchmark: toroidal ERI quartets/s of one integral-direct J/K build,
 learned grid vs the plain adaptive method.
 
-Workload (BASELINE config "Tori1D RHF H chain", the quoted one): 64 cells,
+Workload (the Tori1D RHF H chain the metric is quoted on): 64 cells,
 spacing 1.8 bohr, torus length 115.2 bohr, per H 3 contracted s (4 primitives,
 exponents log-uniform in [0.1,20], seeded) + 1 p (0.727); 384 functions;
 synthetic inputs (seeded), normalised as the Fortran caller would.
