@@ -136,13 +136,15 @@ def ao_to_kmo_stage(eng, r):
     from william_ci_b200 import df
     t0 = time.perf_counter()
     eri = eng.ERI_integral_toroidal()
-    t1 = time.perf_counter()
+    te = time.perf_counter()
     gb = eri.nbytes / 1e9
-    del eri
+    del eri                                   # the host copy; the device keeps its own
     pr, qr = df.band_ranges(r.occ_k)
+    eng.ao_to_kmo(r.C_k, pr, qr)              # warm-up (module load, first allocations)
+    t1 = time.perf_counter()
     out = eng.ao_to_kmo(r.C_k, pr, qr)
     t2 = time.perf_counter()
-    return {"stored_eri_s": t1 - t0, "stored_eri_gb": gb, "ao_to_kmo_s": t2 - t1, "shape": list(out.shape),
+    return {"stored_eri_s": te - t0, "stored_eri_gb": gb, "ao_to_kmo_s": t2 - t1, "shape": list(out.shape),
             "api": "tce_eri_stored then tce_ao_to_kmo (integrals resident on the device, host output)"}
 
 
