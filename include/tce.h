@@ -109,11 +109,14 @@ int tce_shell_block(void *handle, const int32_t sh4[4], int32_t mode, double *bl
  * inside the library would fail or fragment the pool.  No counterpart in the
  * reference.  The call allocates nothing: its scratch (work counter, work
  * item, block) is one file-scope device array of 12 KiB that every GPU using
- * the library holds until exit.  The first call on a device resolves the
- * array's device address; make that first call before any stream capture.
- * Blocks of more than 6^4 integrals are rejected (TCE_ERR_UNSUPPORTED).  All
- * calls share the array: calls that overlap on the GPU race, so do not issue
- * them concurrently from several threads or handles. */
+ * the library holds until exit.  The array's device address is resolved and
+ * the quartet kernel loaded when the handle is created (tce_create /
+ * tce_create_blocks), so that a call never loads a module lazily; the call
+ * runs on the handle's device whichever device the calling thread has
+ * current.  Blocks of more than 6^4 integrals are rejected
+ * (TCE_ERR_UNSUPPORTED).  All calls share the array: calls that overlap on
+ * the GPU race, so do not issue them concurrently from several threads or
+ * handles. */
 int tce_shell_block_noalloc(void *handle, const int32_t sh4[4], int32_t mode, double *blk);
 
 /* Start-up accuracy gate of the fast rule (replaces the ERI part of
@@ -253,6 +256,14 @@ const char *tce_dfjk_last_error(void *handle);
  * iteration).  The OpenMP task unit of the reference is the bra shell pair
  * (eri_direct.f90:298-317); here it is the shell quartet. */
 int tce_set_shard(void *handle, int32_t rank, int32_t nranks);
+
+/* The shell quartets of the handle's current shard (all of them when
+ * unsharded), in the engine's order: *n of them; with items != NULL,
+ * items[4*i .. 4*i+3].  Lets a caller see which quartets a rank evaluates, or
+ * check one shard against another implementation.  No reference counterpart
+ * (the reference splits the bra shell pairs among OpenMP threads,
+ * eri_direct.f90:298-317). */
+int tce_shard_items(void *handle, int64_t *n, int32_t *items);
 
 /* Host-only planner used by tce_set_shard: greedy longest-first assignment
  * of n work items with the given costs to nranks owners (owner[i] in

@@ -5,8 +5,9 @@ gauss_legendre_points (src/module/precompute_t.f90:484-895) as text, exactly
 as written in the reference, so the oracle's table rules and the fast-quad
 self-check can use the reference's own nodes and weights.
 
-Run in the build container (the reference tree is not on the GPU box):
-    python tests/golden/make_quad_tables.py /root/reference
+Run where the reference tree is present (it is not on the GPU box), with the
+root of the reference project as the one required argument:
+    python tests/golden/make_quad_tables.py <reference-root>
 """
 import json
 import os
@@ -32,4 +33,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_quad_tables.py <reference-root>")
+    main(sys.argv[1])

@@ -10,6 +10,7 @@
 #include <atomic>
 #include <cmath>
 #include <mutex>
+#include <queue>
 #include <cstdio>
 #include <cstring>
 #include <numeric>
@@ -319,6 +320,7 @@ int build(Handle *h, const tce_system *sys)
     // ---------------- device ----------------
     int dev = 0;
     CK(h, cudaGetDevice(&dev));
+    h->dev = dev;
     CK(h, cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, dev));
     CK(h, cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
     CK(h, cudaEventCreate(&h->ev0));
@@ -750,6 +752,8 @@ const char *tce_last_error(void *handle)
     return g_err.c_str();
 }
 
+static int noalloc_prepare(Handle *h);
+
 static int create_impl(const tce_system *sys, void **handle, bool blocks_only)
 {
     if (!handle) return fail(nullptr, TCE_ERR_ARG, "handle is NULL");
@@ -757,6 +761,7 @@ static int create_impl(const tce_system *sys, void **handle, bool blocks_only)
     Handle *h = new Handle();
     h->blocks_only = blocks_only ? 1 : 0;
     int s = build(h, sys);
+    if (s == TCE_OK) s = noalloc_prepare(h);
     if (s != TCE_OK) {
         g_err = h->err;
         for (void *p : h->allocs) cudaFree(p);
@@ -824,13 +829,17 @@ int tce_get_info(void *handle, tce_info *info)
 int tce_shard_plan(const double *cost, int64_t n, int32_t nranks, int32_t *owner)
 {
     if (nranks < 1 || n < 0 || (n > 0 && (!cost || !owner))) return fail(nullptr, TCE_ERR_ARG, "bad argument");
-    std::vector<double> load(nranks, 0.0);
+    // least-loaded owner first, ties to the lowest rank: a min-heap of
+    // (load, rank), O(n log nranks) so that fine partitions stay cheap
+    using Slot = std::pair<double, int32_t>;
+    std::priority_queue<Slot, std::vector<Slot>, std::greater<Slot>> heap;
+    for (int32_t r = 0; r < nranks; ++r) heap.push(Slot(0.0, r));
     for (int64_t i = 0; i < n; ++i) {
-        int best = 0;
-        for (int r = 1; r < nranks; ++r)
-            if (load[r] < load[best]) best = r;
-        owner[i] = best;
-        load[best] += cost[i] > 0 ? cost[i] : 0.0;
+        Slot sl = heap.top();
+        heap.pop();
+        owner[i] = sl.second;
+        sl.first += cost[i] > 0 ? cost[i] : 0.0;
+        heap.push(sl);
     }
     return TCE_OK;
 }
@@ -854,6 +863,22 @@ int tce_set_shard(void *handle, int32_t rank, int32_t nranks)
     h->shard_rank = rank;
     h->shard_nranks = nranks;
     CK(h, cudaStreamSynchronize(h->st));
+    return TCE_OK;
+}
+
+int tce_shard_items(void *handle, int64_t *n, int32_t *items)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !n) return fail(h, TCE_ERR_ARG, "NULL argument");
+    *n = (int64_t)h->shard_idx.size();
+    if (items)
+        for (size_t i = 0; i < h->shard_idx.size(); ++i) {
+            const int4 &q = h->items_host[(size_t)h->shard_idx[i]];
+            items[4 * i] = q.x;
+            items[4 * i + 1] = q.y;
+            items[4 * i + 2] = q.z;
+            items[4 * i + 3] = q.w;
+        }
     return TCE_OK;
 }
 
@@ -1012,30 +1037,53 @@ static __device__ __align__(256) unsigned char g_tce_static_scratch[TCE_STATIC_S
 static_assert(TCE_STATIC_OFF_BLK + TCE_STATIC_MAX_BLOCK * sizeof(double) <= TCE_STATIC_SCRATCH_BYTES,
               "static scratch too small for a (dd|dd) block");
 
-namespace {
-constexpr int kMaxDevices = 64;
-std::mutex g_static_mu;
-unsigned char *g_static_ptr[kMaxDevices] = {nullptr};
-
-// Device address of the array on the current device, resolved once per device
-// (the symbol name is only a host-side stand-in for the device storage).
-int static_scratch(Handle *h, unsigned char **out)
+// Device address of the array in the current context.  The symbol name is only
+// a host-side stand-in for the device storage, so host code must ask the
+// runtime for the address; the lookup is repeated on every call (it is cheap)
+// so that a context created anew after cudaDeviceReset is never handed an old
+// address.
+static int static_scratch(Handle *h, unsigned char **out)
 {
-    int dev = 0;
-    CK(h, cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) return fail(h, TCE_ERR_UNSUPPORTED, "device index beyond 64");
-    std::lock_guard<std::mutex> lock(g_static_mu);
-    if (!g_static_ptr[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_tce_static_scratch);
-        if (e != cudaSuccess)
-            return fail(h, TCE_ERR_CUDA, std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
-        g_static_ptr[dev] = static_cast<unsigned char *>(p);
-    }
-    *out = g_static_ptr[dev];
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_tce_static_scratch);
+    if (e != cudaSuccess)
+        return fail(h, TCE_ERR_CUDA, std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
+    *out = static_cast<unsigned char *>(p);
     return TCE_OK;
 }
-}  // namespace
+
+// Run at handle creation, on the handle's device: resolve the array's address
+// and load the quartet kernel of the handle's rule, so that with lazy module
+// loading (the CUDA default) neither happens during a tce_shell_block_noalloc
+// call, where loading a module could take device memory.
+static int noalloc_prepare(Handle *h)
+{
+    unsigned char *p = nullptr;
+    int s = static_scratch(h, &p);
+    if (s) return s;
+    if (tce_preload_quartets(h->S.nq) != TCE_OK) {
+        cudaError_t e = cudaGetLastError();
+        return fail(h, TCE_ERR_CUDA, std::string("loading the quartet kernel: ") + cudaGetErrorString(e));
+    }
+    return TCE_OK;
+}
+
+// Makes the handle's device current for the duration of a call and restores
+// the caller's device afterwards.
+struct DeviceScope {
+    int prev = -1;
+    cudaError_t err = cudaSuccess;
+    explicit DeviceScope(int dev)
+    {
+        err = cudaGetDevice(&prev);
+        if (err == cudaSuccess && prev != dev) err = cudaSetDevice(dev);
+        else prev = -1;
+    }
+    ~DeviceScope()
+    {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
 
 int tce_shell_block_noalloc(void *handle, const int32_t sh4[4], int32_t mode, double *blk)
 {
@@ -1049,6 +1097,10 @@ int tce_shell_block_noalloc(void *handle, const int32_t sh4[4], int32_t mode, do
     if (nblk > TCE_STATIC_MAX_BLOCK)
         return fail(h, TCE_ERR_UNSUPPORTED, "block of " + std::to_string(nblk) + " integrals exceeds the static scratch (" +
                                                  std::to_string(TCE_STATIC_MAX_BLOCK) + ")");
+    // the array, the stream and the kernel all belong to the handle's device,
+    // whichever device the calling thread has current
+    DeviceScope dscope(h->dev);
+    CK(h, dscope.err);
     unsigned char *base = nullptr;
     int s = static_scratch(h, &base);
     if (s) return s;
@@ -1056,8 +1108,10 @@ int tce_shell_block_noalloc(void *handle, const int32_t sh4[4], int32_t mode, do
     int4 q = make_int4(shift_to(h, sh4[0], c1, h->nshuc), shift_to(h, sh4[1], c1, h->nshuc),
                        shift_to(h, sh4[2], c1, h->nshuc), shift_to(h, sh4[3], c1, h->nshuc));
     long long off[2] = {0, nblk};
-    // the work counter must start at zero; the item and offsets are rewritten every call
-    CK(h, cudaMemsetAsync(base + TCE_STATIC_OFF_NEXT, 0, sizeof(unsigned int), h->st));
+    // The item and offsets are rewritten every call; the launch below zeroes the
+    // work counter itself.  Every element of the block is written by the kernel
+    // (TCE_MODE_BLOCK / NOSCREEN copy the whole block), so the previous call's
+    // contents of the array cannot reach this result.
     CK(h, cudaMemcpyAsync(base + TCE_STATIC_OFF_ITEM, &q, sizeof q, cudaMemcpyHostToDevice, h->st));
     CK(h, cudaMemcpyAsync(base + TCE_STATIC_OFF_BOFF, off, sizeof off, cudaMemcpyHostToDevice, h->st));
     QuartetHostArgs a;

@@ -30,6 +30,7 @@ struct Handle {
     double Qmax = 0.0;
     std::vector<int> tnmax;
     // device
+    int dev = 0;                         // CUDA device the handle was built on
     cudaStream_t st = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;   // ordering with a caller on the legacy stream

@@ -58,6 +58,9 @@ struct QuartetHostArgs {
 
 long long tce_plain_scratch_per_warp(const DevSys &S, int max_ncq);
 int tce_launch_quartets(const DevSys &S, const QuartetHostArgs &h, cudaStream_t st);
+// Load the generic quartet kernel for nq nodes on the current device now (with
+// lazy module loading it is otherwise loaded by its first launch).
+int tce_preload_quartets(int nq);
 
 // all-s shell quartets, J/K mode (k_quartets_s)
 struct SArgsHost {

@@ -994,7 +994,7 @@ int tce_launch_quartets(const DevSys &S, const QuartetHostArgs &h, cudaStream_t 
     while (warps > 1 && wbytes * warps > 220 * 1024) --warps;
     if (wbytes > 220 * 1024) return TCE_ERR_UNSUPPORTED;
     const size_t smem = wbytes * warps;
-    cudaMemsetAsync(h.next, 0, sizeof(unsigned int), st);
+    if (cudaMemsetAsync(h.next, 0, sizeof(unsigned int), st) != cudaSuccess) return TCE_ERR_CUDA;
     const int nsm = h.num_sms > 0 ? h.num_sms : 148;
     cudaError_t e;
     if (plain) {
@@ -1014,6 +1014,18 @@ int tce_launch_quartets(const DevSys &S, const QuartetHostArgs &h, cudaStream_t 
     else if (nq == 40) e = launch_nq<40>(S, A, wbytes, nsm, st);
     else if (nq == 64) e = launch_nq<64>(S, A, wbytes, nsm, st);
     else if (nq == 128) e = launch_nq<128>(S, A, wbytes, nsm, st);
+    else return TCE_ERR_UNSUPPORTED;
+    return e == cudaSuccess ? TCE_OK : TCE_ERR_CUDA;
+}
+
+int tce_preload_quartets(int nq)
+{
+    cudaFuncAttributes fa;
+    cudaError_t e;
+    if (nq == 32) e = cudaFuncGetAttributes(&fa, k_quartets<32>);
+    else if (nq == 40) e = cudaFuncGetAttributes(&fa, k_quartets<40>);
+    else if (nq == 64) e = cudaFuncGetAttributes(&fa, k_quartets<64>);
+    else if (nq == 128) e = cudaFuncGetAttributes(&fa, k_quartets<128>);
     else return TCE_ERR_UNSUPPORTED;
     return e == cudaSuccess ? TCE_OK : TCE_ERR_CUDA;
 }

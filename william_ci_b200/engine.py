@@ -45,7 +45,7 @@ EXPORTS = ["tce_create", "tce_destroy", "tce_last_error", "tce_get_info", "tce_s
            "tce_set_fp32_threshold", "tce_dfmp2_energy", "tce_mp2_last_error", "tce_create_blocks",
            "tce_pass_kernels", "tce_set_tensor_cores", "tce_nuclear_attraction", "tce_quad_self_check_nuc",
            "tce_lg_autotune", "tce_lg_lists", "tce_dfjk_create", "tce_dfjk", "tce_dfjk_destroy",
-           "tce_dfjk_last_error", "tce_ao_to_kmo"]
+           "tce_dfjk_last_error", "tce_ao_to_kmo", "tce_shard_items"]
 
 TCE_METHOD_FIXED, TCE_METHOD_LEARNED, TCE_METHOD_PLAIN = 0, 1, 2
 TCE_NFEAT = 12
@@ -103,6 +103,7 @@ def lib():
         L.tce_last_kernel_ms.argtypes = [C.c_void_p, _dp]
         L.tce_set_shard.argtypes = [C.c_void_p, C.c_int32, C.c_int32]
         L.tce_shard_plan.argtypes = [_dp, C.c_int64, C.c_int32, _ip]
+        L.tce_shard_items.argtypes = [C.c_void_p, _lp, _ip]
         L.tce_fp64_peak.argtypes = [_dp]
         L.tce_version.restype = C.c_char_p
         L.tce_items.argtypes = [C.c_void_p, _ip]
@@ -306,6 +307,14 @@ class Engine:
 
     def set_shard(self, rank: int, nranks: int):
         _check(lib().tce_set_shard(self.h, int(rank), int(nranks)), self.h)
+
+    def shard_items(self) -> np.ndarray:
+        """The shell quartets of the current shard (tce_shard_items), shape (n, 4)."""
+        n = C.c_int64()
+        _check(lib().tce_shard_items(self.h, C.byref(n), None), self.h)
+        it = np.zeros(4 * max(n.value, 1), dtype=np.int32)
+        _check(lib().tce_shard_items(self.h, C.byref(n), _i(it)), self.h)
+        return it[:4 * n.value].reshape(n.value, 4)
 
     def stored_JK(self, P: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
         n = self.nbas
