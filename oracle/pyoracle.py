@@ -13,6 +13,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
+FAST_LIB_PATH = os.path.join(HERE, "liboracle_fast.so")
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -30,7 +31,15 @@ def build():
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
+def build_fast(force=True):
+    """The timing build (reference compiler flags, -march=native, pair-vector
+    memo) for this host; rebuilt by default since -march=native ties it to the
+    machine that compiles it."""
+    subprocess.run(["make", "-s", "-C", HERE] + (["-B"] if force else []) + ["fast"], check=True)
+
+
 _lib = None
+_lib_fast = None
 
 
 def lib():
@@ -38,7 +47,22 @@ def lib():
     if _lib is None:
         if not os.path.exists(LIB_PATH):
             build()
-        L = C.CDLL(LIB_PATH)
+        _lib = _bind(C.CDLL(LIB_PATH))
+    return _lib
+
+
+def lib_fast():
+    """liboracle_fast.so (built for this host by build_fast first if absent)."""
+    global _lib_fast
+    if _lib_fast is None:
+        if not os.path.exists(FAST_LIB_PATH):
+            build_fast()
+        _lib_fast = _bind(C.CDLL(FAST_LIB_PATH))
+    return _lib_fast
+
+
+def _bind(L):
+    if True:
         L.orc_iv_log.restype = C.c_double
         L.orc_iv_log.argtypes = [C.c_double, C.c_double]
         L.orc_iv_scaled.restype = C.c_double
@@ -84,8 +108,10 @@ def lib():
         L.orc_overlap_pair.argtypes = [C.c_int, _dp, _ip, _ip, _dp, _dp, C.c_int, _dp, _dp, C.c_int, _dp, _dp]
         L.orc_normalize.restype = C.c_double
         L.orc_normalize.argtypes = [C.c_int, _dp, C.c_int, _dp, _ip, _ip, _dp, _dp]
-        _lib = L
-    return _lib
+        L.orc_pair_cache_free.argtypes = []
+        L.orc_shell_blocks.restype = C.c_int64
+        L.orc_shell_blocks.argtypes = [C.c_void_p, C.c_int64, _ip, C.c_int, _dp]
+    return L
 
 
 def dptr(a: np.ndarray):
@@ -148,7 +174,10 @@ class Oracle:
     """The oracle engine for one supercell basis (direct_init + drivers)."""
 
     def __init__(self, sys, nquad=32, t_nodes=None, t_weights=None, physicist=False, sao=True,
-                 prim_screen=True, schwarz_thr=1e-13, prim_thr=1e-14):
+                 prim_screen=True, schwarz_thr=1e-13, prim_thr=1e-14, fast=False):
+        """fast=True: the timing build (liboracle_fast.so, reference compiler
+        flags and pair-vector memo) instead of the parity build."""
+        self.L = lib_fast() if fast else lib()
         self.sys = sys
         self._keep = [np.ascontiguousarray(sys.ctr, dtype=np.float64).ravel(),
                       np.ascontiguousarray(sys.lxyz, dtype=np.int32).ravel(),
@@ -184,11 +213,11 @@ class Oracle:
         self.sao = sao
         self.physicist = physicist
         self._s = s
-        self.h = lib().orc_create(C.byref(s))
+        self.h = self.L.orc_create(C.byref(s))
 
     def close(self):
         if self.h:
-            lib().orc_destroy(self.h)
+            self.L.orc_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -201,23 +230,23 @@ class Oracle:
     def shells(self):
         nshuc = C.c_int32()
         ncap = C.c_int32()
-        nsh = lib().orc_nshells(self.h, C.byref(nshuc), C.byref(ncap))
+        nsh = self.L.orc_nshells(self.h, C.byref(nshuc), C.byref(ncap))
         out = []
         for s in range(nsh):
             f = C.c_int32()
             n = C.c_int32()
-            lib().orc_shell_info(self.h, s, C.byref(f), C.byref(n))
+            self.L.orc_shell_info(self.h, s, C.byref(f), C.byref(n))
             out.append((f.value, n.value))
         return out, nshuc.value, ncap.value
 
     def schwarz(self):
         n = self.sys.nbas
-        p = lib().orc_schwarz(self.h)
+        p = self.L.orc_schwarz(self.h)
         return np.ctypeslib.as_array(p, shape=(n * n,)).reshape(n, n, order="F").copy()
 
     def prim_table(self):
         mp = C.c_int32()
-        p = lib().orc_prim_table(self.h, C.byref(mp))
+        p = self.L.orc_prim_table(self.h, C.byref(mp))
         if not p:
             return None
         sh, nshuc, _ = self.shells()
@@ -229,7 +258,7 @@ class Oracle:
         w = _dp()
         tb = _dp()
         tn = _ip()
-        lib().orc_t_tables(self.h, C.byref(node), C.byref(w), C.byref(tb), C.byref(tn))
+        self.L.orc_t_tables(self.h, C.byref(node), C.byref(w), C.byref(tb), C.byref(tn))
         _, _, ncap = self.shells()
         nq, ndp = self.nquad, self.sys.ndp
         return (np.ctypeslib.as_array(node, shape=(nq,)).copy(), np.ctypeslib.as_array(w, shape=(nq,)).copy(),
@@ -240,14 +269,27 @@ class Oracle:
         sh, _, _ = self.shells()
         n = [sh[S][1] for S in (S1, S2, S3, S4)]
         blk = np.zeros(n[0] * n[1] * n[2] * n[3])
-        lib().orc_shell_block(self.h, S1, S2, S3, S4, mode, dptr(blk))
+        self.L.orc_shell_block(self.h, S1, S2, S3, S4, mode, dptr(blk))
         return blk.reshape(n, order="F")
+
+    def shell_blocks(self, items, mode=1):
+        """Blocks of the given shell quartets (rows of 4), concatenated in item
+        order (each column-major), and their offsets; OpenMP over the quartets."""
+        it = np.ascontiguousarray(items, dtype=np.int32).reshape(-1, 4)
+        sh, _, _ = self.shells()
+        n = np.array([x[1] for x in sh], dtype=np.int64)
+        sizes = np.prod(n[it], axis=1) if len(it) else np.zeros(0, dtype=np.int64)
+        offs = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+        out = np.zeros(max(int(offs[-1]), 1))
+        if len(it):
+            self.L.orc_shell_blocks(self.h, len(it), iptr(it), int(mode), dptr(out))
+        return out[:offs[-1]], offs
 
     def eri_stored(self):
         n = self.sys.nbas
         esz = self.sys.nfuc if self.sao else n
         eri = np.zeros(esz * n * n * n)
-        nq = lib().orc_eri_stored(self.h, dptr(eri))
+        nq = self.L.orc_eri_stored(self.h, dptr(eri))
         return eri.reshape((esz, n, n, n), order="F"), nq
 
     def direct_jk(self, P):
@@ -255,13 +297,13 @@ class Oracle:
         Pf = np.asfortranarray(P, dtype=np.float64).ravel(order="F").copy()
         J = np.zeros(n * n)
         K = np.zeros(n * n)
-        nq = lib().orc_direct_jk(self.h, dptr(Pf), dptr(J), dptr(K))
+        nq = self.L.orc_direct_jk(self.h, dptr(Pf), dptr(J), dptr(K))
         return J.reshape(n, n, order="F"), K.reshape(n, n, order="F"), nq
 
     def items(self) -> np.ndarray:
-        n = lib().orc_items(self.h, None, 0)
+        n = self.L.orc_items(self.h, None, 0)
         out = np.zeros((max(n, 1), 4), dtype=np.int32)
-        lib().orc_items(self.h, iptr(out), n)
+        self.L.orc_items(self.h, iptr(out), n)
         return out[:n]
 
     def direct_jk_items(self, items, P, J=None, K=None):
@@ -271,7 +313,7 @@ class Oracle:
         Pf = np.asfortranarray(P, dtype=np.float64).ravel(order="F").copy()
         Jf = np.zeros(n * n) if J is None else np.asfortranarray(J).ravel(order="F").copy()
         Kf = np.zeros(n * n) if K is None else np.asfortranarray(K).ravel(order="F").copy()
-        nf = lib().orc_direct_jk_items(self.h, iptr(it), len(it), dptr(Pf), dptr(Jf), dptr(Kf))
+        nf = self.L.orc_direct_jk_items(self.h, iptr(it), len(it), dptr(Pf), dptr(Jf), dptr(Kf))
         return Jf.reshape(n, n, order="F"), Kf.reshape(n, n, order="F"), nf
 
     def one_electron(self):
@@ -280,12 +322,12 @@ class Oracle:
         geo = np.ascontiguousarray(self.sys.geometry, dtype=np.float64).ravel()
         Z = np.ascontiguousarray(self.sys.charges, dtype=np.int32)
         S, T, V = (np.zeros(n * n) for _ in range(3))
-        lib().orc_one_electron(self.h, len(Z), dptr(geo), iptr(Z), dptr(S), dptr(T), dptr(V))
+        self.L.orc_one_electron(self.h, len(Z), dptr(geo), iptr(Z), dptr(S), dptr(T), dptr(V))
         return tuple(M.reshape(n, n, order="F") for M in (S, T, V))
 
     def count(self):
         a, b, c = C.c_int64(), C.c_int64(), C.c_int64()
-        lib().orc_count(self.h, C.byref(a), C.byref(b), C.byref(c))
+        self.L.orc_count(self.h, C.byref(a), C.byref(b), C.byref(c))
         return a.value, b.value, c.value
 
 

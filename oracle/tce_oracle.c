@@ -4,9 +4,10 @@
  * the parity status.  Each routine names the reference file:line it restates
  * (paths relative to the reference project root).
  *
- * Not restated: the pair-vector memo (clifford_tools.f90:467-549 caches the
- * vectors; the values are the same when recomputed), the point-group
- * "symmetry" keyword, and the timers.
+ * The pair-vector memo (clifford_tools.f90:467-549) is compiled only into the
+ * timing build (ORC_PAIR_MEMO); the parity build recomputes the vectors, which
+ * gives the same values.  Not restated: the point-group "symmetry" keyword and
+ * the timers.
  */
 #include <math.h>
 #include <float.h>
@@ -208,6 +209,97 @@ void orc_pair_vector(int N, double A, int i, int l, double phA, double phB, int 
     }
     free(Iv);
 }
+
+/* Memo of the pair Fourier vectors, as pair_vector_cached keeps them
+ * (clifford_tools.f90:467-549): one table shared by the OpenMP threads, keyed
+ * by the bits of (A, phA, phB) and (N, i, l, sgn), open addressing with up to
+ * 64 probes, lock-free lookups (the slot's offset is published last), inserts
+ * one at a time, a pool of at most 16e6 complex numbers (256 MB); a vector that
+ * does not fit is returned uncached.  Compiled only into the timing build
+ * (ORC_PAIR_MEMO, Makefile target `fast`): the parity build recomputes every
+ * vector, which gives the same values. */
+#ifdef ORC_PAIR_MEMO
+#define PV_SLOTS (1u << 18)
+#define PV_POOL_MAX 16000000LL
+static int64_t *pv_key;            /* [4 * PV_SLOTS] */
+static int64_t *pv_off;            /* [PV_SLOTS], -1 = empty; offset in complex numbers */
+static double *pv_pool;            /* [2 * PV_POOL_MAX], re/im interleaved */
+static int64_t pv_used;
+static int pv_ready;
+
+static void pv_init(void)
+{
+    if (__atomic_load_n(&pv_ready, __ATOMIC_ACQUIRE)) return;
+    #pragma omp critical(orc_pv_cache)
+    {
+        if (!pv_ready) {
+            pv_key = (int64_t *)malloc(sizeof(int64_t) * 4 * (size_t)PV_SLOTS);
+            pv_off = (int64_t *)malloc(sizeof(int64_t) * (size_t)PV_SLOTS);
+            pv_pool = (double *)malloc(sizeof(double) * 2 * (size_t)PV_POOL_MAX);
+            for (size_t h = 0; h < PV_SLOTS; ++h) pv_off[h] = -1;
+            pv_used = 0;
+            __atomic_store_n(&pv_ready, 1, __ATOMIC_RELEASE);
+        }
+    }
+}
+
+void orc_pair_cache_free(void)
+{
+    free(pv_key); free(pv_off); free(pv_pool);
+    pv_key = pv_off = NULL; pv_pool = NULL;
+    pv_used = 0;
+    pv_ready = 0;
+}
+
+static void pair_vector_memo(int N, double A, int i, int l, double phA, double phB, int sgn, double *vre, double *vim)
+{
+    pv_init();
+    int64_t k[4];
+    memcpy(&k[0], &A, 8); memcpy(&k[1], &phA, 8); memcpy(&k[2], &phB, 8);
+    k[3] = (int64_t)N + 1000000LL * ((int64_t)i + 64LL * ((int64_t)l + 64LL * (int64_t)(sgn + 1)));
+    uint64_t hh = (uint64_t)k[0] * 31u + (uint64_t)k[1];
+    hh = hh * 31u + (uint64_t)k[2];
+    hh = hh * 31u + (uint64_t)k[3];
+    hh ^= hh >> 31;
+    const unsigned h0 = (unsigned)(hh & (PV_SLOTS - 1));
+    unsigned h = h0;
+    for (int probe = 0; probe < 64; ++probe) {
+        int64_t o = __atomic_load_n(&pv_off[h], __ATOMIC_ACQUIRE);
+        if (o < 0) break;
+        const int64_t *key = pv_key + 4 * (size_t)h;
+        if (key[0] == k[0] && key[1] == k[1] && key[2] == k[2] && key[3] == k[3]) {
+            const double *v = pv_pool + 2 * o;
+            for (int m = 0; m <= N; ++m) { vre[m] = v[2 * m]; vim[m] = v[2 * m + 1]; }
+            return;
+        }
+        h = (h + 1) & (PV_SLOTS - 1);
+    }
+    orc_pair_vector(N, A, i, l, phA, phB, sgn, vre, vim);
+    #pragma omp critical(orc_pv_cache)
+    {
+        unsigned g = h0;
+        int free_slot = 0;
+        for (int probe = 0; probe < 64; ++probe) {
+            if (pv_off[g] < 0) { free_slot = 1; break; }
+            const int64_t *key = pv_key + 4 * (size_t)g;
+            if (key[0] == k[0] && key[1] == k[1] && key[2] == k[2] && key[3] == k[3]) break;
+            g = (g + 1) & (PV_SLOTS - 1);
+        }
+        if (free_slot && pv_used + N + 1 <= PV_POOL_MAX) {
+            const int64_t o = pv_used;
+            double *v = pv_pool + 2 * o;
+            for (int m = 0; m <= N; ++m) { v[2 * m] = vre[m]; v[2 * m + 1] = vim[m]; }
+            pv_used += N + 1;
+            memcpy(pv_key + 4 * (size_t)g, k, sizeof k);
+            __atomic_store_n(&pv_off[g], o, __ATOMIC_RELEASE);
+        }
+    }
+}
+#define PAIR_VECTOR pair_vector_memo
+#else
+void orc_pair_cache_free(void) {}
+#define PAIR_VECTOR orc_pair_vector
+#endif
 
 /* fast_quad_points precompute_t.f90:906-942 : GL on [0,1], t = 0.6u/(1-u) */
 void orc_fast_quad_points(int n, double *t, double *w)
@@ -674,7 +766,7 @@ static void shell_block(const orc_ctx *c, const shellv *SA, const shellv *SB, co
                     Aarg = 2.0 * pe / (av[d] * av[d]);
                     for (int ia = 0; ia <= lsA; ++ia)
                         for (int ib = 0; ib <= lsB; ++ib)
-                            orc_pair_vector(b_N[d], Aarg, ia, ib, av[d] * (cen - rA[d]), av[d] * (cen - rB[d]), -1,
+                            PAIR_VECTOR(b_N[d], Aarg, ia, ib, av[d] * (cen - rA[d]), av[d] * (cen - rB[d]), -1,
                                             &Gre[GI(0, ia, ib, d)], &Gim[GI(0, ia, ib, d)]);
                 } else {
                     for (int ia = 0; ia <= lsA; ++ia)
@@ -703,7 +795,7 @@ static void shell_block(const orc_ctx *c, const shellv *SA, const shellv *SB, co
                             for (int ic = 0; ic <= lsC; ++ic)
                                 for (int id = 0; id <= lsD; ++id) {
                                     size_t o = (size_t)k_off[d + 3 * kl] + (size_t)(kN + 1) * (ic + (lsC + 1) * id);
-                                    orc_pair_vector(kN, KA, ic, id, av[d] * (kcen - rC[d]), av[d] * (kcen - rD[d]), 1,
+                                    PAIR_VECTOR(kN, KA, ic, id, av[d] * (kcen - rC[d]), av[d] * (kcen - rD[d]), 1,
                                                     &Hre[o], &Him[o]);
                                 }
                         }
@@ -888,6 +980,27 @@ void orc_shell_block(orc_ctx *c, int S1, int S2, int S3, int S4, int mode, doubl
     }
     shell_block(c, &v[0], &v[1], &v[2], &v[3], mode == 2, pb, pk, c->mp, blk);
     free(v);
+}
+
+/* Blocks of n shell quartets (items4[4*i..4*i+3]), concatenated in item order,
+ * each column-major as orc_shell_block; OpenMP over the quartets.  Returns the
+ * number of doubles written. */
+int64_t orc_shell_blocks(orc_ctx *c, int64_t n, const int32_t *items4, int mode, double *out)
+{
+    int64_t *off = malloc(sizeof(int64_t) * (size_t)(n + 1));
+    off[0] = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        const int32_t *q = items4 + 4 * i;
+        off[i + 1] = off[i] + (int64_t)c->sh_n[q[0]] * c->sh_n[q[1]] * c->sh_n[q[2]] * c->sh_n[q[3]];
+    }
+    #pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t i = 0; i < n; ++i) {
+        const int32_t *q = items4 + 4 * i;
+        orc_shell_block(c, q[0], q[1], q[2], q[3], mode, out + off[i]);
+    }
+    int64_t tot = off[n];
+    free(off);
+    return tot;
 }
 
 orc_ctx *orc_create(const orc_system *sys)

@@ -65,6 +65,11 @@ void   orc_hermite_E_1D(int i, int j, double p, double PA, double PB, double *E1
 typedef struct orc_ctx orc_ctx;
 orc_ctx *orc_create(const orc_system *sys);
 void     orc_destroy(orc_ctx *c);
+/* Blocks of n shell quartets, concatenated in item order (OpenMP over them). */
+int64_t  orc_shell_blocks(orc_ctx *c, int64_t n, const int32_t *items4, int mode, double *out);
+/* Release the pair-vector memo of the timing build (pair_cache_free,
+ * clifford_tools.f90:555-561); a no-op in the parity build. */
+void     orc_pair_cache_free(void);
 int      orc_nshells(const orc_ctx *c, int *nshuc, int *ncap);
 void     orc_shell_info(const orc_ctx *c, int s, int *first, int *n);
 /* Schwarz matrix Q (nbas x nbas, col-major), shell maxima Qsh (nsh x nsh) */

@@ -1,0 +1,114 @@
+"""The learned grid on the whole 64-cell H chain (the named shape, 384
+functions), held to the oracle rather than to the device's own 128-node engine.
+
+The truth is the oracle (oracle/tce_oracle.c) run with the reference's own
+128-point t-table (gauss_legendre_points, precompute_t.f90:484-895), committed
+as fixtures because the 128-node oracle takes minutes on a few cores:
+
+* tests/golden/heldout_h_chain64.npz: 2000 held-out shell quartets (every
+  angular class) and their oracle blocks; the learned grid's blocks (the rule
+  the network picks, judged; rejects by the plain method) within 1e-10;
+* tests/golden/jk_h_chain64_table128.npz: J and K of the whole chain for the
+  SCF's starting density; the learned-grid pass within 1e-9;
+* tests/golden/scf_h_chain64.json: converged RHF energies (RHF_SAO.f90:237-336)
+  with the oracle's J/K; the device SCF with the learned grid equals the
+  128-table energy, and with the fixed 32-node rule the 32-node energy, each to
+  1e-8 Eh.  The two oracle energies differ by more than that (the 32-node
+  rule's integral errors reach 1.5e-9), which is what the learned grid buys.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, make_system
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(ROOT, "tests", "golden")
+TOL_INT = 1e-10
+
+
+def _rows(a, nf):
+    return np.asarray(a)[:nf]
+
+
+@pytest.fixture(scope="module")
+def chain64_lg():
+    from william_ci_b200 import learned_grid as LG
+    from william_ci_b200.engine import Engine
+    sysm = make_system("h_chain64")
+    eng = Engine(sysm)
+    LG.setup(eng)
+    ho = np.load(os.path.join(GOLD, "heldout_h_chain64.npz"))
+    items = eng.items()
+    held = {tuple(q) for q in ho["items"]}
+    pool = np.array([i for i, q in enumerate(map(tuple, items)) if q not in held])
+    rng = np.random.default_rng(2026)
+    train = items[rng.choice(pool, 8000, replace=False)]
+    ref = LG.ReferenceBlocks(sysm)
+    net, _, _ = LG.train_rule_net(eng, ref, train, epochs=60, seed=0)
+    ref.close()
+    eng.lg_predict_rules(net)
+    yield sysm, eng, net, ho
+    eng.close()
+
+
+def test_heldout_blocks_vs_oracle_table128(chain64_lg):
+    from william_ci_b200 import learned_grid as LG
+    sysm, eng, net, ho = chain64_lg
+    items = eng.items()
+    rule_of = {tuple(q): r for q, r in zip(items, eng.lg_item_rules())}
+    it, T, offs = ho["items"], ho["blocks"], ho["offsets"]
+    rules = np.array([rule_of[tuple(q)] for q in it])
+    worst, n_plain = 0.0, 0
+    for r in np.unique(rules):
+        m = np.nonzero(rules == r)[0]
+        if r == eng.nrules:
+            K, _, o2 = eng.rule_blocks(-2, it[m])
+            keep = np.ones(len(m), bool)
+        else:
+            K, G, o2 = eng.rule_blocks(int(r), it[m], judge=True)
+            keep = LG.judge_estimate(K, G, o2) <= LG.JUDGE_TOL
+            rej = m[~keep]
+            if len(rej):          # the judge's rejects: the plain method
+                Kp, _, op = eng.rule_blocks(-2, it[rej])
+                for j, i in enumerate(rej):
+                    worst = max(worst, float(np.abs(Kp[op[j]:op[j + 1]] - T[offs[i]:offs[i + 1]]).max()))
+                n_plain += len(rej)
+        for j in np.nonzero(keep)[0]:
+            i = m[j]
+            worst = max(worst, float(np.abs(K[o2[j]:o2[j + 1]] - T[offs[i]:offs[i + 1]]).max(initial=0.0)))
+    assert worst <= TOL_INT, worst
+    assert n_plain <= 0.01 * len(it)
+
+
+def test_jk_vs_oracle_table128(chain64_lg):
+    from william_ci_b200.engine import TCE_METHOD_LEARNED
+    sysm, eng, net, ho = chain64_lg
+    z = np.load(os.path.join(GOLD, "jk_h_chain64_table128.npz"))
+    nf = sysm.nfuc
+    eng.set_method(TCE_METHOD_LEARNED)
+    for _ in range(2):                      # the second pass with the judge's rejects routed
+        J, K = eng.direct_JK(z["P"])
+    dJ = np.abs(_rows(J, nf) - z["J"]).max()
+    dK = np.abs(_rows(K, nf) - z["K"]).max()
+    assert dJ <= 1e-9 and dK <= 1e-9, (dJ, dK)
+
+
+def test_converged_rhf_energy_vs_oracle(chain64_lg):
+    from william_ci_b200 import scf
+    from william_ci_b200.engine import TCE_METHOD_LEARNED, Engine
+    sysm, eng, net, ho = chain64_lg
+    ref = json.load(open(os.path.join(GOLD, "scf_h_chain64.json")))
+    z = np.load(os.path.join(GOLD, "systems", "h_chain64_onee.npz"))
+    S, T, V = (scf.fill_with_symmetry(z[k], sysm.nfuc, sysm.ncell) for k in ("S", "T", "V"))
+    args = (S, T, V, float(z["enuc"]), scf.n_occupied(sysm), sysm.nfuc, sysm.ncell)
+    eng.set_method(TCE_METHOD_LEARNED)
+    lg = scf.rhf_sao(*args, eng.direct_JK)
+    with Engine(sysm) as fx:
+        fixed = scf.rhf_sao(*args, fx.direct_JK)
+    assert lg.converged and fixed.converged
+    assert abs(lg.energy - ref["table_128"]["energy"]) < 1e-8, (lg.energy, ref["table_128"]["energy"])
+    assert abs(fixed.energy - ref["fast_quad_32"]["energy"]) < 1e-8, (fixed.energy, ref["fast_quad_32"]["energy"])

@@ -307,3 +307,32 @@ def test_bruteforce_periodic_direction():
         ref = eri(*q)
         v = o.shell_block(*q, mode=2).item()
         assert abs(v - ref) < 1e-9, (q, v, ref)
+
+
+@pytest.mark.parametrize("name,ncell", [("h_chain64", (8, 1, 1)), ("h2_sheet", (2, 2, 1))])
+def test_timing_build_does_the_same_work(name, ncell):
+    """The CPU baseline's timing build (reference compiler flags, -ffast-math,
+    pair-vector memo) evaluates the same quartets to the same J/K as the parity
+    build, twice in a row (the second pass reads the memo)."""
+    sysm = make_system(name, ncell)
+    P = random_density(sysm.nbas, seed=3)
+    ref = po.Oracle(sysm)
+    Jr, Kr, nr = ref.direct_jk(P)
+    po.build_fast(force=False)
+    fast = po.Oracle(sysm, fast=True)
+    for _ in range(2):
+        J, K, nf = fast.direct_jk(P)
+        assert nf == nr
+        assert np.abs(J - Jr).max() < 1e-10 and np.abs(K - Kr).max() < 1e-10
+    fast.close()
+    po.lib_fast().orc_pair_cache_free()
+
+
+def test_batched_blocks_equal_single_blocks():
+    sysm = make_system("h2_sheet", (2, 2, 1))
+    o = po.Oracle(sysm)
+    it = o.items()[:60]
+    B, off = o.shell_blocks(it)
+    for i in (0, 7, 59):
+        b = o.shell_block(*it[i]).ravel(order="F")
+        assert np.array_equal(B[off[i]:off[i + 1]], b)

@@ -186,6 +186,18 @@ class RHFResult:
     P: Optional[np.ndarray] = None            # the density of the last diagonalisation (nbas x nbas)
 
 
+def core_guess_density(S: np.ndarray, T: np.ndarray, V: np.ndarray, nO: int) -> np.ndarray:
+    """The starting density of rhf_sao: guess_AO_RHF_SAO (SAO/guess_RHF_SAO.f90:1-115),
+    the core Hamiltonian T + V diagonalised in the canonical orthogonal basis of
+    S and occupied by guess_occupy_cut."""
+    e, U = np.linalg.eigh(S)
+    X, _ = canonical_X(U, e)
+    cp = X.T @ (T + V) @ X
+    shift_dropped(X, cp)
+    eg, cg = np.linalg.eigh(cp)
+    return guess_occupy_cut(nO, eg, X @ cg)
+
+
 def rhf_sao(S: np.ndarray, T: np.ndarray, V: np.ndarray, enuc: float, nO: int, nfuc: int, ncell,
             jk: Callable[[np.ndarray], Tuple[np.ndarray, np.ndarray]], max_scf: int = MAX_SCF,
             thresh: float = THRESH, diis: bool = True, max_diis: int = MAX_DIIS) -> RHFResult:
