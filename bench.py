@@ -43,6 +43,13 @@ WORKLOAD = "h_chain64"
 SYSTEM_FIXTURE = os.path.join(ROOT, "tests", "golden", "systems", WORKLOAD + ".npz")
 ONEE_FIXTURE = os.path.join(ROOT, "tests", "golden", "systems", WORKLOAD + "_onee.npz")
 PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "jk_pass_learned_grid_h_chain64_traffic.json")
+GOLD = os.path.join(ROOT, "tests", "golden")
+# the 2D and 3D workloads at their named shapes: each timed on one cost-balanced
+# shard of its quartet list (a full pass of the sheet takes over a minute)
+NAMED = {"li_cube": {"shard": 256, "train": 6000,
+                     "workload": "Tori3D Li cube, 4x4x4 cells, d=2.5, L=10 bohr, 3s+2p per Li, nbas=576"},
+         "h2_sheet": {"shard": 1024, "train": 3000,
+                      "workload": "Tori2D H2 sheet, 8x8 cells, d=2.0, L=16x16 bohr, 2s+1p+1d per H, nbas=1408"}}
 L2_FLUSH_BYTES = 512 << 20
 FP32_THRESHOLD = 1e-6        # Schwarz product below which the node sums run in FP32
 
@@ -76,25 +83,38 @@ def config(sysm, extra=None):
 # ---------------------------------------------------------------------------
 # CPU baseline: the oracle port (C restatement of the reference, OpenMP)
 # ---------------------------------------------------------------------------
-def cpu_baseline(sysm, stride, reps=1):
+def cpu_baseline(sysm, stride):
+    """The oracle port on all host cores, two builds: the parity build (-O2,
+    no fast-math, pair vectors recomputed) and the timing build with the
+    reference's own compiler flags (-O3 -ffast-math -funroll-loops
+    -march=native, built here for this host) and its pair-vector memo.  `value`
+    is the faster one (the strongest CPU path available); each build's best of
+    two passes over the sample (the second pass reads the memo)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
-    o = pyoracle.Oracle(sysm)
-    items = o.items()
-    sample = items[::stride]
+    pyoracle.build_fast(force=True)
     P = density(sysm.nbas)
-    best = None
-    nf = 0
-    for _ in range(reps):
-        t0 = time.perf_counter()
-        _, _, nf = o.direct_jk_items(sample, P)
-        dt = time.perf_counter() - t0
-        best = dt if best is None else min(best, dt)
+    res, items, nf = {}, None, 0
+    for kind, fast, reps in (("parity_build", False, 1), ("timing_build", True, 2)):
+        o = pyoracle.Oracle(sysm, fast=fast)
+        if items is None:
+            items = o.items()
+        sample = items[::stride]
+        best = None
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            _, _, nf = o.direct_jk_items(sample, P)
+            dt = time.perf_counter() - t0
+            best = dt if best is None else min(best, dt)
+        res[kind] = {"value": nf / best, "seconds": best}
+        o.close()
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {"value": nf / best, "unit": "quartets/s", "cores": cores, "kind": "port",
-            "sample": "direct_JK over every %d-th of the %d unique shell quartets (%d function quartets, %.2f s); "
-                      "C restatement of the reference (no Fortran compiler here or on the GPU box)"
-                      % (stride, len(items), nf, best)}
+    return {"value": res["timing_build"]["value"], "unit": "quartets/s", "cores": cores, "kind": "port",
+            "sample": "direct_JK over every %d-th of the %d unique shell quartets (%d function quartets); C "
+                      "restatement of the reference (no Fortran compiler here or on the GPU box), timing build: the "
+                      "reference's flags -O3 -ffast-math -funroll-loops -march=native and its pair-vector memo"
+                      % (stride, len(items), nf),
+            "timing_build": res["timing_build"], "parity_build": res["parity_build"]}
 
 
 def nuclear_attraction_stage(eng, sysm):
@@ -113,21 +133,38 @@ def nuclear_attraction_stage(eng, sysm):
                       "host output)"}
 
 
-def scf_iterations(eng, sysm, n_iter=5, V=None):
-    """RHF SCF iteration time (RHF_SAO mirror: host linear algebra + device direct J/K);
+def converged_scf(eng, sysm, V=None):
+    """RHF to convergence (RHF_SAO mirror, thresh 1e-9: host linear algebra +
+    device direct J/K through tce_direct_jk, one CUDA graph per pass) with the
+    learned grid and with the fixed 32-node rule, each energy against the
+    oracle's converged energy with the same quadrature (tests/golden/
+    scf_h_chain64.json: the reference's 128-point table, and its 32-node rule);
     V from the device when given."""
     from william_ci_b200 import scf
+    from william_ci_b200.engine import TCE_METHOD_FIXED, TCE_METHOD_LEARNED
     z = np.load(ONEE_FIXTURE)
+    ref = json.load(open(os.path.join(GOLD, "scf_h_chain64.json")))
     S_, T_, V_ = (scf.fill_with_symmetry(z[k], sysm.nfuc, sysm.ncell) for k in ("S", "T", "V"))
     if V is not None:
         V_ = V
-    r = scf.rhf_sao(S_, T_, V_, float(z["enuc"]), scf.n_occupied(sysm), sysm.nfuc, sysm.ncell, eng.direct_JK,
-                    max_scf=n_iter)
-    it = r.iter_seconds[1:] if len(r.iter_seconds) > 1 else r.iter_seconds
-    jk = r.jk_seconds[1:] if len(r.jk_seconds) > 1 else r.jk_seconds
-    return {"iter_ms": 1e3 * float(np.mean(it)), "jk_ms": 1e3 * float(np.mean(jk)), "iterations_timed": len(it),
-            "energy_after": r.energy, "host": "numpy (SAO transforms, per-k eigh, DIIS)",
-            "note": "64-cell H chain, half-filled band: timing of SCF iterations, not a converged energy"}, r
+    args = (S_, T_, V_, float(z["enuc"]), scf.n_occupied(sysm), sysm.nfuc, sysm.ncell)
+    out, res = {}, None
+    for key, method, truth in (("learned_grid", TCE_METHOD_LEARNED, "table_128"),
+                               ("fixed_32_node_rule", TCE_METHOD_FIXED, "fast_quad_32")):
+        eng.set_method(method)
+        r = scf.rhf_sao(*args, eng.direct_JK)
+        it = r.iter_seconds[1:] if len(r.iter_seconds) > 1 else r.iter_seconds
+        jk = r.jk_seconds[1:] if len(r.jk_seconds) > 1 else r.jk_seconds
+        out[key] = {"energy": r.energy, "converged": bool(r.converged), "iterations": r.iterations,
+                    "iter_ms": 1e3 * float(np.mean(it)), "jk_ms": 1e3 * float(np.mean(jk)),
+                    "oracle_energy": ref[truth]["energy"], "abs_diff_vs_oracle": abs(r.energy - ref[truth]["energy"]),
+                    "oracle_quadrature": truth}
+        if method == TCE_METHOD_LEARNED:
+            res = r
+    eng.set_method(TCE_METHOD_LEARNED)
+    out["oracle_32_vs_128_energy_diff"] = abs(ref["fast_quad_32"]["energy"] - ref["table_128"]["energy"])
+    out["host"] = "numpy (SAO transforms, per-k eigh, DIIS)"
+    return out, res
 
 
 def ao_to_kmo_stage(eng, r):
@@ -211,13 +248,14 @@ def reference_arm(args, sysm):
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
-    o = pyoracle.Oracle(sysm)
+    pyoracle.build_fast(force=True)          # -march=native: compiled for this host
+    o = pyoracle.Oracle(sysm, fast=True)
     items = o.items()
     stride = 8
     sample = items[::stride]
     P = density(sysm.nbas)
-    for _ in range(args.warmup):
-        o.direct_jk_items(sample[:max(1, len(sample) // 8)], P)
+    for w in range(args.warmup):             # the first warm-up pass fills the pair-vector memo
+        o.direct_jk_items(sample if w == 0 else sample[:max(1, len(sample) // 8)], P)
     tot, nf_tot = 0.0, 0
     for _ in range(args.steps):
         t0 = time.perf_counter()
@@ -234,7 +272,8 @@ def reference_arm(args, sysm):
             "cpu_baseline": {"value": v, "unit": "quartets/s", "cores": cores, "kind": "port",
                              "sample": "direct_JK over every %d-th of %d unique shell quartets per step; C restatement "
                                        "of the reference's OpenMP path (the Fortran reference cannot be compiled: no "
-                                       "Fortran compiler)" % (stride, len(items))},
+                                       "Fortran compiler), built with the reference's flags (-O3 -ffast-math "
+                                       "-funroll-loops -march=native) and its pair-vector memo" % (stride, len(items))},
             "e2e": {"value": v, "unit": "quartets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -289,17 +328,73 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # learned-grid set-up (untimed): labels on a sample, network trained on the GPU
 # ---------------------------------------------------------------------------
-def learned_grid_setup(eng, sysm, n_train=16000, seed=2026):
+def heldout(name):
+    """Held-out quartets of a workload and the oracle's blocks of them with the
+    reference's 128-point table (tests/golden/heldout_<name>.npz)."""
+    z = np.load(os.path.join(GOLD, "heldout_%s.npz" % name))
+    return z["items"], z["blocks"], z["offsets"]
+
+
+def item_lookup(items, queries):
+    """Positions of the query quartets in the engine's item list."""
+    key = lambda a: ((a[:, 0].astype(np.int64) * 4096 + a[:, 1]) * 4096 + a[:, 2]) * 4096 + a[:, 3]
+    ki = key(items)
+    order = np.argsort(ki)
+    pos = order[np.searchsorted(ki[order], key(queries))]
+    assert np.array_equal(items[pos], queries)
+    return pos
+
+
+def training_sample(items, held, n, seed=2026):
+    """n quartets drawn from the engine's list, none of them held out."""
+    rng = np.random.default_rng(seed)
+    cand = rng.choice(len(items), min(len(items), n + len(held) + 100), replace=False)
+    hs = {tuple(q) for q in held}
+    keep = [i for i in cand if tuple(items[i]) not in hs][:n]
+    return items[np.array(keep)]
+
+
+def pass_error(eng, items, rules, T, offs):
+    """Largest difference from the truth blocks T of what a learned-grid pass
+    computes for the given quartets: the rule's block where the judge accepts
+    it, the plain method's block where the rule is plain or rejected."""
+    from william_ci_b200 import learned_grid as LG
+    worst, n_rej = 0.0, 0
+    plain_idx = []
+    for r in np.unique(rules):
+        m = np.nonzero(rules == r)[0]
+        if r >= eng.nrules:
+            plain_idx.extend(m.tolist())
+            continue
+        K, G, o2 = eng.rule_blocks(int(r), items[m], judge=True)
+        keep = LG.judge_estimate(K, G, o2) <= LG.JUDGE_TOL
+        plain_idx.extend(m[~keep].tolist())
+        n_rej += int((~keep).sum())
+        for j in np.nonzero(keep)[0]:
+            i = m[j]
+            worst = max(worst, float(np.abs(K[o2[j]:o2[j + 1]] - T[offs[i]:offs[i + 1]]).max(initial=0.0)))
+    if plain_idx:
+        m = np.array(sorted(plain_idx))
+        K, _, o2 = eng.rule_blocks(-2, items[m])
+        for j, i in enumerate(m):
+            worst = max(worst, float(np.abs(K[o2[j]:o2[j + 1]] - T[offs[i]:offs[i + 1]]).max(initial=0.0)))
+    return worst, n_rej
+
+
+def learned_grid_setup(eng, sysm, name, n_train=16000, seed=2026):
+    """Labels for a training sample (against the 128-node reference rule on the
+    engine itself), the network trained on the GPU, rules predicted for every
+    quartet.  The held-out quartets (committed, every angular class) are not
+    trained on; the blocks the pass computes for them are compared with the
+    oracle's blocks under the reference's own 128-point table."""
     from william_ci_b200 import learned_grid as LG
     t0 = time.perf_counter()
     LG.setup(eng)
-    ref = LG.ReferenceBlocks(sysm)
     items = eng.items()
-    rng = np.random.default_rng(seed)
-    idx = rng.choice(len(items), min(n_train + 2000, len(items)), replace=False)
-    tr, ho = items[idx[:-2000]], items[idx[-2000:]]
+    ho, T, offs = heldout(name)
+    tr = training_sample(items, ho, n_train, seed)
     t1 = time.perf_counter()
-    data = LG.make_labels(eng, ref, tr)
+    data = LG.make_labels(eng, LG.DictionaryReference(eng), tr)
     t2 = time.perf_counter()
     net = LG.RuleNet(eng.nrules, seed=0)
     loss = net.train(data["X"], data["ok"], epochs=80, batch=256, lr=2e-3, seed=0)
@@ -307,36 +402,123 @@ def learned_grid_setup(eng, sysm, n_train=16000, seed=2026):
     eng.lg_predict_rules(net, 10.0)
     rules = eng.lg_item_rules()
     t4 = time.perf_counter()
-    # accuracy on a held-out sample: the blocks the learned-grid pass keeps (judge-accepted
-    # dictionary rules; the rest go to the plain method), the plain method and the
-    # system's 32-node rule, each against the 128-node reference
-    rule_of = {tuple(q): r for q, r in zip(items, rules)}
-    T, _, offs = ref.rule_blocks(-1, ho)
-    seg = np.repeat(np.arange(len(ho)), np.diff(offs))
-    worst_lg = 0.0
-    hr = np.array([rule_of[tuple(q)] for q in ho])
-    for r in np.unique(hr):
-        m = np.nonzero(hr == r)[0]
-        if r == eng.nrules:
-            K, _, o2 = eng.rule_blocks(-2, ho[m])
-            keep = np.ones(len(m), bool)
-        else:
-            K, G, o2 = eng.rule_blocks(int(r), ho[m], judge=True)
-            keep = LG.judge_estimate(K, G, o2) <= LG.JUDGE_TOL
-        for j in np.nonzero(keep)[0]:
-            i = m[j]
-            worst_lg = max(worst_lg, float(np.abs(K[o2[j]:o2[j + 1]] - T[offs[i]:offs[i + 1]]).max(initial=0.0)))
+    hr = rules[item_lookup(items, ho)]
+    worst_lg, n_rej = pass_error(eng, ho, hr, T, offs)
     Pl, _, _ = eng.rule_blocks(-2, ho)
     Fx, _, _ = eng.rule_blocks(-1, ho)
-    ref.close()
     R = eng.nrules
+    # the method without the network: the one dictionary rule that the most
+    # training quartets accept (cheaper rule on ties), judged, rejects to plain
+    okfrac = data["ok"].mean(axis=0)
+    single = int(np.argmax(okfrac - 1e-9 * data["cost"].mean(axis=0)))
     return net, {"labels_s": t2 - t1, "train_s": t3 - t2, "predict_s": t4 - t3, "setup_total_s": t4 - t0,
                  "train_quartets": int(len(tr)), "rules": R, "train_loss": float(loss),
                  "on_learned_grid": int(np.sum(rules < R)), "plain_direct": int(np.sum(rules >= R)),
-                 "max_err_vs_reference": {"learned_grid": worst_lg, "plain": float(np.abs(Pl - T).max()),
-                                          "fixed_32_node_rule": float(np.abs(Fx - T).max()),
-                                          "sample": "%d held-out shell quartets, 128-node mapped Gauss-Legendre "
-                                                    "reference" % len(ho)}}
+                 "heldout_judge_rejects": n_rej,
+                 "max_err_vs_oracle_table128": {
+                     "learned_grid": worst_lg, "plain": float(np.abs(Pl - T).max()),
+                     "fixed_32_node_rule": float(np.abs(Fx - T).max()),
+                     "sample": "%d held-out shell quartets (every angular class), oracle blocks with the reference's "
+                               "128-point table (tests/golden/heldout_%s.npz)" % (len(ho), name)}}, \
+        {"single_rule": single, "single_rule_ok_fraction": float(okfrac[single]), "rules": rules}
+
+
+def function_quartets(Q, first, nsh, items, thr=1e-13):
+    """Function quartets of the given shell quartets that pass the Schwarz
+    screen Q(ij) Q(kl) >= thr (the unit of the metric), counted on the host."""
+    tot = 0
+    sizes = nsh[items]
+    key = ((sizes[:, 0] * 7 + sizes[:, 1]) * 7 + sizes[:, 2]) * 7 + sizes[:, 3]
+    for k in np.unique(key):
+        grp = items[key == k]
+        n = nsh[grp[0]]
+        a = np.arange(n[0]); b = np.arange(n[1]); c = np.arange(n[2]); d = np.arange(n[3])
+        for lo in range(0, len(grp), 20000):
+            g = grp[lo:lo + 20000]
+            fA, fB, fC, fD = (first[g[:, i]] for i in range(4))
+            qb = Q[fA[:, None, None] + a[None, :, None], fB[:, None, None] + b[None, None, :]]
+            qk = Q[fC[:, None, None] + c[None, :, None], fD[:, None, None] + d[None, None, :]]
+            tot += int(np.count_nonzero(qb.reshape(len(g), -1, 1) * qk.reshape(len(g), 1, -1) >= thr))
+    return tot
+
+
+def named_shape_stage(name, flush, steps=5):
+    """One of the 2D / 3D workloads at its named shape (the whole supercell in
+    the handle): set-up, the learned grid trained on it, the held-out errors
+    against the 128-table oracle, and the J/K pass timed on one cost-balanced
+    shard of its quartet list with the learned grid, the fixed 32-node rule
+    and the plain method (CUDA events on the handle's stream, L2 flushed
+    between timed passes, one CUDA graph per pass)."""
+    import torch
+    from william_ci_b200.engine import TCE_METHOD_FIXED, TCE_METHOD_LEARNED, TCE_METHOD_PLAIN, Engine
+    from william_ci_b200.system import AOSystem
+    cfg = NAMED[name]
+    sysm = AOSystem.load(os.path.join(GOLD, "systems", name + ".npz"))
+    t0 = time.perf_counter()
+    eng = Engine(sysm)
+    create_s = time.perf_counter() - t0
+    info = eng.info()
+    _, lg, _ = learned_grid_setup(eng, sysm, name, n_train=cfg["train"])
+    eng.set_shard(0, cfg["shard"])
+    sh = eng.shard_items()
+    Q = eng.schwarz()
+    first = np.array([f for f, _ in eng.shells()])
+    nsh = np.array([n for _, n in eng.shells()])
+    nfq = function_quartets(Q, first, nsh, sh)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    n, nf = sysm.nbas, sysm.nfuc
+    P = density(n)
+    dP = torch.from_numpy(P.ravel(order="F").copy()).to(dev)
+    dJ = torch.zeros(nf * n, dtype=torch.float64, device=dev)
+    dK = torch.zeros(nf * n, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    eng.set_graph(True)
+
+    def timed(method, nsteps, warm):
+        eng.set_method(method)
+        for _ in range(warm):
+            eng.direct_JK_device(dP.data_ptr(), dJ.data_ptr(), dK.data_ptr(), stream.cuda_stream)
+            torch.cuda.synchronize()
+        tot = 0.0
+        for i in range(nsteps):
+            flush.fill_(float(i))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            eng.direct_JK_device(dP.data_ptr(), dJ.data_ptr(), dK.data_ptr(), stream.cuda_stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            tot += e0.elapsed_time(e1)
+        return tot / nsteps
+
+    lg_ms = timed(TCE_METHOD_LEARNED, steps, 2)
+    flops, nprim = eng.lg_work()
+    fixed_ms = timed(TCE_METHOD_FIXED, steps, 1)
+    plain_ms = timed(TCE_METHOD_PLAIN, 1, 1)
+    eng.close()
+    peak = _fp64_peak()
+    return {"workload": cfg["workload"], "nbas": sysm.nbas, "create_s": create_s,
+            "shell_quartets": info["n_shell_quartets"], "function_quartets": info["n_func_quartets"],
+            "device_bytes": info["device_bytes"],
+            "timed_shard": {"of": cfg["shard"], "shell_quartets": int(len(sh)), "function_quartets": nfq,
+                            "plan": "cost-balanced shard 0 of %d (tce_set_shard)" % cfg["shard"]},
+            "learned_grid": {"value": nfq / (lg_ms * 1e-3), "unit": "quartets/s", "ms_per_pass": lg_ms},
+            "fixed_rule": {"value": nfq / (fixed_ms * 1e-3), "ms_per_pass": fixed_ms},
+            "plain": {"value": nfq / (plain_ms * 1e-3), "ms_per_pass": plain_ms},
+            "lg_over_plain": plain_ms / lg_ms,
+            "roofline": {"bound": "fp64", "achieved": flops / (lg_ms * 1e-3) / 1e12, "peak": peak,
+                         "unit": "TFLOP/s", "frac": flops / (lg_ms * 1e-3) / 1e12 / peak,
+                         "algorithmic_flops_per_pass": flops, "primitive_quartets": nprim},
+            "setup": lg}
+
+
+_PEAK = []
+
+
+def _fp64_peak():
+    from william_ci_b200.engine import fp64_peak_tflops
+    if not _PEAK:
+        _PEAK.append(fp64_peak_tflops())
+    return _PEAK[0]
 
 
 def timed_passes(eng, step, steps, flush, stream, world, dist):
@@ -369,8 +551,7 @@ def main():
 
     import torch
     import torch.distributed as dist
-    from william_ci_b200.engine import (TCE_METHOD_FIXED, TCE_METHOD_LEARNED, TCE_METHOD_PLAIN, Engine,
-                                        fp64_peak_tflops)
+    from william_ci_b200.engine import TCE_METHOD_FIXED, TCE_METHOD_LEARNED, TCE_METHOD_PLAIN, Engine
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -382,7 +563,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
 
     eng = Engine(sysm)
-    net, lg_info = learned_grid_setup(eng, sysm)
+    net, lg_info, lg_extra = learned_grid_setup(eng, sysm, WORKLOAD)
     if world > 1:
         eng.set_shard(rank, world)
     info = eng.info()
@@ -394,18 +575,24 @@ def main():
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
 
-    def step():
-        eng.direct_JK_device(dP.data_ptr(), dJ.data_ptr(), dK.data_ptr(), stream.cuda_stream)
-        if world > 1:
-            dist.all_reduce(dJ)
-            dist.all_reduce(dK)
+    def step_on(e):
+        def step():
+            e.direct_JK_device(dP.data_ptr(), dJ.data_ptr(), dK.data_ptr(), stream.cuda_stream)
+            if world > 1:
+                dist.all_reduce(dJ)
+                dist.all_reduce(dK)
+        return step
 
-    def run(method, steps, warmup):
-        eng.set_method(method)
+    step = step_on(eng)
+
+    def run(method, steps, warmup, e=None):
+        e = eng if e is None else e
+        st_ = step_on(e)
+        e.set_method(method)
         for _ in range(warmup):      # synchronised: one-time list changes (rejects moved) finish here
-            step()
+            st_()
             torch.cuda.synchronize()
-        tot, kern = timed_passes(eng, step, steps, flush, stream, world, dist)
+        tot, kern = timed_passes(e, st_, steps, flush, stream, world, dist)
         t = torch.tensor([tot, kern], dtype=torch.float64, device=dev)
         if world > 1:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -448,6 +635,8 @@ def main():
     # kernels of one learned-grid pass: one per work list (kernel class, rule size,
     # FP32 panels), the plain list on the side stream, the judge's fallback launch
     launches_per_step = eng.pass_kernels()
+    # each work list's kernel alone: time and algorithmic work, for per-kernel fractions
+    per_list = eng.lg_list_profile(3) if world == 1 else None
     # comparison arms on the same device: the plain adaptive method and the system's 32-node rule
     plain_steps = max(2, min(args.steps, 3))
     plain_ms, _ = run(TCE_METHOD_PLAIN, plain_steps, 1)
@@ -455,34 +644,63 @@ def main():
     eng.set_fp32_threshold(0.0)
     lg64_ms, _ = run(TCE_METHOD_LEARNED, args.steps, args.warmup)
     eng.set_fp32_threshold(FP32_THRESHOLD)
+    # the reference's own higher-accuracy setting (nquad_128: the 40-node mapped rule)
+    ho, T_ho, offs_ho = heldout(WORKLOAD)
+    eng40 = Engine(sysm, nquad=40)
+    if world > 1:
+        eng40.set_shard(rank, world)
+    eng40.set_graph(True)
+    r40_ms, _ = run(TCE_METHOD_FIXED, args.steps, args.warmup, e=eng40)
+    B40, _, _ = eng40.rule_blocks(-1, ho)
+    err40 = float(np.abs(B40 - T_ho).max())
+    eng40.close()
+    # the method without the network: one dictionary rule for every quartet, judged
+    net_rules = eng.lg_item_rules()
+    single = lg_extra["single_rule"]
+    eng.lg_set_item_rules(np.full(len(net_rules), single, dtype=np.int32))
+    single_ms, _ = run(TCE_METHOD_LEARNED, args.steps, args.warmup)
+    single_err, single_rej = pass_error(eng, ho, np.full(len(ho), single), T_ho, offs_ho)
+    single_plain = eng.lg_stats()["plain_direct"]
+    eng.lg_set_item_rules(net_rules)
     eng.set_method(TCE_METHOD_LEARNED)
+    for _ in range(2):               # back to the network's rules (their rejects already routed)
+        step()
+        torch.cuda.synchronize()
 
-    # ---- end to end through the public API: pinned host P in, J/K out, every step
+    # ---- end to end through the public API: pinned host P in, J/K out, every step;
+    # L2 flushed before each step (outside the timed call), as for the device timing
     Pp = torch.from_numpy(Ph.ravel(order="F").copy()).pin_memory()
     Jp = torch.zeros(n * n, dtype=torch.float64).pin_memory()
     Kp = torch.zeros(n * n, dtype=torch.float64).pin_memory()
     e2e_steps = max(3, args.steps // 2)
+    e2e_s = 0.0
     if world == 1:
         eng.direct_JK_ptrs(Pp.data_ptr(), Jp.data_ptr(), Kp.data_ptr())     # warm
-        t0 = time.perf_counter()
-        for _ in range(e2e_steps):
+        for i in range(e2e_steps):
+            flush.fill_(float(i))
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
             eng.direct_JK_ptrs(Pp.data_ptr(), Jp.data_ptr(), Kp.data_ptr())
-        e2e_s = (time.perf_counter() - t0) / e2e_steps
+            e2e_s += time.perf_counter() - t0
+        e2e_s /= e2e_steps
     else:
-        dist.barrier()
-        t0 = time.perf_counter()
-        for _ in range(e2e_steps):
+        for i in range(e2e_steps):
+            flush.fill_(float(i))
+            torch.cuda.synchronize()
+            dist.barrier()
+            t0 = time.perf_counter()
             dP.copy_(Pp, non_blocking=True)
             step()
             Jp[: nf * n].copy_(dJ, non_blocking=True)
             Kp[: nf * n].copy_(dK, non_blocking=True)
             torch.cuda.synchronize()
-        e2e_s = (time.perf_counter() - t0) / e2e_steps
+            e2e_s += time.perf_counter() - t0
+        e2e_s /= e2e_steps
         te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
         e2e_s = float(te[0])
     e2e = {"value": nq_total / e2e_s, "unit": "quartets/s", "h2d_bytes_per_step": 8 * n * n,
-           "d2h_bytes_per_step": 2 * 8 * nf * n, "ms_per_step": 1e3 * e2e_s,
+           "d2h_bytes_per_step": 2 * 8 * nf * n, "ms_per_step": 1e3 * e2e_s, "l2": "flushed before each step",
            "api": "tce_direct_jk, learned grid (host buffers, pinned)" if world == 1 else
                   "tce_direct_jk_device + NCCL all-reduce + pinned copies"}
 
@@ -492,7 +710,7 @@ def main():
             dist.destroy_process_group()
         return
 
-    peak = fp64_peak_tflops()
+    peak = _fp64_peak()
     lg_flops, lg_nprim = eng.lg_work() if world == 1 else (None, None)
     achieved = lg_flops / (lg_kern * 1e-3) / 1e12 if world == 1 else None
     traffic = None
@@ -501,6 +719,16 @@ def main():
             traffic = json.load(open(PROFILE_TRAFFIC)).get("dram_bytes_per_pass")
         except Exception:
             traffic = None
+    kernels = None
+    if per_list:
+        names = {0: "k_quartets<%d>", 1: "k_quartets_s%s<%d>", 2: "k_quartets_r1%s<%d>"}
+        kernels = []
+        for w in per_list:
+            nm = names[w["kind"]] % ((w["nq"],) if w["kind"] == 0 else ("_tc" if w["tc"] else "", w["nq"]))
+            kernels.append({"kernel": nm + (" fp32" if w["fp32"] else ""), "cls": w["cls"], "quartets": w["n"],
+                            "ms": w["ms"], "flops": w["flops"],
+                            "tflops": w["flops"] / (w["ms"] * 1e-3) / 1e12 if w["ms"] > 0 else None,
+                            "frac": w["flops"] / (w["ms"] * 1e-3) / 1e12 / peak if w["ms"] > 0 else None})
     roofline = {"bound": "fp64", "kernel": "the learned-grid J/K pass, one CUDA graph: k_quartets<32|64>, "
                                            "k_quartets_s[_tc], k_quartets_r1[_tc] (per-quartet rule, judge, fused "
                                            "J/K scatter) and the plain launches",
@@ -508,7 +736,9 @@ def main():
                 "frac": (achieved / peak) if (achieved and peak) else None, "traffic": traffic,
                 "peak_source": "measured FP64 FMA throughput of this GPU (tce_fp64_peak probe); MEASURED_PEAKS.json "
                                "holds no FP64 figure",
-                "algorithmic_flops_per_launch": lg_flops, "primitive_quartets": lg_nprim, "pass_ms": lg_kern}
+                "algorithmic_flops_per_launch": lg_flops, "primitive_quartets": lg_nprim, "pass_ms": lg_kern,
+                "per_list": kernels}
+    lg_err = lg_info["max_err_vs_oracle_table128"]
     line = {"metric": METRIC, "value": value, "unit": "quartets/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded exponents/coefficients)",
@@ -521,9 +751,19 @@ def main():
                                     "function_quartets": nq_total}),
             "plain": {"value": nq_total / (plain_ms * 1e-3), "ms_per_step": plain_ms, "steps": plain_steps,
                       "method": "device adaptive Gauss-Kronrod bisection (15/7 panels, Bessel columns per panel)"},
-            "lg_over_plain": plain_ms / ms_step,
             "fixed_rule": {"value": nq_total / (fixed_ms * 1e-3), "ms_per_step": fixed_ms,
-                           "method": "the reference's 32-node mapped Gauss-Legendre rule on the same engine"},
+                           "max_err_vs_oracle_table128": lg_err["fixed_32_node_rule"],
+                           "method": "the reference's default 32-node mapped Gauss-Legendre rule on the same engine"},
+            "rule_40_node": {"value": nq_total / (r40_ms * 1e-3), "ms_per_step": r40_ms,
+                             "max_err_vs_oracle_table128": err40,
+                             "method": "the reference's nquad_128 setting: 40-node mapped Gauss-Legendre rule, same "
+                                       "engine"},
+            "single_rule_judged": {"value": nq_total / (single_ms * 1e-3), "ms_per_step": single_ms,
+                                   "max_err_vs_oracle_table128": single_err, "rule": single,
+                                   "train_accept_fraction": lg_extra["single_rule_ok_fraction"],
+                                   "plain_list": single_plain, "heldout_judge_rejects": single_rej,
+                                   "method": "the method without the network: the one dictionary rule most training "
+                                             "quartets accept, for every quartet, judge and plain fallback"},
             "learned_grid_fp64_only": {"value": nq_total / (lg64_ms * 1e-3), "ms_per_step": lg64_ms},
             "fp32_panels": fp32,
             "cuda_graph": "each J/K pass replayed as one CUDA graph (tce_set_graph)",
@@ -533,11 +773,35 @@ def main():
             "e2e": e2e, "roofline": roofline, "clocks": clk, "gpu_launches": args.steps * launches_per_step}
     if world == 1:
         Vdev, line["nuclear_attraction"] = nuclear_attraction_stage(eng, sysm)
-        line["rhf_scf"], r_scf = scf_iterations(eng, sysm, V=Vdev)
+        line["rhf_scf"], r_scf = converged_scf(eng, sysm, V=Vdev)
         line["ao_to_kmo"] = ao_to_kmo_stage(eng, r_scf)
+        eng.close()
         line["dfmp2"] = dfmp2_timing()
+        line["named_shapes"] = {nm: named_shape_stage(nm, flush) for nm in NAMED}
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(sysm, stride=1)
+    # the north-star figures last, so that a reader of the end of the line has them
+    summary = {"lg_over_plain": plain_ms / ms_step,
+               "lg_over_rule_40_node": r40_ms / ms_step, "lg_over_single_rule_judged": single_ms / ms_step,
+               "max_err_vs_oracle_table128": {"learned_grid": lg_err["learned_grid"], "rule_40_node": err40,
+                                              "single_rule_judged": single_err,
+                                              "fixed_32_node_rule": lg_err["fixed_32_node_rule"],
+                                              "plain": lg_err["plain"]},
+               "pass_ms": {"learned_grid": ms_step, "rule_40_node": r40_ms, "single_rule_judged": single_ms,
+                           "fixed_32_node_rule": fixed_ms, "plain": plain_ms}}
+    if "rhf_scf" in line:
+        summary["rhf_energy_abs_diff_vs_oracle"] = {k: line["rhf_scf"][k]["abs_diff_vs_oracle"]
+                                                    for k in ("learned_grid", "fixed_32_node_rule")}
+    if "named_shapes" in line:
+        summary["named_shapes"] = {k: {"lg_quartets_per_s": v["learned_grid"]["value"],
+                                       "lg_over_plain": v["lg_over_plain"],
+                                       "lg_max_err_vs_oracle_table128":
+                                           v["setup"]["max_err_vs_oracle_table128"]["learned_grid"],
+                                       "roofline_frac": v["roofline"]["frac"]}
+                                   for k, v in line["named_shapes"].items()}
+    if "cpu_baseline" in line:
+        summary["cpu_baseline_timing_build"] = line["cpu_baseline"]["value"]
+    line["summary"] = summary
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

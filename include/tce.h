@@ -210,6 +210,14 @@ int tce_lg_autotune(void *handle, int32_t reps, int32_t *ntuned, int32_t *nswitc
  * counterpart. */
 int tce_lg_lists(void *handle, int32_t *n, int32_t *info);
 
+/* Per-list measurement of the learned-grid pass: each work list (in the order
+ * and kernel form tce_lg_lists reports) launched alone reps times on the
+ * handle's stream, ms[i] the fastest launch (CUDA events), flops[i] its
+ * algorithmic FP64 operations (counted as tce_lg_work).  With ms or flops
+ * NULL only *n (the number of lists) is set.  Uses the handle's host-entry
+ * J/K buffers as scratch.  No reference counterpart. */
+int tce_lg_list_profile(void *handle, int32_t reps, int32_t *n, double *ms, double *flops);
+
 /* Nuclear attraction matrix of the handle's system (replaces
  * nuclear_attraction_matrix_toroidal_{1,2,3}D, 1D_Nuclear_attraction_toroidal.f90
  * :169-276 / 3D_Nuclear_attraction_toroidal.f90:113-196, with the per-pair

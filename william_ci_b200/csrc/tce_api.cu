@@ -8,6 +8,8 @@
 // data.
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <cstdlib>
 #include <cmath>
 #include <mutex>
 #include <queue>
@@ -204,8 +206,23 @@ int run_blocks(Handle *h, const std::vector<int4> &items, const std::vector<int>
     return TCE_OK;
 }
 
+// Wall time of the phases of build() on stderr when TCE_TIMING is set (the
+// device phases are synchronised where the phase ends anyway).
+struct PhaseClock {
+    bool on = std::getenv("TCE_TIMING") != nullptr;
+    std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+    void mark(const char *what)
+    {
+        if (!on) return;
+        auto n = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "tce_create %-28s %8.3f s\n", what, std::chrono::duration<double>(n - t).count());
+        t = n;
+    }
+};
+
 int build(Handle *h, const tce_system *sys)
 {
+    PhaseClock clk;
     // ---------------- validate + copy ----------------
     if (!sys) return fail(h, TCE_ERR_ARG, "sys is NULL");
     if (sys->ndp < 1 || sys->ndp > 3) return fail(h, TCE_ERR_ARG, "ndp must be 1, 2 or 3");
@@ -359,6 +376,7 @@ int build(Handle *h, const tce_system *sys)
     }
     if ((s = dalloc(h, &h->d_next, 1))) return s;
 
+    clk.mark("setup (host shells, device)");
     // ---------------- t-tables (setup_t_tables) ----------------
     {
         double *tb, *Tt;
@@ -387,6 +405,7 @@ int build(Handle *h, const tce_system *sys)
         if ((s = upload(h, &h->d_gmax, gm))) return s;
     }
 
+    clk.mark("t-tables");
     // ---------------- unit pairs + primitive-pair scalars ----------------
     const int nreal = 3 - h->ndp;
     long long npp_tot = 0, e_tot = 0;
@@ -464,6 +483,7 @@ int build(Handle *h, const tce_system *sys)
         return TCE_OK;
     }
 
+    clk.mark("unit pairs");
     // ---------------- Schwarz: diagonal blocks, SI in the unit cell (ERI_toroidal.f90:200-236) ----------
     {
         std::vector<int4> items;
@@ -505,6 +525,7 @@ int build(Handle *h, const tce_system *sys)
             if (h->Qsh[U.S1 + (size_t)h->nsh * U.S2] * h->Qmax >= h->thr) ++h->n_unit_sig;
     }
 
+    clk.mark("Schwarz");
     // ---------------- primitive Schwarz table (ERI_toroidal.f90:296-337) ----------------
     if (h->prim_screen) {
         std::vector<int4> items;
@@ -519,6 +540,7 @@ int build(Handle *h, const tce_system *sys)
         if ((s = run_blocks(h, items, &sel, TCE_MODE_PRIMTAB, 0, nullptr, nullptr))) return s;
     }
 
+    clk.mark("primitive table");
     // ---------------- unique quartets (ERI_toroidal.f90:342-401) ----------------
     {
         unsigned long long *d_cnt = nullptr;
@@ -540,6 +562,7 @@ int build(Handle *h, const tce_system *sys)
         CK(h, cudaStreamSynchronize(h->st));
         dfree(h, d_raw);
         dfree(h, d_cnt);
+    clk.mark("enumeration");
         // order: most expensive first (dynamic scheduling, LPT); cost ~ pairs x rows x vector length
         std::vector<double> cost(items.size());
         for (size_t i = 0; i < items.size(); ++i) {
@@ -569,12 +592,14 @@ int build(Handle *h, const tce_system *sys)
             sorted[i] = items[ord[i]];
             h->cost_host[i] = cost[ord[i]];
         }
+    clk.mark("cost + sort");
         if ((s = upload(h, &h->d_items, sorted))) return s;
         h->items_host = std::move(sorted);
         h->shard_idx.resize(h->items_host.size());
         std::iota(h->shard_idx.begin(), h->shard_idx.end(), 0LL);
         if ((s = make_lists(h, h->items_host))) return s;
         if ((s = lg_rebuild_lists(h))) return s;
+    clk.mark("work lists");
         // algorithmic work of one J/K pass
         unsigned long long *d_np = nullptr;
         double *d_fl = nullptr;
@@ -591,6 +616,7 @@ int build(Handle *h, const tce_system *sys)
         dfree(h, d_np);
         dfree(h, d_fl);
     }
+    clk.mark("work count");
     if ((s = dalloc(h, &h->d_P, (size_t)nbas * nbas))) return s;
     if ((s = dalloc(h, &h->d_J, (size_t)h->nfuc * nbas))) return s;
     if ((s = dalloc(h, &h->d_K, (size_t)h->nfuc * nbas))) return s;

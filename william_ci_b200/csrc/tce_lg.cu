@@ -1369,6 +1369,70 @@ int tce_lg_autotune(void *handle, int32_t reps, int32_t *ntuned, int32_t *nswitc
     return TCE_OK;
 }
 
+int tce_lg_list_profile(void *handle, int32_t reps, int32_t *n, double *ms, double *flops)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !n) return fail(h, TCE_ERR_ARG, "NULL argument");
+    if (!ms || !flops) {
+        *n = (int32_t)h->lg_lists.size();
+        return TCE_OK;
+    }
+    if (*n < (int32_t)h->lg_lists.size()) return fail(h, TCE_ERR_ARG, "arrays hold fewer lists than the handle has");
+    if (!h->d_rules || h->lg_lists.empty()) return fail(h, TCE_ERR_STATE, "no learned-grid lists");
+    if (!h->d_P || !h->d_J || !h->d_K) return fail(h, TCE_ERR_STATE, "handle without J/K buffers");
+    if (reps < 1) reps = 1;
+    int s;
+    if ((s = ensure_plain(h))) return s;
+    QuartetHostArgs a;
+    fill_common(h, a);
+    a.mode = TCE_MODE_JK;
+    a.prim_screen = h->prim_screen;
+    a.P = h->d_P;
+    a.J = h->d_J;
+    a.K = h->d_K;
+    CK(h, cudaMemsetAsync(h->d_P, 0, sizeof(double) * (size_t)h->nbas * h->nbas, h->st));
+    unsigned long long *d_np = nullptr;
+    double *d_fl = nullptr;
+    if ((s = dalloc(h, &d_np, 1))) return s;
+    if ((s = dalloc(h, &d_fl, 1))) return s;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(h, cudaEventCreate(&e0));
+    CK(h, cudaEventCreate(&e1));
+    s = TCE_OK;
+    for (size_t i = 0; i < h->lg_lists.size() && s == TCE_OK; ++i) {
+        auto &w = h->lg_lists[i];
+        double best = 1e300;
+        for (int r = 0; r < reps && s == TCE_OK; ++r) {
+            cudaMemsetAsync(h->d_fb_count, 0, sizeof(unsigned int), h->st);
+            cudaEventRecord(e0, h->st);
+            s = lg_launch_list(h, w, a, h->d_P, h->d_J, h->d_K, lg_tc(h, w), h->st);
+            cudaEventRecord(e1, h->st);
+            if (s == TCE_OK && cudaEventSynchronize(e1) != cudaSuccess) s = TCE_ERR_CUDA;
+            float t = 0.f;
+            if (s == TCE_OK) cudaEventElapsedTime(&t, e0, e1);
+            best = std::min(best, (double)t);
+        }
+        if (s != TCE_OK) break;
+        cudaMemsetAsync(d_np, 0, sizeof(unsigned long long), h->st);
+        cudaMemsetAsync(d_fl, 0, sizeof(double), h->st);
+        s = tce_launch_count_work(h->S, w.d, (int)w.n, h->prim_screen, h->d_tnmax, d_np, d_fl, h->st, w.rule,
+                                  h->d_rules, h->d_rule_tnmax);
+        if (s == TCE_OK && cudaMemcpyAsync(flops + i, d_fl, sizeof(double), cudaMemcpyDeviceToHost, h->st) != cudaSuccess)
+            s = TCE_ERR_CUDA;
+        if (s == TCE_OK && cudaStreamSynchronize(h->st) != cudaSuccess) s = TCE_ERR_CUDA;
+        ms[i] = best;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    dfree(h, d_np);
+    dfree(h, d_fl);
+    if (s != TCE_OK) return fail(h, s, "list profile launch failed");
+    CK(h, cudaMemsetAsync(h->d_fb_count, 0, sizeof(unsigned int), h->st));
+    CK(h, cudaStreamSynchronize(h->st));
+    *n = (int32_t)h->lg_lists.size();
+    return TCE_OK;
+}
+
 int tce_lg_item_rules(void *handle, int32_t *rule)
 {
     Handle *h = static_cast<Handle *>(handle);

@@ -45,7 +45,7 @@ EXPORTS = ["tce_create", "tce_destroy", "tce_last_error", "tce_get_info", "tce_s
            "tce_set_fp32_threshold", "tce_dfmp2_energy", "tce_mp2_last_error", "tce_create_blocks",
            "tce_pass_kernels", "tce_set_tensor_cores", "tce_nuclear_attraction", "tce_quad_self_check_nuc",
            "tce_lg_autotune", "tce_lg_lists", "tce_dfjk_create", "tce_dfjk", "tce_dfjk_destroy",
-           "tce_dfjk_last_error", "tce_ao_to_kmo", "tce_shard_items"]
+           "tce_dfjk_last_error", "tce_ao_to_kmo", "tce_shard_items", "tce_lg_list_profile"]
 
 TCE_METHOD_FIXED, TCE_METHOD_LEARNED, TCE_METHOD_PLAIN = 0, 1, 2
 TCE_NFEAT = 12
@@ -137,6 +137,7 @@ def lib():
         L.tce_nuclear_attraction.argtypes = [C.c_void_p, C.c_int32, _dp, _ip, _dp]
         L.tce_lg_autotune.argtypes = [C.c_void_p, C.c_int32, _ip, _ip, _dp]
         L.tce_lg_lists.argtypes = [C.c_void_p, _ip, _ip]
+        L.tce_lg_list_profile.argtypes = [C.c_void_p, C.c_int32, _ip, _dp, _dp]
         L.tce_ao_to_kmo.argtypes = [C.c_void_p, _dp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _dp]
         L.tce_dfjk_create.argtypes = [C.c_int32, C.c_int32, C.c_int32, _ip, _dp, _dp, C.POINTER(C.c_void_p)]
         L.tce_dfjk.argtypes = [C.c_void_p, _dp, _dp, _dp]
@@ -419,6 +420,19 @@ class Engine:
         _check(lib().tce_lg_lists(self.h, C.byref(n), _i(info)), self.h)
         keys = ("kind", "cls", "nq", "fp32", "tc", "n")
         return [dict(zip(keys, (int(x) for x in info[6 * i:6 * i + 6]))) for i in range(n.value)]
+
+    def lg_list_profile(self, reps: int = 3) -> list:
+        """Each learned-grid list launched alone (tce_lg_list_profile): the lists
+        of lg_lists() with their fastest time (ms) and algorithmic FP64 operations."""
+        n = C.c_int32(0)
+        _check(lib().tce_lg_list_profile(self.h, int(reps), C.byref(n), None, None), self.h)
+        ms = np.zeros(max(n.value, 1))
+        fl = np.zeros(max(n.value, 1))
+        _check(lib().tce_lg_list_profile(self.h, int(reps), C.byref(n), _d(ms), _d(fl)), self.h)
+        out = self.lg_lists()
+        for i, w in enumerate(out[:n.value]):
+            w["ms"], w["flops"] = float(ms[i]), float(fl[i])
+        return out[:n.value]
 
     def set_tensor_cores(self, on: bool = True):
         """FP64 tensor-core node sums where a kernel has them (tce_set_tensor_cores)."""

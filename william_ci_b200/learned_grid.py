@@ -76,6 +76,34 @@ class ReferenceBlocks:
             e.close()
 
 
+class DictionaryReference:
+    """The same label reference on the engine itself: the 128-node rule is
+    loaded as a two-rule dictionary (its two halves of 64 nodes), both halves'
+    blocks are summed, and the rule dictionary is loaded back.  No second
+    handle is built, which matters for large systems (the 8x8 sheet's handle
+    takes tens of seconds and gigabytes to build).  Per-item rules keep their
+    indices: the dictionary put back is the same."""
+
+    def __init__(self, engine: Engine):
+        self.eng = engine
+
+    def rule_blocks(self, rule, items, mode=1, judge=False):
+        assert rule == -1
+        t, w = reference_rule()
+        z = np.zeros(64)
+        self.eng.lg_set_rules([(t[:64], w[:64], z), (t[64:], w[64:], z)])
+        try:
+            K0, _, offs = self.eng.rule_blocks(0, items, mode=mode)
+            K1, _, _ = self.eng.rule_blocks(1, items, mode=mode)
+        finally:
+            rules, _ = dictionary()
+            self.eng.lg_set_rules(rules)
+        return K0 + K1, None, offs
+
+    def close(self):
+        pass
+
+
 def setup(engine: Engine, net: Optional["RuleNet"] = None):
     """Load the dictionary and the plain rule into an engine; predict rules with `net`."""
     rules, _ = dictionary()
