@@ -139,7 +139,8 @@ def converged_scf(eng, sysm, V=None):
     learned grid and with the fixed 32-node rule, each energy against the
     oracle's converged energy with the same quadrature (tests/golden/
     scf_h_chain64.json: the reference's 128-point table, and its 32-node rule);
-    V from the device when given."""
+    V of the 32-node rule from the device when given, V of the learned-grid
+    SCF from a 128-node handle."""
     from william_ci_b200 import scf
     from william_ci_b200.engine import TCE_METHOD_FIXED, TCE_METHOD_LEARNED
     z = np.load(ONEE_FIXTURE)
@@ -147,10 +148,18 @@ def converged_scf(eng, sysm, V=None):
     S_, T_, V_ = (scf.fill_with_symmetry(z[k], sysm.nfuc, sysm.ncell) for k in ("S", "T", "V"))
     if V is not None:
         V_ = V
-    args = (S_, T_, V_, float(z["enuc"]), scf.n_occupied(sysm), sysm.nfuc, sysm.ncell)
+    # the nuclear attraction integrals use the t-quadrature too: the learned-grid
+    # SCF takes V from a handle with the 128-node reference rule, as the oracle's
+    # 128-table SCF takes it from that table
+    from william_ci_b200 import learned_grid as LG
+    from william_ci_b200.engine import Engine
+    t128, w128 = LG.reference_rule()
+    with Engine(sysm, t_nodes=t128, t_weights=w128) as e128:
+        V128 = e128.nuclear_attraction()
     out, res = {}, None
-    for key, method, truth in (("learned_grid", TCE_METHOD_LEARNED, "table_128"),
-                               ("fixed_32_node_rule", TCE_METHOD_FIXED, "fast_quad_32")):
+    for key, method, truth, Vm in (("learned_grid", TCE_METHOD_LEARNED, "table_128", V128),
+                                   ("fixed_32_node_rule", TCE_METHOD_FIXED, "fast_quad_32", V_)):
+        args = (S_, T_, Vm, float(z["enuc"]), scf.n_occupied(sysm), sysm.nfuc, sysm.ncell)
         eng.set_method(method)
         r = scf.rhf_sao(*args, eng.direct_JK)
         it = r.iter_seconds[1:] if len(r.iter_seconds) > 1 else r.iter_seconds

@@ -371,6 +371,17 @@ int build(Handle *h, const tce_system *sys)
         if ((s = upload(h, &q, h->sh_coef))) return s; S.sh_coef = q;
         if ((s = upload(h, &q, h->sh_cmax))) return s; S.sh_cmax = q;
         if ((s = upload(h, &p, h->lxyz))) return s; S.fn_pw = p;
+        {
+            std::vector<int4> fc((size_t)nbas);
+            for (int f = 0; f < nbas; ++f) {
+                const int c = f / h->nfuc;
+                fc[(size_t)f] = make_int4(c % h->ncl[0], (c / h->ncl[0]) % h->ncl[1], c / (h->ncl[0] * h->ncl[1]),
+                                          f - c * h->nfuc);
+            }
+            int4 *d_fc = nullptr;
+            if ((s = upload(h, &d_fc, fc))) return s;
+            S.fn_cell = d_fc;
+        }
         if ((s = upload(h, &q, h->tnode))) return s; S.tnode = q;
         if ((s = upload(h, &q, h->tweight))) return s; S.tweight = q;
     }
@@ -557,43 +568,31 @@ int build(Handle *h, const tce_system *sys)
         if ((s = dalloc(h, &d_raw, (size_t)h->nitems))) return s;
         CK(h, cudaMemsetAsync(d_cnt, 0, 2 * sizeof(unsigned long long), h->st));
         CKS(h, tce_launch_enumerate(S, h->d_Qsh, h->Qmax, d_raw, d_cnt, (unsigned long long)h->nitems, d_cnt + 1, h->st));
-        std::vector<int4> items((size_t)h->nitems);
-        CK(h, cudaMemcpyAsync(items.data(), d_raw, items.size() * sizeof(int4), cudaMemcpyDeviceToHost, h->st));
+    clk.mark("enumeration");
+        // work order on the device (tce_sort_items): most expensive first, ties by
+        // the quartet, so that the enumeration's arbitrary order never leaks
+        // into the list every rank of a sharded run must share
+        double *d_cost = nullptr;
+        int *d_mnc = nullptr;
+        if ((s = dalloc(h, &h->d_items, (size_t)h->nitems))) return s;
+        if ((s = dalloc(h, &d_cost, (size_t)h->nitems))) return s;
+        if ((s = dalloc(h, &d_mnc, 1))) return s;
+        CK(h, cudaMemsetAsync(d_mnc, 0, sizeof(int), h->st));
+        CKS(h, tce_sort_items(S, d_raw, h->nitems, h->d_items, d_cost, d_mnc, h->st));
+        std::vector<int4> sorted((size_t)h->nitems);
+        h->cost_host.resize((size_t)h->nitems);
+        int mnc = 1;
+        CK(h, cudaMemcpyAsync(sorted.data(), h->d_items, sorted.size() * sizeof(int4), cudaMemcpyDeviceToHost, h->st));
+        CK(h, cudaMemcpyAsync(h->cost_host.data(), d_cost, h->cost_host.size() * sizeof(double),
+                              cudaMemcpyDeviceToHost, h->st));
+        CK(h, cudaMemcpyAsync(&mnc, d_mnc, sizeof(int), cudaMemcpyDeviceToHost, h->st));
         CK(h, cudaStreamSynchronize(h->st));
+        h->max_ncomb = std::max(h->max_ncomb, mnc);
         dfree(h, d_raw);
         dfree(h, d_cnt);
-    clk.mark("enumeration");
-        // order: most expensive first (dynamic scheduling, LPT); cost ~ pairs x rows x vector length
-        std::vector<double> cost(items.size());
-        for (size_t i = 0; i < items.size(); ++i) {
-            const int4 &q = items[i];
-            int cK = q.z / h->nshuc, SK0 = q.z % h->nshuc, SLp = shift_to(h, q.w, cK, h->nshuc);
-            const UnitPair &Ub = h->up[(size_t)q.x * h->nsh + q.y];
-            const UnitPair &Uk = h->up[(size_t)SK0 * h->nsh + SLp];
-            int nc = ncomb_of(h, q.x, q.y, q.z, q.w);
-            h->max_ncomb = std::max(h->max_ncomb, nc);
-            cost[i] = (double)Ub.npp * Uk.npp * nc * h->ndp * std::min(Ub.Nlen, Uk.Nlen);
-        }
-        std::vector<size_t> ord(items.size());
-        std::iota(ord.begin(), ord.end(), 0);
-        // ties broken by the quartet itself: the enumeration kernel emits items in
-        // no fixed order, and every rank of a sharded run must see the same list
-        std::sort(ord.begin(), ord.end(), [&](size_t x, size_t y) {
-            if (cost[x] != cost[y]) return cost[x] > cost[y];
-            const int4 &a = items[x], &b = items[y];
-            if (a.x != b.x) return a.x < b.x;
-            if (a.y != b.y) return a.y < b.y;
-            if (a.z != b.z) return a.z < b.z;
-            return a.w < b.w;
-        });
-        std::vector<int4> sorted(items.size());
-        h->cost_host.resize(items.size());
-        for (size_t i = 0; i < ord.size(); ++i) {
-            sorted[i] = items[ord[i]];
-            h->cost_host[i] = cost[ord[i]];
-        }
+        dfree(h, d_cost);
+        dfree(h, d_mnc);
     clk.mark("cost + sort");
-        if ((s = upload(h, &h->d_items, sorted))) return s;
         h->items_host = std::move(sorted);
         h->shard_idx.resize(h->items_host.size());
         std::iota(h->shard_idx.begin(), h->shard_idx.end(), 0LL);

@@ -58,6 +58,7 @@ struct DevSys {
     const double *sh_coef;    // [sh_coff + comp*np + p]
     const double *sh_cmax;    // [sh_eoff + p]
     const int *fn_pw;         // [3*nbas]
+    const int4 *fn_cell;      // [nbas]: cell coordinates (x, y, z) and index in the unit cell
     // pairs
     const UnitPair *up;
     const PairPrim *pp;
@@ -222,6 +223,18 @@ __device__ __forceinline__ int tce_shift_to(int idx, int refcell, int nblk, cons
     return (cx + ncl[0] * (cy + ncl[1] * cz)) * nblk + loc;
 }
 
+// tce_shift_to for functions, without integer division: the function's cell
+// coordinates come from the table fn_cell, the reference cell's are given.
+__device__ __forceinline__ int tce_shift_fn(const DevSys &S, int f, int rx, int ry, int rz)
+{
+    const int4 c = __ldg(S.fn_cell + f);
+    int cx = c.x - rx, cy = c.y - ry, cz = c.z - rz;
+    cx += cx < 0 ? S.ncl[0] : 0;
+    cy += cy < 0 ? S.ncl[1] : 0;
+    cz += cz < 0 ? S.ncl[2] : 0;
+    return (cx + S.ncl[0] * (cy + S.ncl[1] * cz)) * S.nfuc + c.w;
+}
+
 // J/K contributions of one function quartet f = (i,j|k,l) of the block of
 // shell quartet (fI..|..), every stored element (p1 in the unit cell) once:
 // J(p1,p2) += E P(p3,p4), K(p1,p4) += -1/2 E P(p2,p3) (eri_direct.f90:331-357).
@@ -238,9 +251,9 @@ __device__ __forceinline__ void tce_scatter_jk(const DevSys &S, const double *__
         int t[4];
 #pragma unroll
         for (int ii = 0; ii < 4; ++ii) t[ii] = f[perm[ip][ii]];
-        int ref = t[0] / S.nfuc;
+        const int4 rc = __ldg(S.fn_cell + t[0]);
 #pragma unroll
-        for (int ii = 0; ii < 4; ++ii) img[ip][ii] = tce_shift_to(t[ii], ref, S.nfuc, S.ncl);
+        for (int ii = 0; ii < 4; ++ii) img[ip][ii] = tce_shift_fn(S, t[ii], rc.x, rc.y, rc.z);
         const int *g = img[ip];
         bool inblk = g[0] >= fI && g[0] < fI + nA && g[1] >= fJ && g[1] < fJ + nB && g[2] >= fK && g[2] < fK + nC &&
                      g[3] >= fL && g[3] < fL + nD;

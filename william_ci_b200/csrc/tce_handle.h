@@ -104,7 +104,6 @@ struct Handle {
     int fb_pending = 0;
     long long fb_version = -1;           // work_version of the pass the copy came from
     int route_rejects = 1;
-    std::vector<long long> item_order;   // items_host indices in quartet order (lookup)
     double judge_tol = 1e-10, plain_tol = 1e-11;
     int plain_max_panels = 24;
     double plain_scale = 0.6;

@@ -514,3 +514,88 @@ int tce_launch_sym_fill(int nf, int fpuc, const int *ncl, double *eri, cudaStrea
     k_sym_fill<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(nf, fpuc, ncl[0], ncl[1], ncl[2], eri);
     return cudaGetLastError() == cudaSuccess ? TCE_OK : TCE_ERR_CUDA;
 }
+
+// ---------------------------------------------------------------------------
+// Work order of the unique quartets: most expensive first (dynamic scheduling
+// takes the dear quartets first, longest-processing-time order), ties by the
+// quartet (x, y, z, w) so that every rank of a sharded run sees the same list.
+// Cost ~ primitive pairs x power combinations x periodic directions x the
+// shorter pair-vector length.  Two stable radix sorts on the device: by the
+// packed quartet, then by the complemented cost.
+// ---------------------------------------------------------------------------
+#include <thrust/execution_policy.h>
+#include <thrust/gather.h>
+#include <thrust/sequence.h>
+#include <thrust/sort.h>
+
+__global__ void k_item_cost(DevSys S, const int4 *__restrict__ items, long long n, unsigned long long *ck,
+                            unsigned long long *qk, double *cost, int *max_ncomb)
+{
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int nc = 0;
+    if (i < n) {
+        const int4 q = items[i];
+        const int cK = q.z / S.nshuc, SK0 = q.z - cK * S.nshuc;
+        const int SLp = tce_shift_to(q.w, cK, S.nshuc, S.ncl);
+        const UnitPair &Ub = S.up[(long long)q.x * S.nsh + q.y];
+        const UnitPair &Uk = S.up[(long long)SK0 * S.nsh + SLp];
+        nc = (S.sh_l[q.x] + 1) * (S.sh_l[q.y] + 1) * (S.sh_l[q.z] + 1) * (S.sh_l[q.w] + 1);
+        const double c = (double)Ub.npp * Uk.npp * nc * S.ndp * (Ub.Nlen < Uk.Nlen ? Ub.Nlen : Uk.Nlen);
+        cost[i] = c;
+        ck[i] = ~(unsigned long long)c;
+        const unsigned long long ns = (unsigned long long)S.nsh;
+        qk[i] = (((unsigned long long)q.x * ns + (unsigned long long)q.y) * ns + (unsigned long long)q.z) * ns +
+                (unsigned long long)q.w;
+    }
+    for (int o = 16; o > 0; o >>= 1) nc = max(nc, __shfl_xor_sync(0xffffffffu, nc, o));
+    if ((threadIdx.x & 31) == 0 && nc > 0) atomicMax(max_ncomb, nc);
+}
+
+__global__ void k_gather_items(const int4 *__restrict__ in, const double *__restrict__ cin,
+                               const long long *__restrict__ idx, long long n, int4 *out, double *cout)
+{
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const long long j = idx[i];
+        out[i] = in[j];
+        cout[i] = cin[j];
+    }
+}
+
+int tce_sort_items(const DevSys &S, const int4 *items, long long n, int4 *sorted, double *cost_sorted,
+                   int *d_max_ncomb, cudaStream_t st)
+{
+    if (n <= 0) return TCE_OK;
+    unsigned long long *ck = nullptr, *qk = nullptr;
+    double *cost = nullptr;
+    long long *idx = nullptr;
+    cudaError_t e = cudaMalloc(&ck, sizeof(unsigned long long) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&qk, sizeof(unsigned long long) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&cost, sizeof(double) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&idx, sizeof(long long) * n);
+    int rc = TCE_OK;
+    if (e != cudaSuccess) {
+        rc = TCE_ERR_NOMEM;
+    } else {
+        const unsigned blocks = (unsigned)((n + 255) / 256);
+        k_item_cost<<<blocks, 256, 0, st>>>(S, items, n, ck, qk, cost, d_max_ncomb);
+        try {
+            auto pol = thrust::cuda::par.on(st);
+            thrust::sequence(pol, idx, idx + n);
+            thrust::stable_sort_by_key(pol, qk, qk + n, idx);
+            thrust::gather(pol, idx, idx + n, ck, qk);            // qk now holds the cost keys in quartet order
+            thrust::stable_sort_by_key(pol, qk, qk + n, idx);
+        } catch (...) {
+            rc = TCE_ERR_CUDA;
+        }
+        if (rc == TCE_OK) {
+            k_gather_items<<<blocks, 256, 0, st>>>(items, cost, idx, n, sorted, cost_sorted);
+            if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) rc = TCE_ERR_CUDA;
+        }
+    }
+    cudaFree(ck);
+    cudaFree(qk);
+    cudaFree(cost);
+    cudaFree(idx);
+    return rc;
+}

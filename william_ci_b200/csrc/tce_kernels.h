@@ -108,6 +108,11 @@ int tce_launch_enumerate(const DevSys &S, const double *Qsh, double Qmax, int4 *
 int tce_launch_stored_jk(int n1, int nbas, int physicist, const double *P, const double *eri, double *J, double *K,
                          cudaStream_t st);
 int tce_launch_sym_fill(int nf, int fpuc, const int *ncl, double *eri, cudaStream_t st);
+// Unique quartets in work order (most expensive first, ties by the quartet),
+// with their costs; *d_max_ncomb (device) raised to the largest power-combination
+// count among them.
+int tce_sort_items(const DevSys &S, const int4 *items, long long n, int4 *sorted, double *cost_sorted,
+                   int *d_max_ncomb, cudaStream_t st);
 int tce_launch_count_work(const DevSys &S, const int4 *items, int nitems, int prim_screen, const int *tnmax,
                           unsigned long long *nprim, double *flops, cudaStream_t st, const int *item_rule = nullptr,
                           const RuleDev *rules = nullptr, const int *rule_tnmax = nullptr);

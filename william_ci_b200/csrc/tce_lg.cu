@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <unordered_set>
 #include <random>
 
 #include "tce_handle.h"
@@ -458,26 +459,29 @@ int lg_rebuild_lists(Handle *h)
             pl.push_back(q);
         }
     }
+    // rank of each rule in list order: more nodes first, then the rule index
+    std::vector<int> by_rank(h->lg_nrules), rank_of(h->lg_nrules);
+    std::iota(by_rank.begin(), by_rank.end(), 0);
+    std::stable_sort(by_rank.begin(), by_rank.end(),
+                     [&](int x, int y) { return h->rules_host[x].nn > h->rules_host[y].nn; });
+    for (int i = 0; i < h->lg_nrules; ++i) rank_of[by_rank[i]] = i;
     for (int key = 0; key < 3 * 16 * 4; ++key) {
         if (lg[key].empty()) continue;
         // quartets of one rule next to each other, so that the warps working at
         // the same time on an SM read the same T table (L1 reuse); rules with
         // more nodes first, each rule's quartets in the original (dearest
-        // first) order
+        // first) order: a counting sort over the rules' ranks
         {
-            std::vector<size_t> ord(lg[key].size());
-            std::iota(ord.begin(), ord.end(), 0);
             const std::vector<int> &rk = rl[key];
-            std::stable_sort(ord.begin(), ord.end(), [&](size_t x, size_t y) {
-                const int nx = h->rules_host[rk[x]].nn, ny = h->rules_host[rk[y]].nn;
-                if (nx != ny) return nx > ny;
-                return rk[x] < rk[y];
-            });
-            std::vector<int4> li(ord.size());
-            std::vector<int> lr(ord.size());
-            for (size_t i = 0; i < ord.size(); ++i) {
-                li[i] = lg[key][ord[i]];
-                lr[i] = rk[ord[i]];
+            std::vector<long long> cnt((size_t)h->lg_nrules + 1, 0);
+            for (int r : rk) ++cnt[(size_t)rank_of[(size_t)r] + 1];
+            for (size_t i = 1; i < cnt.size(); ++i) cnt[i] += cnt[i - 1];
+            std::vector<int4> li(rk.size());
+            std::vector<int> lr(rk.size());
+            for (size_t i = 0; i < rk.size(); ++i) {
+                const long long at = cnt[(size_t)rank_of[(size_t)rk[i]]]++;
+                li[(size_t)at] = lg[key][i];
+                lr[(size_t)at] = rk[i];
             }
             lg[key].swap(li);
             rl[key].swap(lr);
@@ -589,18 +593,6 @@ int lg_read_rejects(Handle *h, cudaStream_t st)
     return TCE_OK;
 }
 
-static bool quartet_less(const int4 &a, const int4 &b)
-{
-    if (a.x != b.x) return a.x < b.x;
-    if (a.y != b.y) return a.y < b.y;
-    if (a.z != b.z) return a.z < b.z;
-    return a.w < b.w;
-}
-
-// Before a learned-grid pass: if the last pass has finished (its copy is in)
-// and its work lists are still the current ones, its rejects get the plain
-// method (item rule = lg_nrules) and the lists are rebuilt.  Up to fb_cap
-// rejects are moved; with more, the judge's fallback keeps them.
 int lg_absorb_rejects(Handle *h)
 {
     if (!h->fb_pending) return TCE_OK;
@@ -611,23 +603,19 @@ int lg_absorb_rejects(Handle *h)
     const unsigned int n = h->h_fb[0];
     if (n == 0 || n > (unsigned int)h->fb_cap || h->fb_version != h->work_version) return TCE_OK;
     if (h->item_rule.size() != h->items_host.size()) return TCE_OK;
-    if (h->item_order.size() != h->items_host.size()) {
-        h->item_order.resize(h->items_host.size());
-        std::iota(h->item_order.begin(), h->item_order.end(), 0LL);
-        std::sort(h->item_order.begin(), h->item_order.end(), [&](long long x, long long y) {
-            return quartet_less(h->items_host[(size_t)x], h->items_host[(size_t)y]);
-        });
-    }
+    // the rejects came from this shard's pass: look them up among its items
+    const unsigned long long ns = (unsigned long long)h->nsh;
+    auto key = [ns](const int4 &q) {
+        return (((unsigned long long)q.x * ns + (unsigned long long)q.y) * ns + (unsigned long long)q.z) * ns +
+               (unsigned long long)q.w;
+    };
     const int4 *rej = reinterpret_cast<const int4 *>(h->h_fb + 4);
+    std::unordered_set<unsigned long long> want;
+    for (unsigned int i = 0; i < n; ++i) want.insert(key(rej[i]));
     long long moved = 0;
-    for (unsigned int i = 0; i < n; ++i) {
-        auto it = std::lower_bound(h->item_order.begin(), h->item_order.end(), rej[i], [&](long long x, const int4 &v) {
-            return quartet_less(h->items_host[(size_t)x], v);
-        });
-        if (it == h->item_order.end()) continue;
-        const int4 &f = h->items_host[(size_t)*it];
-        if (f.x != rej[i].x || f.y != rej[i].y || f.z != rej[i].z || f.w != rej[i].w) continue;
-        int &r = h->item_rule[(size_t)*it];
+    for (long long i : h->shard_idx) {
+        if (!want.count(key(h->items_host[(size_t)i]))) continue;
+        int &r = h->item_rule[(size_t)i];
         if (r >= 0 && r < h->lg_nrules) {
             r = h->lg_nrules;
             ++moved;

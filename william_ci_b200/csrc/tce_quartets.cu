@@ -75,67 +75,69 @@ __device__ __forceinline__ double ldT(const double *p)
     return *p;
 }
 
+// One row I_r(t_k) = sgn sum_n F_n T[n][k] of the nodes of one chunk: the
+// 8-node groups g0 .. g0 + 3 (32 nodes, fewer at the end of the rule), out[x]
+// for node 8 g0 + x.
 template <int NQ, bool RO>
 __device__ __forceinline__ void row_dot(const RuleView &R, int d, const double2 *__restrict__ G, int nppb, int ib_,
                                         const double2 *__restrict__ H, int nppk, int ik_, int nm, double phi,
-                                        double sgn, double *out)
+                                        double sgn, int g0, double *out)
 {
     constexpr int NG = NQ / 8;
     const double *T = R.T + (size_t)d * R.strideD;
     const int *gm = R.gmax + d * TCE_MAXG;
     double c1, s1;
     sincos(phi, &s1, &c1);
+    double acc[32];
 #pragma unroll
-    for (int g0 = 0; g0 < NG; g0 += 4) {
-        double acc[32];
+    for (int x = 0; x < 32; ++x) acc[x] = 0.0;
+    double cn = 1.0, sn = 0.0;
+    int n = 0;
 #pragma unroll
-        for (int x = 0; x < 32; ++x) acc[x] = 0.0;
-        double cn = 1.0, sn = 0.0;
-        int n = 0;
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            if (g0 + s >= NG) break;
-            int nend = gm[g0 + s];
-            nend = nend < nm ? nend : nm;
-            for (; n <= nend; ++n) {
-                if (n > 0) {
-                    if ((n & 31) == 0) {
-                        sincos((double)n * phi, &sn, &cn);
-                    } else {
-                        double tmp = cn * c1 - sn * s1;
-                        sn = sn * c1 + cn * s1;
-                        cn = tmp;
-                    }
+    for (int s = 0; s < 4; ++s) {
+        if (g0 + s >= NG) break;
+        int nend = gm[g0 + s];
+        nend = nend < nm ? nend : nm;
+        for (; n <= nend; ++n) {
+            if (n > 0) {
+                if ((n & 31) == 0) {
+                    sincos((double)n * phi, &sn, &cn);
+                } else {
+                    double tmp = cn * c1 - sn * s1;
+                    sn = sn * c1 + cn * s1;
+                    cn = tmp;
                 }
-                double2 g = __ldg(G + (size_t)n * nppb + ib_);
-                double2 h = __ldg(H + (size_t)n * nppk + ik_);
-                double ar = g.x * h.x - g.y * h.y, ai = g.x * h.y + g.y * h.x;
-                double F = ar * cn - ai * sn;
-                const double *Tn = T + (size_t)n * NQ + 8 * g0;
+            }
+            double2 g = __ldg(G + (size_t)n * nppb + ib_);
+            double2 h = __ldg(H + (size_t)n * nppk + ik_);
+            double ar = g.x * h.x - g.y * h.y, ai = g.x * h.y + g.y * h.x;
+            double F = ar * cn - ai * sn;
+            const double *Tn = T + (size_t)n * NQ + 8 * g0;
 #pragma unroll
-                for (int g = 0; g < 4; ++g) {
-                    if (g >= s && g0 + g < NG) {
+            for (int g = 0; g < 4; ++g) {
+                if (g >= s && g0 + g < NG) {
 #pragma unroll
-                        for (int kk = 0; kk < 8; ++kk)
-                            acc[8 * g + kk] = fma(F, ldT<RO>(Tn + 8 * g + kk), acc[8 * g + kk]);
-                    }
+                    for (int kk = 0; kk < 8; ++kk)
+                        acc[8 * g + kk] = fma(F, ldT<RO>(Tn + 8 * g + kk), acc[8 * g + kk]);
                 }
             }
         }
-#pragma unroll
-        for (int x = 0; x < 32; ++x)
-            if (8 * g0 + x < NQ) out[8 * g0 + x] = acc[x] * sgn;
     }
+#pragma unroll
+    for (int x = 0; x < 32; ++x)
+        if (8 * g0 + x < NQ) out[x] = acc[x] * sgn;
 }
 
 struct QCtx {
     int SI, SJ, SK, SL, nA, nB, nC, nD, lsA, lsB, lsC, lsD, ncomb, ncq, NN, R;
+    int cqg;   // lanes per component in the component contraction (power of two)
     UnitPair Ub, Uk;
     double Tsh[3];
 };
 
 // per-warp shared memory: [qlist rowcap int2][qfac rowcap][rows rowcap*RS]
-// [real nreal*cstride*RS][blkK blkcap][blkG blkcap][extra]
+// [real nreal*cstride*RS][blkK blkcap][blkG blkcap][extra]; RS = 33 (rows of a
+// chunk of 32 nodes plus padding), 17 for the plain method's 16-node panels
 struct WarpBuf {
     int2 *qlist;
     double *qfac, *rows, *realb, *blkK, *blkG, *extra;
@@ -169,11 +171,13 @@ __device__ __forceinline__ void tce_dmma(double &d0, double &d1, double a, doubl
 // A fragments of rows 8 m + l/4 (m = 0..3) at order 4 s + l%4, cos and sin
 // of n phi by the three-term recurrence in steps of four (re-seeded every 32
 // orders), and loads the next step's G, H and T before the current step's
-// mma instructions.  Output as row_dot: rows[r * (NQ + 1) + k] = sgn I_r(t_k).
+// mma instructions.  Nodes of one chunk (8-node groups g0c .. g0c + 3); output
+// as row_dot: rows[r * 33 + x] = sgn I_r(t_{8 g0c + x}).
 template <int NQ>
-__device__ void tc_rows(const DevSys &S, const RuleView &Rv, const QCtx &Q, int nb, const WarpBuf &b, int lane)
+__device__ void tc_rows(const DevSys &S, const RuleView &Rv, const QCtx &Q, int nb, const WarpBuf &b, int lane,
+                        int g0c)
 {
-    constexpr int RS = NQ + 1;
+    constexpr int RS = 32 + 1;
     const int rq = lane >> 2, cq = lane & 3;
     const int lsA = Q.lsA, lsB = Q.lsB, lsC = Q.lsC, lsD = Q.lsD, R = Q.R;
     const int nppb = Q.Ub.npp, nppk = Q.Uk.npp;
@@ -214,8 +218,8 @@ __device__ void tc_rows(const DevSys &S, const RuleView &Rv, const QCtx &Q, int 
             return S.a[0] * (S.pp[Q.Ub.pp_off + pq.x].cen[0] - (S.pp[Q.Uk.pp_off + pq.y].cen[0] + Q.Tsh[0]));
         };
         const double2 *Gv = S.vec + Q.Ub.vec_off, *Hv = S.vec + Q.Uk.vec_off;
-#pragma unroll 1
-        for (int g0 = 0; g0 < NQ / 8; g0 += 4) {
+        {
+            const int g0 = g0c;
             int gmb[4], nend = -1;
 #pragma unroll
             for (int t = 0; t < 4; ++t) {
@@ -290,7 +294,7 @@ __device__ void tc_rows(const DevSys &S, const RuleView &Rv, const QCtx &Q, int 
 #pragma unroll
                 for (int t = 0; t < 4; ++t)
 #pragma unroll
-                    for (int i = 0; i < 2; ++i) b.rows[(size_t)r * RS + 8 * (g0 + t) + 2 * cq + i] = acc[8 * m + 2 * t + i] * sg[m];
+                    for (int i = 0; i < 2; ++i) b.rows[(size_t)r * RS + 8 * t + 2 * cq + i] = acc[8 * m + 2 * t + i] * sg[m];
             }
         }
     }
@@ -301,118 +305,141 @@ template <int NQ, bool RO>
 __device__ void process_batch(const DevSys &S, const RuleView &Rv, const QCtx &Q, int nb, const WarpBuf &b, int lane,
                               int cstride, bool tc)
 {
-    constexpr int RS = NQ + 1;
+    // The rule's nodes in chunks of NC (32): the rows of one chunk, then its
+    // share of every component's node sum.  The row dots restart their order
+    // loop per 32 nodes anyway, so chunking costs no extra arithmetic and the
+    // per-warp row buffer holds 32 nodes instead of NQ (more warps per SM).
+    constexpr int NC = NQ < 32 ? NQ : 32;
+    constexpr int RS = NC + 1;
     const int ndp = S.ndp, nreal = 3 - ndp;
     const int lsA = Q.lsA, lsB = Q.lsB, lsC = Q.lsC, lsD = Q.lsD, ncomb = Q.ncomb, R = Q.R;
     const int nppb = Q.Ub.npp, nppk = Q.Uk.npp;
     const int nrows = nb * R;
-    bool rows_done = false;
-    // tensor-core rows when the launch asks for them (32- and 64-node rules)
-    if constexpr (RO && (NQ == 32 || NQ == 64)) {
-        if (tc && ndp == 1) {
-            tc_rows<NQ>(S, Rv, Q, nb, b, lane);
-            rows_done = true;
-        }
-    }
-    for (int r = lane; r < (rows_done ? 0 : nrows); r += 32) {
-        int p = r / R, rem = r - p * R;
-        int d = rem / ncomb, cmb = rem - d * ncomb;
-        int ia = cmb % (lsA + 1), t1 = cmb / (lsA + 1);
-        int ib = t1 % (lsB + 1), t2 = t1 / (lsB + 1);
-        int ic = t2 % (lsC + 1), id = t2 / (lsC + 1);
-        int2 pq = b.qlist[p];
-        const PairPrim &Pb = S.pp[Q.Ub.pp_off + pq.x];
-        const PairPrim &Pk = S.pp[Q.Uk.pp_off + pq.y];
-        const double2 *G = S.vec + Q.Ub.vec_off +
-                           ((((long long)d * (lsA + 1) + ia) * (lsB + 1) + ib) * 2 + 0) * (long long)Q.Ub.Nlen * nppb;
-        const double2 *H = S.vec + Q.Uk.vec_off +
-                           ((((long long)d * (lsC + 1) + ic) * (lsD + 1) + id) * 2 + 1) * (long long)Q.Uk.Nlen * nppk;
-        int nm = Pb.N[d] < Pk.N[d] ? Pb.N[d] : Pk.N[d];
-        double phi = S.a[d] * (Pb.cen[d] - (Pk.cen[d] + Q.Tsh[d]));
-        double sgn = pow(S.a[d], -(double)(ia + ib + ic + id));
-        row_dot<NQ, RO>(Rv, d, G, nppb, pq.x, H, nppk, pq.y, nm, phi, sgn, b.rows + (size_t)r * RS);
-    }
-    __syncwarp();
     const int npA = S.sh_np[Q.SI], npB = S.sh_np[Q.SJ], npC = S.sh_np[Q.SK], npD = S.sh_np[Q.SL];
     const bool judge = Rv.wg != nullptr;
-    for (int p = 0; p < nb; ++p) {
-        int2 pq = b.qlist[p];
-        const PairPrim &Pb = S.pp[Q.Ub.pp_off + pq.x];
-        const PairPrim &Pk = S.pp[Q.Uk.pp_off + pq.y];
-        const double pp_ = Pb.esum, qq = Pk.esum;
-        if (nreal > 0) {
-            const double *Eb = S.ecoef + Q.Ub.e_off + (long long)pq.x * nreal * (lsA + 1) * (lsB + 1) * TCE_ECO;
-            const double *Ek = S.ecoef + Q.Uk.e_off + (long long)pq.y * nreal * (lsC + 1) * (lsD + 1) * TCE_ECO;
-            for (int k = lane; k < NQ; k += 32) {
-                double t = Rv.t[k], t2 = t * t;
-                double D2 = 1.0 / (pp_ * qq + (pp_ + qq) * t2);
-                double w = pp_ * qq * t2 * D2, rs = PI_D * sqrt(D2);
-                for (int dr = 0; dr < nreal; ++dr) {
-                    int d = ndp + dr;
-                    double Rr = Pb.cen[d] - (Pk.cen[d] + Q.Tsh[d]);
-                    double gt[4 * TCE_LMAX + 2];
-                    gt[0] = (Rr == 0.0) ? rs : rs * exp(-w * Rr * Rr);
-                    double gm1 = 0.0, g0 = gt[0];
-                    for (int n = 0; n < Q.NN; ++n) {
-                        double gp1 = 2.0 * w * Rr * g0 - 2.0 * (double)n * w * gm1;
-                        gt[n + 1] = gp1;
-                        gm1 = g0;
-                        g0 = gp1;
-                    }
-                    for (int cmb = 0; cmb < ncomb; ++cmb) {
-                        int ia = cmb % (lsA + 1), u1 = cmb / (lsA + 1);
-                        int ib = u1 % (lsB + 1), u2 = u1 / (lsB + 1);
-                        int ic = u2 % (lsC + 1), id = u2 / (lsC + 1);
-                        const double *eb = Eb + ((dr * (lsA + 1) + ia) * (lsB + 1) + ib) * TCE_ECO;
-                        const double *ek = Ek + ((dr * (lsC + 1) + ic) * (lsD + 1) + id) * TCE_ECO;
-                        double val = 0.0;
-                        for (int n = 0; n <= ia + ib; ++n) {
-                            double sb = (n & 1) ? -eb[n] : eb[n];
-                            for (int kk = 0; kk <= ic + id; ++kk) val += sb * ek[kk] * gt[n + kk];
+#pragma unroll 1
+    for (int k0 = 0; k0 < NQ; k0 += NC) {
+        const int g0c = k0 / 8, kn = NQ - k0 < NC ? NQ - k0 : NC;
+        bool rows_done = false;
+        // tensor-core rows when the launch asks for them (32- and 64-node rules)
+        if constexpr (RO && (NQ == 32 || NQ == 64)) {
+            if (tc && ndp == 1) {
+                tc_rows<NQ>(S, Rv, Q, nb, b, lane, g0c);
+                rows_done = true;
+            }
+        }
+        for (int r = lane; r < (rows_done ? 0 : nrows); r += 32) {
+            int p = r / R, rem = r - p * R;
+            int d = rem / ncomb, cmb = rem - d * ncomb;
+            int ia = cmb % (lsA + 1), t1 = cmb / (lsA + 1);
+            int ib = t1 % (lsB + 1), t2 = t1 / (lsB + 1);
+            int ic = t2 % (lsC + 1), id = t2 / (lsC + 1);
+            int2 pq = b.qlist[p];
+            const PairPrim &Pb = S.pp[Q.Ub.pp_off + pq.x];
+            const PairPrim &Pk = S.pp[Q.Uk.pp_off + pq.y];
+            const double2 *G = S.vec + Q.Ub.vec_off +
+                               ((((long long)d * (lsA + 1) + ia) * (lsB + 1) + ib) * 2 + 0) * (long long)Q.Ub.Nlen * nppb;
+            const double2 *H = S.vec + Q.Uk.vec_off +
+                               ((((long long)d * (lsC + 1) + ic) * (lsD + 1) + id) * 2 + 1) * (long long)Q.Uk.Nlen * nppk;
+            int nm = Pb.N[d] < Pk.N[d] ? Pb.N[d] : Pk.N[d];
+            double phi = S.a[d] * (Pb.cen[d] - (Pk.cen[d] + Q.Tsh[d]));
+            double sgn = pow(S.a[d], -(double)(ia + ib + ic + id));
+            row_dot<NQ, RO>(Rv, d, G, nppb, pq.x, H, nppk, pq.y, nm, phi, sgn, g0c, b.rows + (size_t)r * RS);
+        }
+        __syncwarp();
+        for (int p = 0; p < nb; ++p) {
+            int2 pq = b.qlist[p];
+            const PairPrim &Pb = S.pp[Q.Ub.pp_off + pq.x];
+            const PairPrim &Pk = S.pp[Q.Uk.pp_off + pq.y];
+            const double pp_ = Pb.esum, qq = Pk.esum;
+            if (nreal > 0) {
+                const double *Eb = S.ecoef + Q.Ub.e_off + (long long)pq.x * nreal * (lsA + 1) * (lsB + 1) * TCE_ECO;
+                const double *Ek = S.ecoef + Q.Uk.e_off + (long long)pq.y * nreal * (lsC + 1) * (lsD + 1) * TCE_ECO;
+                for (int k = lane; k < kn; k += 32) {
+                    double t = Rv.t[k0 + k], t2 = t * t;
+                    double D2 = 1.0 / (pp_ * qq + (pp_ + qq) * t2);
+                    double w = pp_ * qq * t2 * D2, rs = PI_D * sqrt(D2);
+                    for (int dr = 0; dr < nreal; ++dr) {
+                        int d = ndp + dr;
+                        double Rr = Pb.cen[d] - (Pk.cen[d] + Q.Tsh[d]);
+                        double gt[4 * TCE_LMAX + 2];
+                        gt[0] = (Rr == 0.0) ? rs : rs * exp(-w * Rr * Rr);
+                        double gm1 = 0.0, g0 = gt[0];
+                        for (int n = 0; n < Q.NN; ++n) {
+                            double gp1 = 2.0 * w * Rr * g0 - 2.0 * (double)n * w * gm1;
+                            gt[n + 1] = gp1;
+                            gm1 = g0;
+                            g0 = gp1;
                         }
-                        b.realb[((size_t)dr * cstride + cmb) * RS + k] = val;
+                        for (int cmb = 0; cmb < ncomb; ++cmb) {
+                            int ia = cmb % (lsA + 1), u1 = cmb / (lsA + 1);
+                            int ib = u1 % (lsB + 1), u2 = u1 / (lsB + 1);
+                            int ic = u2 % (lsC + 1), id = u2 / (lsC + 1);
+                            const double *eb = Eb + ((dr * (lsA + 1) + ia) * (lsB + 1) + ib) * TCE_ECO;
+                            const double *ek = Ek + ((dr * (lsC + 1) + ic) * (lsD + 1) + id) * TCE_ECO;
+                            double val = 0.0;
+                            for (int n = 0; n <= ia + ib; ++n) {
+                                double sb = (n & 1) ? -eb[n] : eb[n];
+                                for (int kk = 0; kk <= ic + id; ++kk) val += sb * ek[kk] * gt[n + kk];
+                            }
+                            b.realb[((size_t)dr * cstride + cmb) * RS + k] = val;
+                        }
                     }
+                }
+                __syncwarp();
+            }
+            const double fac = b.qfac[p];
+            const double *rowp = b.rows + (size_t)p * R * RS;
+            const int i = pq.x / Q.Ub.np2, j = pq.x % Q.Ub.np2;
+            const int kp = pq.y / Q.Uk.np2, lp = pq.y % Q.Uk.np2;
+            // The component quartets: sum_k w_k I_x I_y I_z per component.  G lanes
+            // share one component and split its nodes (G = 32 / next power of two of
+            // the component count, at most NQ), so that the warp holds 32 / G
+            // components at once and each needs log2(G) shuffles instead of a full
+            // warp reduction; each component's block entry has one owning lane.
+            const int G = Q.cqg < NC ? Q.cqg : NC;
+            const int slots = 32 / G, slot = lane / G, sub = lane - slot * G;
+            for (int c0 = 0; c0 < Q.ncq; c0 += slots) {
+                const int cq = c0 + slot;
+                double vK = 0.0, vG = 0.0;
+                int ca = 0, cb = 0, cc = 0, cd = 0;
+                if (cq < Q.ncq) {
+                    ca = cq % Q.nA;
+                    const int r1 = cq / Q.nA;
+                    cb = r1 % Q.nB;
+                    const int r2 = r1 / Q.nB;
+                    cc = r2 % Q.nC;
+                    cd = r2 / Q.nC;
+                    const int *pa = S.fn_pw + 3 * (S.sh_first[Q.SI] + ca);
+                    const int *pb = S.fn_pw + 3 * (S.sh_first[Q.SJ] + cb);
+                    const int *pc = S.fn_pw + 3 * (S.sh_first[Q.SK] + cc);
+                    const int *pd = S.fn_pw + 3 * (S.sh_first[Q.SL] + cd);
+                    const double *rw[3];
+    #pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        const int cm = pa[d] + (lsA + 1) * (pb[d] + (lsB + 1) * (pc[d] + (lsC + 1) * pd[d]));
+                        rw[d] = (d < ndp) ? rowp + ((size_t)d * ncomb + cm) * RS
+                                          : b.realb + ((size_t)(d - ndp) * cstride + cm) * RS;
+                    }
+                    for (int k = sub; k < kn; k += G) {
+                        const double prod = rw[0][k] * rw[1][k] * rw[2][k];
+                        vK = fma(Rv.wk[k0 + k], prod, vK);
+                        if (judge) vG = fma(Rv.wg[k0 + k], prod, vG);
+                    }
+                }
+                for (int o = G >> 1; o > 0; o >>= 1) {
+                    vK += __shfl_xor_sync(0xffffffffu, vK, o);
+                    if (judge) vG += __shfl_xor_sync(0xffffffffu, vG, o);
+                }
+                if (cq < Q.ncq && sub == 0) {
+                    const double cf = S.sh_coef[S.sh_coff[Q.SI] + ca * npA + i] * S.sh_coef[S.sh_coff[Q.SJ] + cb * npB + j] *
+                                      S.sh_coef[S.sh_coff[Q.SK] + cc * npC + kp] * S.sh_coef[S.sh_coff[Q.SL] + cd * npD + lp];
+                    b.blkK[cq] += fac * cf * vK;
+                    if (judge) b.blkG[cq] += fac * cf * vG;
                 }
             }
             __syncwarp();
         }
-        const double fac = b.qfac[p];
-        const double *rowp = b.rows + (size_t)p * R * RS;
-        const int i = pq.x / Q.Ub.np2, j = pq.x % Q.Ub.np2;
-        const int kp = pq.y / Q.Uk.np2, lp = pq.y % Q.Uk.np2;
-        for (int cq = 0; cq < Q.ncq; ++cq) {
-            int ca = cq % Q.nA, r1 = cq / Q.nA;
-            int cb = r1 % Q.nB, r2 = r1 / Q.nB;
-            int cc = r2 % Q.nC, cd = r2 / Q.nC;
-            const int *pa = S.fn_pw + 3 * (S.sh_first[Q.SI] + ca);
-            const int *pb = S.fn_pw + 3 * (S.sh_first[Q.SJ] + cb);
-            const int *pc = S.fn_pw + 3 * (S.sh_first[Q.SK] + cc);
-            const int *pd = S.fn_pw + 3 * (S.sh_first[Q.SL] + cd);
-            int cm[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) cm[d] = pa[d] + (lsA + 1) * (pb[d] + (lsB + 1) * (pc[d] + (lsC + 1) * pd[d]));
-            double vK = 0.0, vG = 0.0;
-            for (int k = lane; k < NQ; k += 32) {
-                double prod = 1.0;
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    double x = (d < ndp) ? rowp[((size_t)d * ncomb + cm[d]) * RS + k]
-                                         : b.realb[((size_t)(d - ndp) * cstride + cm[d]) * RS + k];
-                    prod *= x;
-                }
-                vK += Rv.wk[k] * prod;
-                if (judge) vG += Rv.wg[k] * prod;
-            }
-            vK = tce_warp_sum(vK);
-            if (judge) vG = tce_warp_sum(vG);
-            if (lane == 0) {
-                double cf = S.sh_coef[S.sh_coff[Q.SI] + ca * npA + i] * S.sh_coef[S.sh_coff[Q.SJ] + cb * npB + j] *
-                            S.sh_coef[S.sh_coff[Q.SK] + cc * npC + kp] * S.sh_coef[S.sh_coff[Q.SL] + cd * npD + lp];
-                b.blkK[cq] += fac * cf * vK;
-                if (judge) b.blkG[cq] += fac * cf * vG;
-            }
-        }
-        __syncwarp();
     }
 }
 
@@ -423,6 +450,11 @@ __device__ __forceinline__ void make_ctx(const DevSys &S, int4 q, QCtx &Q)
     Q.lsA = S.sh_l[Q.SI]; Q.lsB = S.sh_l[Q.SJ]; Q.lsC = S.sh_l[Q.SK]; Q.lsD = S.sh_l[Q.SL];
     Q.ncomb = (Q.lsA + 1) * (Q.lsB + 1) * (Q.lsC + 1) * (Q.lsD + 1);
     Q.ncq = Q.nA * Q.nB * Q.nC * Q.nD;
+    {
+        int p2 = 1;
+        while (p2 < Q.ncq) p2 <<= 1;
+        Q.cqg = p2 >= 32 ? 1 : 32 / p2;
+    }
     Q.NN = Q.lsA + Q.lsB + Q.lsC + Q.lsD;
     Q.R = Q.ncomb * S.ndp;
     const int cK = Q.SK / S.nshuc;
@@ -548,9 +580,9 @@ __device__ void consume(const DevSys &S, const QuartetArgs &A, const QCtx &Q, co
                     int g[4];
 #pragma unroll
                     for (int ii = 0; ii < 4; ++ii) g[ii] = f[perm[ip][ii]];
-                    int ref = g[0] / S.nfuc;
+                    const int4 rc = __ldg(S.fn_cell + g[0]);
 #pragma unroll
-                    for (int ii = 0; ii < 4; ++ii) g[ii] = tce_shift_to(g[ii], ref, S.nfuc, S.ncl);
+                    for (int ii = 0; ii < 4; ++ii) g[ii] = tce_shift_fn(S, g[ii], rc.x, rc.y, rc.z);
                     long long e;
                     if (A.physicist)
                         e = g[0] + (long long)A.eri_size * (g[2] + (long long)S.nbas * (g[1] + (long long)S.nbas * g[3]));
@@ -598,7 +630,7 @@ __global__ void __launch_bounds__(256) k_quartets(DevSys S, QuartetArgs A)
 {
     extern __shared__ double smem[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const WarpBuf b = warp_buf(A, smem + (size_t)wib * A.warp_smem_doubles, 3 - S.ndp, NQ + 1);
+    const WarpBuf b = warp_buf(A, smem + (size_t)wib * A.warp_smem_doubles, 3 - S.ndp, (NQ < 32 ? NQ : 32) + 1);
     const bool lg = (A.method == TCE_METHOD_LEARNED);
     RuleView Rfix;
     if (A.rule_override >= 0) {
@@ -979,7 +1011,7 @@ int tce_launch_quartets(const DevSys &S, const QuartetHostArgs &h, cudaStream_t 
     const int nq = plain ? 16 : (dict ? h.dict_nq : S.nq);
     const int R = h.max_ncomb * S.ndp;
     const int rowcap = R > 32 ? R : 32;
-    const int RS = nq + 1;
+    const int RS = (nq < 32 ? nq : 32) + 1;   // rows of one chunk of at most 32 nodes
     const int nreal = 3 - S.ndp;
     const int blkcap = (h.max_ncq + 3) / 4 * 4;
     long long wdoubles = 2LL * rowcap + (long long)rowcap * RS + (long long)nreal * h.max_ncomb * RS + 2LL * blkcap + 8;
