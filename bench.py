@@ -198,10 +198,13 @@ def dfmp2_timing(n_scf=8):
     """DF-MP2 on the 128-cell chain (the DF-MP2 configuration: the 64-cell chain's
     cell and basis on 128 cells, even-tempered auxiliary 4s/2p/1d per H, ratio
     2.5 from 0.1): orbitals from n_scf RHF iterations (timing, not converged),
-    device integrals, host fitting, device (ov|ov) contraction + energy in FP64
-    and in split-BF16 on the tensor cores (CUDA events)."""
+    then the C-ABI route a Fortran caller takes: tce_df_create (device
+    integrals, per-k metric factorisation, df_B) and tce_dfmp2 (L vectors,
+    (ov|ov) contraction and energy) in FP64 and in split-BF16 on the tensor
+    cores; the density-fitted J/K of the SCF (tce_dfjk) from the handle's df_B
+    and Bh."""
     from william_ci_b200 import df, scf
-    from william_ci_b200.engine import Engine, dfmp2_energy
+    from william_ci_b200.engine import Engine
     from william_ci_b200.system import AOSystem
     base = os.path.join(ROOT, "tests", "golden", "systems")
     ao = AOSystem.load(os.path.join(base, "h_chain128.npz"))
@@ -213,22 +216,20 @@ def dfmp2_timing(n_scf=8):
         r = scf.rhf_sao(S_, T_, V_, float(z["enuc"]), scf.n_occupied(ao), ao.nfuc, ao.ncell, eng.direct_JK,
                         max_scf=n_scf)
     t1 = time.perf_counter()
-    dfit = df.DensityFitting(df.df_system(ao, aux))
-    Vm, T3 = dfit.metric(), dfit.three_index()
+    dev = df.DeviceDF(ao, aux)
     t2 = time.perf_counter()
-    B, dfit.ndrop, Bh = df.fit_B(Vm, T3, dfit.ncl, dfit.dfs.nau, bh=True)
-    (p0, p1), (q0, q1) = df.band_ranges(r.occ_k)
-    L = dfit.L(B, r.C_k, (p0, p1), (q0, q1))
+    e64 = dev.dfmp2(r.C_k, r.eps_k, r.occ_k, mode=0)           # first call: module load, allocations
     t3 = time.perf_counter()
-    args = (dfit.ncl, L, r.eps_k[:, p0:p1], r.occ_k[:, p0:p1], r.eps_k[:, q0:q1], r.occ_k[:, q0:q1])
-    dfmp2_energy(*args, mode=1)                                  # warm-up
-    e16 = min((dfmp2_energy(*args, mode=1) for _ in range(3)), key=lambda d: d["ms"])
-    e64 = min((dfmp2_energy(*args, mode=0) for _ in range(3)), key=lambda d: d["ms"])
-    N, nau, ov = dfit.N, dfit.dfs.nau, (p1 - p0) * (q1 - q0)
-    flops = 3.0 * 8.0 * N ** 3 * ov * ov * nau          # complex MACs, three split-BF16 products
-    dfit.eng.close()
+    e64 = dev.dfmp2(r.C_k, r.eps_k, r.occ_k, mode=0)
+    t4 = time.perf_counter()
+    e16 = dev.dfmp2(r.C_k, r.eps_k, r.occ_k, mode=1)
+    t5 = time.perf_counter()
+    B, ndrop, Bh = dev.fitted(bh=True)
+    dev.close()
+    (p0, p1), (q0, q1) = df.band_ranges(r.occ_k)
+    N, nau = int(np.prod(ao.ncell)), aux.nfuc
     # density-fitted J/K of the SCF (df_JK) on the device, with the last RHF density
-    jk = df.DFJK(B, Bh, dfit.ncl, dfit.dfs.nfuc_ao, nau)
+    jk = df.DFJK(B, Bh, ao.ncell, ao.nfuc, nau)
     jk(r.P)
     tj = []
     for _ in range(5):
@@ -238,15 +239,15 @@ def dfmp2_timing(n_scf=8):
     jk.close()
     return {"workload": "Tori1D H chain, 128 cells, L=230.4, nbas=768, aux 4s/2p/1d per H (naux %d), no=%d nv=%d"
                         % (N * nau, p1 - p0, q1 - q0),
-            "rhf_iterations": r.iterations, "rhf_s": t1 - t0, "integrals_s": t2 - t1, "host_fit_s": t3 - t2,
-            "metric_pivots_dropped": int(dfit.ndrop),
-            "contraction_energy_ms_split_bf16": e16["ms"], "contraction_energy_ms_fp64": e64["ms"],
+            "rhf_iterations": r.iterations, "rhf_s": t1 - t0,
+            "df_create_s": t2 - t1, "dfmp2_fp64_s": t4 - t3, "dfmp2_split_bf16_s": t5 - t4,
+            "stage_s_excluding_rhf": (t2 - t1) + (t4 - t3),
+            "metric_pivots_dropped": int(ndrop),
             "emp2_split_bf16": e16["emp2"], "emp2_fp64": e64["emp2"],
             "split_bf16_rel_err_vs_fp64": abs(e16["emp2"] - e64["emp2"]) / max(abs(e64["emp2"]), 1e-300),
-            "zero_gap_terms": e64["nzero"],
             "df_jk_ms": 1e3 * float(np.median(tj)),
-            "df_jk_api": "tce_dfjk (host P in, J and K out; df_B and the k-space Bh resident on the device)",
-            "tensor_tflops_split_bf16": flops / (e16["ms"] * 1e-3) / 1e12,
+            "api": "tce_df_create (integrals, fitting, df_B on the device) + tce_dfmp2 (L vectors, contraction, "
+                   "energy); tce_dfjk with the handle's df_B and Bh",
             "note": "orbitals of %d RHF iterations of a half-filled band (zero-gap terms left out as kMP2_calc does); "
                     "times the DF-MP2 stage, not a converged MP2 energy" % n_scf}
 

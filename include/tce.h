@@ -416,6 +416,39 @@ int tce_dfmp2_energy(int32_t ncell, const int32_t ncl[3], const int32_t *kcoord,
                      double *ms);
 const char *tce_mp2_last_error(void);
 
+/* ------------------------------------------------------------------------
+ * Density fitting and DF-MP2 from one handle (replaces df_init,
+ * df_toroidal.f90:352-701 with chol_f :1174-1216, df_L_kap :1053-1104 and
+ * kMP2_calc, MP2_SAO.f90:6-151).  tce_df_create takes the orbital system (as
+ * tce_create) and the auxiliary basis on the same supercell (normalised, cells
+ * numbered as the orbitals), and the atoms (geometry(natoms,3) column-major,
+ * cells x fastest, atoms of a cell together): it builds the fit's system
+ * (per cell the orbital functions, the auxiliary functions and one constant
+ * dummy per atom), computes the metric (P0|Q R) and the three-index
+ * (mu0 nu|P R) integrals on the device, factorises V(k) per k (pivoted
+ * Cholesky, tolerance 1e-10) and keeps df_B on the device.  At most 32
+ * auxiliary functions per cell.  Own error string: tce_df_last_error. */
+int tce_df_create(const tce_system *ao, const tce_system *aux, int32_t natoms, const double *geometry, void **df);
+int tce_df_destroy(void *df);
+const char *tce_df_last_error(void *df);
+/* Host copies of the metric Vm(nau, naux) and T3(nfuc, nbas, naux), naux = nau
+ * cells, column-major (either may be NULL). */
+int tce_df_integrals(void *df, double *Vm, double *T3);
+/* Host copies of df_B(nfuc, nbas, naux) and of the k-space
+ * df_Bh(nfuc, nau, nfuc, cells, nkh) (complex, interleaved), the inputs of
+ * tce_dfjk_create; ndrop: the most metric pivots dropped at any k.  Any
+ * pointer may be NULL. */
+int tce_df_fitted(void *df, double *B, double *Bh, int32_t *ndrop);
+/* E_MP2 = 2 E2d - E2x of an RHF solution: coeff is coeff_SAO (nbas x nbas
+ * complex, interleaved, column-major, k blocks on the diagonal), eps and occ
+ * the orbital energies and occupations (2 or 0) in the same order (k block by
+ * k block).  The band ranges are cc_dims' (occupied 1..max_k nocc(k), virtual
+ * min_k nocc(k)+1..nfuc); the L vectors are formed on the device and
+ * contracted as tce_dfmp2_energy (mode 0 FP64, 1 split-BF16).  e2d, e2x may be
+ * NULL. */
+int tce_dfmp2(void *df, const double *coeff, const double *eps, const int32_t *occ, int32_t mode, double *e_mp2,
+              double *e2d, double *e2x);
+
 /* Library build identification (sm_100a, version). */
 const char *tce_version(void);
 

@@ -30,7 +30,7 @@ from typing import Dict, List, Tuple
 import numpy as np
 import scipy.linalg.lapack as lapack
 
-from .engine import Engine, dfmp2_energy
+from .engine import Engine, TCEError, dfmp2_energy, lib, tce_system
 from .system import AOSystem, Basis, BasisBlock
 
 METRIC_TOL = 1e-10           # metric_tol_aux (df_toroidal.f90:68)
@@ -340,3 +340,85 @@ def dfmp2(dfit: DensityFitting, C_k, eps_k, occ_k, mode: int = 1, B=None) -> Dic
     L = dfit.L(B, C_k, (p0, p1), (q0, q1))
     return dfmp2_energy(dfit.ncl, L, eps_k[:, p0:p1], occ_k[:, p0:p1], eps_k[:, q0:q1], occ_k[:, q0:q1],
                         mode=mode)
+
+
+class DeviceDF:
+    """df_init, df_L_kap and kMP2_calc behind one libtce handle (tce_df_create,
+    tce_dfmp2): the fit's integrals, the per-k factorisation of the metric,
+    df_B and the L vectors all on the device; a Fortran caller gets E_MP2 from
+    the same two calls."""
+
+    def __init__(self, ao: AOSystem, aux: AOSystem):
+        import ctypes as C
+        self.ao, self.aux = ao, aux
+        s1, self._k1 = tce_system(ao)
+        s2, self._k2 = tce_system(aux)
+        self._geo = np.asfortranarray(ao.geometry, dtype=np.float64).ravel(order="F").copy()
+        self.h = C.c_void_p()
+        code = lib().tce_df_create(C.byref(s1), C.byref(s2), len(ao.charges),
+                                   self._geo.ctypes.data_as(C.POINTER(C.c_double)), C.byref(self.h))
+        if code:
+            raise TCEError(code, lib().tce_df_last_error(None).decode())
+        self.ncl = tuple(ao.ncell)
+        self.N = int(np.prod(self.ncl))
+        self.nf, self.nau = ao.nfuc, aux.nfuc
+
+    def _ck(self, code):
+        if code:
+            raise TCEError(code, lib().tce_df_last_error(self.h).decode())
+
+    def integrals(self):
+        """Vm (nau, naux) and T3 (nfuc, nbas, naux)."""
+        import ctypes as C
+        naux, nb = self.nau * self.N, self.nf * self.N
+        Vm = np.zeros(self.nau * naux)
+        T3 = np.zeros(self.nf * nb * naux)
+        dp = C.POINTER(C.c_double)
+        self._ck(lib().tce_df_integrals(self.h, Vm.ctypes.data_as(dp), T3.ctypes.data_as(dp)))
+        return Vm.reshape(self.nau, naux, order="F"), T3.reshape(self.nf, nb, naux, order="F")
+
+    def fitted(self, bh: bool = False):
+        """df_B (nfuc, nbas, naux), the most dropped pivots, and with bh=True the
+        k-space Bh (nfuc, nau, nfuc, N, nkh) of the density-fitted J/K."""
+        import ctypes as C
+        naux, nb = self.nau * self.N, self.nf * self.N
+        B = np.zeros(self.nf * nb * naux)
+        nkh = int((khalf(self.ncl) >= 0).sum())
+        Bh = np.zeros(2 * self.nf * self.nau * self.nf * self.N * nkh) if bh else None
+        nd = C.c_int32()
+        dp = C.POINTER(C.c_double)
+        self._ck(lib().tce_df_fitted(self.h, B.ctypes.data_as(dp), Bh.ctypes.data_as(dp) if bh else None,
+                                     C.byref(nd)))
+        B = B.reshape(self.nf, nb, naux, order="F")
+        if not bh:
+            return B, nd.value
+        return B, nd.value, Bh.view(np.complex128).reshape(self.nf, self.nau, self.nf, self.N, nkh, order="F")
+
+    def dfmp2(self, C_k: np.ndarray, eps_k: np.ndarray, occ_k: np.ndarray, mode: int = 0) -> Dict[str, float]:
+        """E_MP2 from the SCF's k-block orbitals (N, nf, nf), energies and occupations (N, nf)."""
+        import ctypes as C
+        N, nf = self.N, self.nf
+        n = N * nf
+        coeff = np.zeros((n, n), dtype=np.complex128)
+        for k in range(N):
+            coeff[k * nf:(k + 1) * nf, k * nf:(k + 1) * nf] = C_k[k]
+        cf = np.asfortranarray(coeff).ravel(order="F").copy().view(np.float64)
+        eps = np.ascontiguousarray(eps_k, dtype=np.float64).ravel()
+        occ = np.ascontiguousarray(occ_k, dtype=np.int32).ravel()
+        e, e2d, e2x = C.c_double(), C.c_double(), C.c_double()
+        dp = C.POINTER(C.c_double)
+        self._ck(lib().tce_dfmp2(self.h, cf.ctypes.data_as(dp), eps.ctypes.data_as(dp),
+                                 occ.ctypes.data_as(C.POINTER(C.c_int32)), int(mode), C.byref(e), C.byref(e2d),
+                                 C.byref(e2x)))
+        return {"emp2": e.value, "e2d": e2d.value, "e2x": e2x.value}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().tce_df_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

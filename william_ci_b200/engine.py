@@ -45,7 +45,8 @@ EXPORTS = ["tce_create", "tce_destroy", "tce_last_error", "tce_get_info", "tce_s
            "tce_set_fp32_threshold", "tce_dfmp2_energy", "tce_mp2_last_error", "tce_create_blocks",
            "tce_pass_kernels", "tce_set_tensor_cores", "tce_nuclear_attraction", "tce_quad_self_check_nuc",
            "tce_lg_autotune", "tce_lg_lists", "tce_dfjk_create", "tce_dfjk", "tce_dfjk_destroy",
-           "tce_dfjk_last_error", "tce_ao_to_kmo", "tce_shard_items", "tce_lg_list_profile"]
+           "tce_dfjk_last_error", "tce_ao_to_kmo", "tce_shard_items", "tce_lg_list_profile",
+           "tce_df_create", "tce_df_destroy", "tce_df_last_error", "tce_df_integrals", "tce_df_fitted", "tce_dfmp2"]
 
 TCE_METHOD_FIXED, TCE_METHOD_LEARNED, TCE_METHOD_PLAIN = 0, 1, 2
 TCE_NFEAT = 12
@@ -149,6 +150,13 @@ def lib():
         L.tce_dfmp2_energy.argtypes = [C.c_int32, _ip, _ip, C.c_int32, C.c_int32, C.c_int32, _dp, _dp, _ip, _dp,
                                        _ip, C.c_int32, _dp, _dp, _lp, _dp, _dp]
         L.tce_mp2_last_error.restype = C.c_char_p
+        L.tce_df_create.argtypes = [C.POINTER(TceSystem), C.POINTER(TceSystem), C.c_int32, _dp, C.POINTER(C.c_void_p)]
+        L.tce_df_destroy.argtypes = [C.c_void_p]
+        L.tce_df_last_error.restype = C.c_char_p
+        L.tce_df_last_error.argtypes = [C.c_void_p]
+        L.tce_df_integrals.argtypes = [C.c_void_p, _dp, _dp]
+        L.tce_df_fitted.argtypes = [C.c_void_p, _dp, _dp, _ip]
+        L.tce_dfmp2.argtypes = [C.c_void_p, _dp, _dp, _ip, C.c_int32, _dp, _dp, _dp]
         _lib = L
     return _lib
 
@@ -167,6 +175,35 @@ def _i(a: np.ndarray):
     return a.ctypes.data_as(_ip)
 
 
+def tce_system(system: AOSystem, nquad: int = 32, t_nodes=None, t_weights=None, physicist=False, sao=True,
+               prim_screen=True, schwarz_thr=1e-13, prim_thr=1e-14):
+    """The flat tce_system of a supercell basis, and the arrays it points into
+    (keep them alive as long as the struct is used)."""
+    keep = [np.ascontiguousarray(system.ctr, dtype=np.float64).ravel(),
+            np.ascontiguousarray(system.lxyz, dtype=np.int32).ravel(),
+            np.ascontiguousarray(system.prim_off, dtype=np.int32),
+            np.ascontiguousarray(system.exps, dtype=np.float64),
+            np.ascontiguousarray(system.coefs, dtype=np.float64)]
+    s = TceSystem()
+    s.ndp = system.ndp
+    for d in range(3):
+        s.ncell[d] = system.ncell[d]
+        s.L[d] = system.L[d]
+    s.nfuc = system.nfuc
+    s.nbas = system.nbas
+    s.nquad = nquad
+    s.ctr, s.lxyz, s.prim_off, s.exps, s.coefs = (_d(keep[0]), _i(keep[1]), _i(keep[2]), _d(keep[3]), _d(keep[4]))
+    if t_nodes is not None:
+        tn = np.ascontiguousarray(t_nodes, dtype=np.float64)
+        tw = np.ascontiguousarray(t_weights, dtype=np.float64)
+        keep += [tn, tw]
+        s.nquad = len(tn)
+        s.t_nodes, s.t_weights = _d(tn), _d(tw)
+    s.physicist, s.sao, s.prim_screen = int(physicist), int(sao), int(prim_screen)
+    s.schwarz_thr, s.prim_thr = schwarz_thr, prim_thr
+    return s, keep
+
+
 class Engine:
     """Device engine for one supercell basis (normalised coefficients)."""
 
@@ -175,29 +212,8 @@ class Engine:
         self.sys = system
         self.physicist = bool(physicist)
         self.sao = bool(sao)
-        self._keep = [np.ascontiguousarray(system.ctr, dtype=np.float64).ravel(),
-                      np.ascontiguousarray(system.lxyz, dtype=np.int32).ravel(),
-                      np.ascontiguousarray(system.prim_off, dtype=np.int32),
-                      np.ascontiguousarray(system.exps, dtype=np.float64),
-                      np.ascontiguousarray(system.coefs, dtype=np.float64)]
-        s = TceSystem()
-        s.ndp = system.ndp
-        for d in range(3):
-            s.ncell[d] = system.ncell[d]
-            s.L[d] = system.L[d]
-        s.nfuc = system.nfuc
-        s.nbas = system.nbas
-        s.nquad = nquad
-        s.ctr, s.lxyz, s.prim_off, s.exps, s.coefs = (_d(self._keep[0]), _i(self._keep[1]), _i(self._keep[2]),
-                                                      _d(self._keep[3]), _d(self._keep[4]))
-        if t_nodes is not None:
-            tn = np.ascontiguousarray(t_nodes, dtype=np.float64)
-            tw = np.ascontiguousarray(t_weights, dtype=np.float64)
-            self._keep += [tn, tw]
-            s.nquad = len(tn)
-            s.t_nodes, s.t_weights = _d(tn), _d(tw)
-        s.physicist, s.sao, s.prim_screen = int(physicist), int(sao), int(prim_screen)
-        s.schwarz_thr, s.prim_thr = schwarz_thr, prim_thr
+        s, self._keep = tce_system(system, nquad, t_nodes, t_weights, physicist, sao, prim_screen, schwarz_thr,
+                                   prim_thr)
         self._s = s
         h = C.c_void_p()
         create = lib().tce_create_blocks if blocks_only else lib().tce_create
