@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-pass", action="store_true",
+                    help="for ncu --profile-from-start off: set the learned grid up (tce_lg_setup), run two warm "
+                         "passes, then one pass between cudaProfilerStart and cudaProfilerStop, and exit")
     return ap.parse_args()
 
 
@@ -551,6 +554,31 @@ def timed_passes(eng, step, steps, flush, stream, world, dist):
     return sum(a.elapsed_time(b) for a, b in ev), float(np.mean(kern))
 
 
+def profile_pass(sysm):
+    """One learned-grid pass of the workload inside cudaProfilerStart/Stop (the
+    kernels of the pass as separate launches, no graph), after the set-up
+    through the C ABI (tce_lg_setup), the kernel-form tuning and two warm
+    passes (the judge's rejects moved to the plain list)."""
+    import torch
+    from william_ci_b200.engine import TCE_METHOD_LEARNED, Engine
+    eng = Engine(sysm)
+    eng.lg_setup(n_train=16000, seed=2026, epochs=80)
+    eng.set_method(TCE_METHOD_LEARNED)
+    eng.set_fp32_threshold(FP32_THRESHOLD)
+    eng.lg_autotune(3)
+    P = density(sysm.nbas)
+    for _ in range(2):
+        eng.direct_JK(P)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    eng.direct_JK(P)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    print(json.dumps({"profiled": "one learned-grid J/K pass", "kernels": eng.pass_kernels(),
+                      "kernel_ms": eng.last_kernel_ms(), "stats": eng.lg_stats()}))
+    eng.close()
+
+
 def main():
     args = parse()
     from william_ci_b200.system import AOSystem
@@ -562,6 +590,9 @@ def main():
     import torch
     import torch.distributed as dist
     from william_ci_b200.engine import TCE_METHOD_FIXED, TCE_METHOD_LEARNED, TCE_METHOD_PLAIN, Engine
+    if args.profile_pass:
+        profile_pass(sysm)
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -321,6 +321,32 @@ int tce_lg_rule_gmax(void *handle, int32_t *gmax);
  * (n = 15) with the embedded 7-point Gauss weights, mapped t = scale u/(1-u). */
 int tce_set_plain_rule(void *handle, int32_t n, const double *u, const double *wk, const double *wg, double scale);
 
+/* Host-only: the (2n+1)-point Gauss-Kronrod rule on u in [0, 1] (ascending
+ * nodes u, Kronrod weights wk, embedded n-point Gauss weights wg, zero off the
+ * Gauss nodes), by Laurie's algorithm and the Golub-Welsch eigenvalue
+ * problem in extended precision; 1 <= n <= 64.  The rules of the
+ * learned-grid dictionary are these, mapped by t = s u/(1-u). */
+int tce_gk_rule(int32_t n, double *u, double *wk, double *wg);
+
+/* Host-only: the learned grid's rule dictionary as tce_lg_setup loads it:
+ * *nrules rules (K15, K21, K31, K41, K61 times 21 map scales 0.6 2^(j/2),
+ * j = -18..2, order-major), rule r with nn[r] nodes t[64r+k], Kronrod weights
+ * wk[64r+k] and Gauss weights wg[64r+k]; any array may be NULL. */
+int tce_lg_dictionary(int32_t *nrules, int32_t *nn, double *t, double *wk, double *wg);
+
+/* The whole set-up of the learned grid in one call, for a caller without the
+ * Python host side: load the dictionary and the plain method's panel rule,
+ * draw n_train of the handle's quartets (seeded), label them against the
+ * 128-node mapped Gauss-Legendre reference evaluated on the handle (a rule is
+ * correct when its block is within label_tol of the reference, 3e-14 is the
+ * tested value, the judge accepts it, and the two next smaller scales of its
+ * order are correct too), train the rule-picking network on the GPU (epochs,
+ * batches of 256, Adam at 2e-3) and set every quartet's rule
+ * (tce_lg_predict_rules, plain factor 10).  Then tce_set_method(h,
+ * TCE_METHOD_LEARNED).  With net_out the trained network is returned (free it
+ * with tce_mlp_destroy), else it is freed.  No reference counterpart. */
+int tce_lg_setup(void *handle, int64_t n_train, uint64_t seed, int32_t epochs, double label_tol, void **net_out);
+
 /* Per-item rules (engine item order); value nrules sends the item straight to
  * the plain method. */
 int tce_lg_set_item_rules(void *handle, const int32_t *rule);

@@ -346,3 +346,39 @@ def test_autotune_keeps_the_results(chain16_lg):
         J1, K1 = eng.direct_JK(P)
         assert np.abs(J1 - J0).max() <= 1e-12 * scale and np.abs(K1 - K0).max() <= 1e-12 * scale
     eng.set_graph(False)
+
+
+def test_learned_grid_setup_from_the_c_abi(systems):
+    """tce_lg_setup: the dictionary, labels, training and prediction inside
+    libtce (the route of a Fortran caller): held-out blocks of the rules it sets
+    within 1e-10 of the 128-node reference, J/K equal to the plain method's."""
+    from william_ci_b200 import learned_grid as LG
+    from william_ci_b200.engine import TCE_METHOD_LEARNED, TCE_METHOD_PLAIN, Engine
+    sysm = systems("h_chain64", (16, 1, 1))
+    eng = Engine(sysm)
+    eng.lg_setup(n_train=4000, seed=7, epochs=60)
+    rules = eng.lg_item_rules()
+    items = eng.items()
+    ref = LG.ReferenceBlocks(sysm)
+    sel = np.random.default_rng(12).choice(len(items), 1500, replace=False)
+    T, _, offs = ref.rule_blocks(-1, items[sel])
+    worst = 0.0
+    for r in np.unique(rules[sel]):
+        m = np.nonzero(rules[sel] == r)[0]
+        if r == eng.nrules:
+            K, _, o2 = eng.rule_blocks(-2, items[sel][m])
+        else:
+            K, G, o2 = eng.rule_blocks(int(r), items[sel][m], judge=True)
+            m, K, o2 = _accepted(m, K, o2, LG.judge_estimate(K, G, o2))
+        for j, i in enumerate(m):
+            worst = max(worst, np.abs(K[o2[j]:o2[j + 1]] - T[offs[i]:offs[i + 1]]).max(initial=0.0))
+    assert worst <= TOL_INT
+    P = random_density(sysm.nbas, 2) * 0.05
+    eng.set_method(TCE_METHOD_PLAIN)
+    Jp, Kp = eng.direct_JK(P)
+    eng.set_method(TCE_METHOD_LEARNED)
+    Jl, Kl = eng.direct_JK(P)
+    scale = np.abs(P).sum()
+    assert np.abs(Jl - Jp).max() <= 1e-10 * scale and np.abs(Kl - Kp).max() <= 1e-10 * scale
+    ref.close()
+    eng.close()

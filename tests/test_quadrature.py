@@ -81,3 +81,22 @@ def test_mlp_oracle_gradient_finite_differences():
         fd = (mlp_ref.loss_grad(p + e, mu, sig, X, Y, nf, nh, nc)[0] -
               mlp_ref.loss_grad(p - e, mu, sig, X, Y, nf, nh, nc)[0]) / (2 * h)
         assert abs(fd - g[i]) < 1e-6 * max(1.0, abs(g[i]))
+
+
+def test_library_kronrod_rules_equal_the_exact_ones():
+    """libtce's Gauss-Kronrod rules (Laurie's algorithm, extended precision,
+    tce_gk_rule) against the ones built here from the definition in 60-digit
+    arithmetic, and the dictionary tce_lg_setup loads against the host's."""
+    from william_ci_b200 import engine as E
+    from william_ci_b200 import learned_grid as LG
+    for n in Q.RULE_ORDERS + (1, 3):
+        u, wk, wg = E.gk_rule(n)
+        u2, wk2, wg2 = Q.gauss_kronrod(n)
+        assert np.abs(u - u2).max() < 1e-15 and np.abs(wk - wk2).max() < 1e-15 and np.abs(wg - wg2).max() < 1e-15
+    lib_rules = E.lg_dictionary()
+    host_rules, _ = LG.dictionary()
+    assert len(lib_rules) == len(host_rules)
+    for a, b in zip(lib_rules, host_rules):
+        for x, y in zip(a, b):
+            assert x.shape == y.shape
+            assert np.abs(x - y).max() <= 1e-15 * np.abs(y).max()

@@ -46,7 +46,8 @@ EXPORTS = ["tce_create", "tce_destroy", "tce_last_error", "tce_get_info", "tce_s
            "tce_pass_kernels", "tce_set_tensor_cores", "tce_nuclear_attraction", "tce_quad_self_check_nuc",
            "tce_lg_autotune", "tce_lg_lists", "tce_dfjk_create", "tce_dfjk", "tce_dfjk_destroy",
            "tce_dfjk_last_error", "tce_ao_to_kmo", "tce_shard_items", "tce_lg_list_profile",
-           "tce_df_create", "tce_df_destroy", "tce_df_last_error", "tce_df_integrals", "tce_df_fitted", "tce_dfmp2"]
+           "tce_df_create", "tce_df_destroy", "tce_df_last_error", "tce_df_integrals", "tce_df_fitted", "tce_dfmp2",
+           "tce_gk_rule", "tce_lg_dictionary", "tce_lg_setup"]
 
 TCE_METHOD_FIXED, TCE_METHOD_LEARNED, TCE_METHOD_PLAIN = 0, 1, 2
 TCE_NFEAT = 12
@@ -157,6 +158,9 @@ def lib():
         L.tce_df_integrals.argtypes = [C.c_void_p, _dp, _dp]
         L.tce_df_fitted.argtypes = [C.c_void_p, _dp, _dp, _ip]
         L.tce_dfmp2.argtypes = [C.c_void_p, _dp, _dp, _ip, C.c_int32, _dp, _dp, _dp]
+        L.tce_gk_rule.argtypes = [C.c_int32, _dp, _dp, _dp]
+        L.tce_lg_dictionary.argtypes = [_ip, _ip, _dp, _dp, _dp]
+        L.tce_lg_setup.argtypes = [C.c_void_p, C.c_int64, C.c_uint64, C.c_int32, C.c_double, C.POINTER(C.c_void_p)]
         _lib = L
     return _lib
 
@@ -394,6 +398,14 @@ class Engine:
         _check(lib().tce_lg_item_rules(self.h, _i(r)), self.h)
         return r
 
+    def lg_setup(self, n_train: int = 16000, seed: int = 2026, epochs: int = 80, label_tol: float = 3e-14):
+        """The learned grid's whole set-up inside libtce (tce_lg_setup): dictionary,
+        labels, training on the GPU, per-quartet rules."""
+        _check(lib().tce_lg_setup(self.h, int(n_train), int(seed), int(epochs), float(label_tol), None), self.h)
+        n = C.c_int32()
+        _check(lib().tce_lg_dictionary(C.byref(n), None, None, None, None))
+        self.nrules = n.value
+
     def lg_predict_rules(self, net, plain_factor: float = 10.0):
         _check(lib().tce_lg_predict_rules(self.h, net.h, float(plain_factor)), self.h)
 
@@ -561,3 +573,22 @@ def fp64_peak_tflops() -> float:
     v = C.c_double()
     _check(lib().tce_fp64_peak(C.byref(v)))
     return v.value
+
+
+def gk_rule(n: int):
+    """(2n+1)-point Gauss-Kronrod rule on [0,1] built by libtce (host-only, no GPU
+    needed): nodes, Kronrod weights, embedded Gauss weights."""
+    u, wk, wg = (np.zeros(2 * n + 1) for _ in range(3))
+    _check(lib().tce_gk_rule(int(n), _d(u), _d(wk), _d(wg)))
+    return u, wk, wg
+
+
+def lg_dictionary():
+    """The rule dictionary libtce builds (tce_lg_dictionary): list of (t, wk, wg)."""
+    n = C.c_int32()
+    _check(lib().tce_lg_dictionary(C.byref(n), None, None, None, None))
+    R = n.value
+    nn = np.zeros(R, dtype=np.int32)
+    t, wk, wg = (np.zeros(64 * R) for _ in range(3))
+    _check(lib().tce_lg_dictionary(C.byref(n), _i(nn), _d(t), _d(wk), _d(wg)))
+    return [(t[64 * r:64 * r + nn[r]], wk[64 * r:64 * r + nn[r]], wg[64 * r:64 * r + nn[r]]) for r in range(R)]
