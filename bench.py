@@ -652,9 +652,14 @@ def main():
     tune = eng.lg_autotune(3) if world == 1 else None
     if tune is not None:
         names = {0: "generic", 1: "all-s", 2: "one-p"}
+        shapes = {1: "16x32", 2: "32x16", 3: "16x16", 4: "8x64"}
+
+        def form(w):
+            if not w["tc"]:
+                return "CUDA cores"
+            return "tensor cores" + (" %s tiles per pass" % shapes[w["tc"]] if w["kind"] == 1 else "")
         tune["lists"] = ["%s cls%d nq%d%s: %s, %d quartets" % (names[w["kind"]], w["cls"], w["nq"],
-                                                                " fp32" if w["fp32"] else "",
-                                                                "tensor cores" if w["tc"] else "CUDA cores", w["n"])
+                                                                " fp32" if w["fp32"] else "", form(w), w["n"])
                          for w in eng.lg_lists()]
     # every pass is one CUDA-graph launch from here on
     eng.set_graph(True)
@@ -766,6 +771,8 @@ def main():
         kernels = []
         for w in per_list:
             nm = names[w["kind"]] % ((w["nq"],) if w["kind"] == 0 else ("_tc" if w["tc"] else "", w["nq"]))
+            if w["kind"] == 1 and w["tc"]:
+                nm += " tile shape %d" % w["tc"]
             kernels.append({"kernel": nm + (" fp32" if w["fp32"] else ""), "cls": w["cls"], "quartets": w["n"],
                             "ms": w["ms"], "flops": w["flops"],
                             "tflops": w["flops"] / (w["ms"] * 1e-3) / 1e12 if w["ms"] > 0 else None,

@@ -194,19 +194,29 @@ int tce_set_tensor_cores(void *handle, int32_t on);
 
 /* Kernel-form tuning of the learned-grid pass (after tce_lg_predict_rules /
  * tce_lg_set_item_rules): every work list that has both a CUDA-core and an
- * FP64 tensor-core kernel is timed with each (reps launches each, CUDA
- * events; the fastest launch counts) and keeps the faster, also when the
- * lists are rebuilt later (new rules, rejects moved to the plain list).
+ * FP64 tensor-core kernel is timed in each of its forms (the CUDA-core
+ * kernel, the tensor-core kernel, and for the all-s quartets each tile shape
+ * of the tensor-core kernel: 16 primitive quartets x 32 nodes per pass, 32 x
+ * 16, 16 x 16, 8 x 64) with reps launches each (CUDA events; the fastest
+ * launch counts) and keeps the fastest, also when the lists are rebuilt later
+ * (new rules, rejects moved to the plain list).
  * ntuned: lists timed; nswitched: lists whose choice differs from the built-in
  * default; ms_saved: estimated time per pass saved against the default.  Uses
  * the handle's host-entry J/K buffers as scratch; results of later passes are
  * the same up to the summation order.  No reference counterpart. */
 int tce_lg_autotune(void *handle, int32_t reps, int32_t *ntuned, int32_t *nswitched, double *ms_saved);
 
+/* Set the kernel form of learned-grid work list `list` (its index in
+ * tce_lg_lists) by hand, as tce_lg_autotune would: 0 the CUDA-core kernel,
+ * 1 the tensor-core kernel, for all-s lists 1..4 its tile shape.  The form is
+ * kept for the list's key across rebuilds.  No reference counterpart. */
+int tce_lg_set_list_form(void *handle, int32_t list, int32_t form);
+
 /* The learned-grid work lists of the handle: *n lists; with info (6 int32
  * per list, *n on entry = its capacity in lists): kind (0 generic, 1 all-s,
  * 2 one-p), class bits, padded rule nodes (32/64), FP32 panels, kernel form in
- * use (0 CUDA cores, 1 FP64 tensor cores), quartets.  No reference
+ * use (0 CUDA cores, >= 1 FP64 tensor cores; for the all-s kernel 1..4 its
+ * tile shape in the order of tce_lg_autotune), quartets.  No reference
  * counterpart. */
 int tce_lg_lists(void *handle, int32_t *n, int32_t *info);
 

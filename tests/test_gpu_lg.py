@@ -382,3 +382,32 @@ def test_learned_grid_setup_from_the_c_abi(systems):
     assert np.abs(Jl - Jp).max() <= 1e-10 * scale and np.abs(Kl - Kp).max() <= 1e-10 * scale
     ref.close()
     eng.close()
+
+
+def test_every_all_s_tile_shape_gives_the_same_jk(chain16_lg):
+    """The all-s tensor-core kernel in each tile shape the autotuner can pick
+    (16 x 32, 32 x 16, 16 x 16, 8 x 64 primitive quartets x nodes per pass),
+    set by hand on every all-s list: J/K equal the CUDA-core kernel's to 1e-12
+    of the density scale."""
+    from william_ci_b200.engine import TCE_METHOD_LEARNED
+    sysm, eng, net = chain16_lg
+    P = random_density(sysm.nbas, 9) * 0.05
+    scale = np.abs(P).sum()
+    eng.set_method(TCE_METHOD_LEARNED)
+    eng.set_fp32_threshold(0.0)
+    eng.set_graph(False)
+    eng.lg_predict_rules(net)
+    eng.direct_JK(P)                     # the judge's rejects move to the plain list
+    lists = eng.lg_lists()
+    alls = [i for i, w in enumerate(lists) if w["kind"] == 1]
+    assert alls
+    for i in alls:
+        eng.lg_set_list_form(i, 0)
+    J0, K0 = eng.direct_JK(P)
+    for shape in (1, 2, 3, 4):
+        for i in alls:
+            eng.lg_set_list_form(i, shape)
+        J, K = eng.direct_JK(P)
+        assert np.abs(J - J0).max() <= 1e-12 * scale and np.abs(K - K0).max() <= 1e-12 * scale, shape
+    for i in alls:
+        eng.lg_set_list_form(i, 1)

@@ -89,7 +89,9 @@ int tce_launch_quartets_s_lg(const DevSys &S, const SArgsHost &h, int nq, bool f
 int tce_launch_quartets_r1_lg(const DevSys &S, int cls, const SArgsHost &h, int nq, bool fp32, cudaStream_t st);
 // all-s quartets of one periodic direction, learned grid, node sums on the FP64
 // tensor cores (k_quartets_s_tc, mma.sync m8n8k4)
-int tce_launch_quartets_s_tc(const DevSys &S, const SArgsHost &h, int nq, cudaStream_t st);
+int tce_launch_quartets_s_tc(const DevSys &S, const SArgsHost &h, int nq, int shape, cudaStream_t st);
+// number of tile shapes of the all-s tensor-core kernel for nq-node rules (shapes 1..n)
+int tce_tc_shapes_s(int nq);
 // one-p s/p classes of one periodic direction, learned grid, tensor-core node
 // sums (k_quartets_r1_tc); cls as tce_launch_quartets_r1
 int tce_launch_quartets_r1_tc(const DevSys &S, int cls, const SArgsHost &h, int nq, cudaStream_t st);

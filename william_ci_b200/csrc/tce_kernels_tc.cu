@@ -71,17 +71,20 @@ __device__ __forceinline__ int tce_pool_add(const DevSys &S, const SArgs &A, con
 }
 
 // MT row tiles of 8 per warp: batches of 8 MT primitive quartets; acc holds
-// the batch's 8 MT x 32 nodes of one pass (MT tiles x 4 node tiles x 2 per lane)
+// the batch's 8 MT rows x 8 NT nodes of one pass (MT x NT tiles, 2 per lane).
+// The one-p kernel uses MT = 2; the all-s kernel takes (MT, NT) as template
+// parameters, its tile shape (TCE_TC_SHAPES) chosen per work list by
+// tce_lg_autotune.
 constexpr int TCE_TC_MT = 2;
 constexpr int TCE_TC_BATCH = 8 * TCE_TC_MT;
-// node tiles of 8 per pass of the all-s kernel (4: 32 nodes per pass)
+// node tiles of 8 per pass of the one-p kernel and of the all-s default (4: 32 nodes per pass)
 constexpr int TCE_TC_NT = 4;
 
-template <int NQ>
+template <int NQ, int MTP, int NTP>
 __global__ void __launch_bounds__(256, 2) k_quartets_s_tc(DevSys S, SArgs A)
 {
-    constexpr int MT = TCE_TC_MT, BT = TCE_TC_BATCH;
-    constexpr int NT = (NQ / 8) < TCE_TC_NT ? (NQ / 8) : TCE_TC_NT;   // node tiles per pass
+    constexpr int MT = MTP, BT = 8 * MTP;
+    constexpr int NT = (NQ / 8) < NTP ? (NQ / 8) : NTP;   // node tiles per pass
     extern __shared__ double smem[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int rq = lane >> 2, cq = lane & 3;   // fragment row in an 8-row tile, fragment column
@@ -614,15 +617,34 @@ int tce_launch_quartets_r1_tc(const DevSys &S, int cls, const SArgsHost &h, int 
     return cudaGetLastError() == cudaSuccess ? TCE_OK : TCE_ERR_CUDA;
 }
 
-int tce_launch_quartets_s_tc(const DevSys &S, const SArgsHost &h, int nq, cudaStream_t st)
+int tce_tc_shapes_s(int nq)
+{
+    return (nq == 32 || nq == 64) ? 4 : 0;
+}
+
+// shape 1: 16 rows x 32 nodes per pass (the default), 2: 32 x 16, 3: 16 x 16,
+// 4: 8 rows x 64 nodes (x 32 for 32-node rules)
+int tce_launch_quartets_s_tc(const DevSys &S, const SArgsHost &h, int nq, int shape, cudaStream_t st)
 {
     if (!h.item_rule || !h.rules || !h.rule_T || !h.fb_items || !h.fb_count) return TCE_ERR_ARG;
     if (S.ndp != 1 || (nq != 32 && nq != 64)) return TCE_ERR_UNSUPPORTED;
+    if (shape < 1 || shape > tce_tc_shapes_s(nq)) return TCE_ERR_ARG;
     SArgs A{};
     tc_args(A, h);
-    cudaMemsetAsync(h.next, 0, sizeof(unsigned int), st);
+    if (cudaMemsetAsync(h.next, 0, sizeof(unsigned int), st) != cudaSuccess) return TCE_ERR_CUDA;
     const int nsm = h.num_sms > 0 ? h.num_sms : 148;
-    if (nq == 32) tc_launch(k_quartets_s_tc<32>, S, A, nsm, st);
-    else tc_launch(k_quartets_s_tc<64>, S, A, nsm, st);
+#define TCE_S_TC(NQv)                                                              \
+    switch (shape) {                                                               \
+    case 1: tc_launch(k_quartets_s_tc<NQv, 2, 4>, S, A, nsm, st); break;           \
+    case 2: tc_launch(k_quartets_s_tc<NQv, 4, 2>, S, A, nsm, st); break;           \
+    case 3: tc_launch(k_quartets_s_tc<NQv, 2, 2>, S, A, nsm, st); break;           \
+    default: tc_launch(k_quartets_s_tc<NQv, 1, 8>, S, A, nsm, st); break;          \
+    }
+    if (nq == 32) {
+        TCE_S_TC(32)
+    } else {
+        TCE_S_TC(64)
+    }
+#undef TCE_S_TC
     return cudaGetLastError() == cudaSuccess ? TCE_OK : TCE_ERR_CUDA;
 }

@@ -516,10 +516,15 @@ int lg_rebuild_lists(Handle *h)
 // FP64 quartets with 32-node rules, the generic rows with 64-node rules (the
 // forms measured faster on the 64-cell chain); FP32-panel lists keep their
 // CUDA-core kernels unless tuned otherwise.
-static bool lg_tc_available(const Handle *h, const Handle::LgList &w)
+// kernel forms of a list: 0 the CUDA-core kernel, 1.. the FP64 tensor-core
+// kernel (the all-s kernel in each of its tile shapes, TCE_TC_SHAPES)
+static int lg_nforms(const Handle *h, const Handle::LgList &w)
 {
-    return h->ndp == 1 && (w.nq == 32 || w.nq == 64);
+    if (h->ndp != 1 || (w.nq != 32 && w.nq != 64)) return 1;
+    return w.kind == 1 ? 1 + tce_tc_shapes_s(w.nq) : 2;
 }
+
+static bool lg_tc_available(const Handle *h, const Handle::LgList &w) { return lg_nforms(h, w) > 1; }
 
 static int lg_tc_default(const Handle *h, const Handle::LgList &w)
 {
@@ -535,7 +540,8 @@ static int lg_tc(const Handle *h, const Handle::LgList &w)
     return w.tc >= 0 ? w.tc : lg_tc_default(h, w);
 }
 
-// one learned-grid list with kernel form tc (0 CUDA cores, 1 FP64 tensor cores)
+// one learned-grid list with kernel form tc (0 CUDA cores, >= 1 FP64 tensor
+// cores; for the all-s kernel the tile shape)
 static int lg_launch_list(Handle *h, const Handle::LgList &w, const QuartetHostArgs &a, const double *dP, double *dJ,
                           double *dK, int tc, cudaStream_t st)
 {
@@ -572,7 +578,8 @@ static int lg_launch_list(Handle *h, const Handle::LgList &w, const QuartetHostA
     b.fb_items = h->d_fb_items;
     b.fb_count = h->d_fb_count;
     if (w.kind == 1)
-        return tc ? tce_launch_quartets_s_tc(h->S, b, w.nq, st) : tce_launch_quartets_s_lg(h->S, b, w.nq, w.fp32 != 0, st);
+        return tc ? tce_launch_quartets_s_tc(h->S, b, w.nq, tc, st)
+                  : tce_launch_quartets_s_lg(h->S, b, w.nq, w.fp32 != 0, st);
     return tc ? tce_launch_quartets_r1_tc(h->S, w.cls, b, w.nq, st)
               : tce_launch_quartets_r1_lg(h->S, w.cls, b, w.nq, w.fp32 != 0, st);
 }
@@ -1315,9 +1322,11 @@ int tce_lg_autotune(void *handle, int32_t reps, int32_t *ntuned, int32_t *nswitc
     double saved = 0.0;
     s = TCE_OK;
     for (auto &w : h->lg_lists) {
-        if (!lg_tc_available(h, w)) continue;
-        double best[2] = {1e300, 1e300};
-        for (int tc = 0; tc < 2 && s == TCE_OK; ++tc)
+        const int nf = lg_nforms(h, w);
+        if (nf < 2) continue;
+        double best[8];
+        for (int f = 0; f < 8; ++f) best[f] = 1e300;
+        for (int tc = 0; tc < nf && s == TCE_OK; ++tc)
             for (int r = 0; r < reps && s == TCE_OK; ++r) {
                 cudaMemsetAsync(h->d_fb_count, 0, sizeof(unsigned int), h->st);
                 cudaEventRecord(e0, h->st);
@@ -1329,11 +1338,14 @@ int tce_lg_autotune(void *handle, int32_t reps, int32_t *ntuned, int32_t *nswitc
                 best[tc] = std::min(best[tc], (double)ms);
             }
         if (s != TCE_OK) break;
-        // the other form only when it is clearly faster: isolated launches differ a
+        // another form only when it is clearly faster: isolated launches differ a
         // little from launches inside the pass, so near-ties keep the default
         const int dflt = lg_tc_default(h, w);
-        const double alt_t = best[1 - dflt], def_t = best[dflt];
-        const int choice = (alt_t < 0.97 * def_t && def_t - alt_t > 0.02) ? 1 - dflt : dflt;
+        int alt = dflt == 0 ? 1 : 0;
+        for (int f = 0; f < nf; ++f)
+            if (f != dflt && best[f] < best[alt]) alt = f;
+        const double alt_t = best[alt], def_t = best[dflt];
+        const int choice = (alt_t < 0.97 * def_t && def_t - alt_t > 0.02) ? alt : dflt;
         const int key = ((w.kind * 16 + w.cls) * 2 + (w.nq == 64 ? 1 : 0)) * 2 + (w.fp32 ? 1 : 0);
         h->tc_choice[key] = choice;
         w.tc = choice;
@@ -1418,6 +1430,24 @@ int tce_lg_list_profile(void *handle, int32_t reps, int32_t *n, double *ms, doub
     CK(h, cudaMemsetAsync(h->d_fb_count, 0, sizeof(unsigned int), h->st));
     CK(h, cudaStreamSynchronize(h->st));
     *n = (int32_t)h->lg_lists.size();
+    return TCE_OK;
+}
+
+int tce_lg_set_list_form(void *handle, int32_t list, int32_t form)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h) return fail(h, TCE_ERR_ARG, "NULL handle");
+    if (list < 0 || list >= (int32_t)h->lg_lists.size()) return fail(h, TCE_ERR_ARG, "no such work list");
+    auto &w = h->lg_lists[(size_t)list];
+    if (form < 0 || form >= lg_nforms(h, w)) return fail(h, TCE_ERR_ARG, "the list has no such kernel form");
+    const int key = ((w.kind * 16 + w.cls) * 2 + (w.nq == 64 ? 1 : 0)) * 2 + (w.fp32 ? 1 : 0);
+    h->tc_choice[key] = form;
+    w.tc = form;
+    // the captured pass is re-captured with the new form; rejects of the last
+    // pass stay valid (same items and rules)
+    const bool keep_fb = h->fb_version == h->work_version;
+    ++h->work_version;
+    if (keep_fb) h->fb_version = h->work_version;
     return TCE_OK;
 }
 

@@ -47,7 +47,7 @@ EXPORTS = ["tce_create", "tce_destroy", "tce_last_error", "tce_get_info", "tce_s
            "tce_lg_autotune", "tce_lg_lists", "tce_dfjk_create", "tce_dfjk", "tce_dfjk_destroy",
            "tce_dfjk_last_error", "tce_ao_to_kmo", "tce_shard_items", "tce_lg_list_profile",
            "tce_df_create", "tce_df_destroy", "tce_df_last_error", "tce_df_integrals", "tce_df_fitted", "tce_dfmp2",
-           "tce_gk_rule", "tce_lg_dictionary", "tce_lg_setup"]
+           "tce_gk_rule", "tce_lg_dictionary", "tce_lg_setup", "tce_lg_set_list_form"]
 
 TCE_METHOD_FIXED, TCE_METHOD_LEARNED, TCE_METHOD_PLAIN = 0, 1, 2
 TCE_NFEAT = 12
@@ -140,6 +140,7 @@ def lib():
         L.tce_lg_autotune.argtypes = [C.c_void_p, C.c_int32, _ip, _ip, _dp]
         L.tce_lg_lists.argtypes = [C.c_void_p, _ip, _ip]
         L.tce_lg_list_profile.argtypes = [C.c_void_p, C.c_int32, _ip, _dp, _dp]
+        L.tce_lg_set_list_form.argtypes = [C.c_void_p, C.c_int32, C.c_int32]
         L.tce_ao_to_kmo.argtypes = [C.c_void_p, _dp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _dp]
         L.tce_dfjk_create.argtypes = [C.c_int32, C.c_int32, C.c_int32, _ip, _dp, _dp, C.POINTER(C.c_void_p)]
         L.tce_dfjk.argtypes = [C.c_void_p, _dp, _dp, _dp]
@@ -461,6 +462,10 @@ class Engine:
         for i, w in enumerate(out[:n.value]):
             w["ms"], w["flops"] = float(ms[i]), float(fl[i])
         return out[:n.value]
+
+    def lg_set_list_form(self, i: int, form: int):
+        """Kernel form of learned-grid list i by hand (tce_lg_set_list_form)."""
+        _check(lib().tce_lg_set_list_form(self.h, int(i), int(form)), self.h)
 
     def set_tensor_cores(self, on: bool = True):
         """FP64 tensor-core node sums where a kernel has them (tce_set_tensor_cores)."""
