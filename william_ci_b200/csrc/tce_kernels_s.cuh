@@ -624,8 +624,9 @@ __global__ void __launch_bounds__(256, LG ? 2 : 1) k_quartets_r1(DevSys S, SArgs
                                 const int k = 8 * g0 + x;
                                 if (k >= NQ) break;
                                 const double t2 = tn[k] * tn[k];
-                                const double D2 = 1.0 / (pq_ + ps * t2);
-                                const double w = pq_ * t2 * D2, rs = PI_D * sqrt(D2);
+                                // D2 = 1 / (pq + (p + q) t^2) and PI sqrt(D2) from one reciprocal square root
+                                const double rr = rsqrt(pq_ + ps * t2), D2 = rr * rr;
+                                const double w = pq_ * t2 * D2, rs = PI_D * rr;
                                 double gy[NN + 1], gz[NN + 1];
                                 gy[0] = (Ry == 0.0) ? rs : rs * exp(-w * Ry * Ry);
                                 gz[0] = (Rz == 0.0) ? rs : rs * exp(-w * Rz * Rz);

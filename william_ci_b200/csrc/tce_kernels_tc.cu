@@ -472,8 +472,8 @@ __global__ void __launch_bounds__(256, 2) k_quartets_r1_tc(DevSys S, SArgs A)
                                 for (int i = 0; i < 2; ++i) {
                                     const int k = 8 * (g0 + t) + 2 * cq + i;
                                     const double t2 = tn[k] * tn[k];
-                                    const double D2 = 1.0 / (pq_ + ps * t2);
-                                    const double w = pq_ * t2 * D2, rs = PI_D * sqrt(D2);
+                                    const double rr = rsqrt(pq_ + ps * t2), D2 = rr * rr;
+                                    const double w = pq_ * t2 * D2, rs = PI_D * rr;
                                     double gy[NN + 1], gz[NN + 1];
                                     gy[0] = (Ry == 0.0) ? rs : rs * exp(-w * Ry * Ry);
                                     gz[0] = (Rz == 0.0) ? rs : rs * exp(-w * Rz * Rz);

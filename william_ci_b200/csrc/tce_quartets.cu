@@ -357,8 +357,8 @@ __device__ void process_batch(const DevSys &S, const RuleView &Rv, const QCtx &Q
                 const double *Ek = S.ecoef + Q.Uk.e_off + (long long)pq.y * nreal * (lsC + 1) * (lsD + 1) * TCE_ECO;
                 for (int k = lane; k < kn; k += 32) {
                     double t = Rv.t[k0 + k], t2 = t * t;
-                    double D2 = 1.0 / (pp_ * qq + (pp_ + qq) * t2);
-                    double w = pp_ * qq * t2 * D2, rs = PI_D * sqrt(D2);
+                    const double rr = rsqrt(pp_ * qq + (pp_ + qq) * t2), D2 = rr * rr;
+                    double w = pp_ * qq * t2 * D2, rs = PI_D * rr;
                     for (int dr = 0; dr < nreal; ++dr) {
                         int d = ndp + dr;
                         double Rr = Pb.cen[d] - (Pk.cen[d] + Q.Tsh[d]);
@@ -421,11 +421,26 @@ __device__ void process_batch(const DevSys &S, const RuleView &Rv, const QCtx &Q
                         rw[d] = (d < ndp) ? rowp + ((size_t)d * ncomb + cm) * RS
                                           : b.realb + ((size_t)(d - ndp) * cstride + cm) * RS;
                     }
-                    for (int k = sub; k < kn; k += G) {
-                        const double prod = rw[0][k] * rw[1][k] * rw[2][k];
-                        vK = fma(Rv.wk[k0 + k], prod, vK);
-                        if (judge) vG = fma(Rv.wg[k0 + k], prod, vG);
+                    // two partial sums per estimate: shorter dependent FMA chains
+                    double vK1 = 0.0, vG1 = 0.0;
+                    int k = sub;
+                    for (; k + G < kn; k += 2 * G) {
+                        const double p0 = rw[0][k] * rw[1][k] * rw[2][k];
+                        const double p1 = rw[0][k + G] * rw[1][k + G] * rw[2][k + G];
+                        vK = fma(Rv.wk[k0 + k], p0, vK);
+                        vK1 = fma(Rv.wk[k0 + k + G], p1, vK1);
+                        if (judge) {
+                            vG = fma(Rv.wg[k0 + k], p0, vG);
+                            vG1 = fma(Rv.wg[k0 + k + G], p1, vG1);
+                        }
                     }
+                    if (k < kn) {
+                        const double p0 = rw[0][k] * rw[1][k] * rw[2][k];
+                        vK = fma(Rv.wk[k0 + k], p0, vK);
+                        if (judge) vG = fma(Rv.wg[k0 + k], p0, vG);
+                    }
+                    vK += vK1;
+                    vG += vG1;
                 }
                 for (int o = G >> 1; o > 0; o >>= 1) {
                     vK += __shfl_xor_sync(0xffffffffu, vK, o);
