@@ -473,6 +473,7 @@ def named_shape_stage(name, flush, steps=5):
     info = eng.info()
     _, lg, _ = learned_grid_setup(eng, sysm, name, n_train=cfg["train"])
     eng.set_shard(0, cfg["shard"])
+    lg["autotune"] = eng.lg_autotune(2)           # CUDA-core or tensor-core rows per generic list
     sh = eng.shard_items()
     Q = eng.schwarz()
     first = np.array([f for f, _ in eng.shells()])

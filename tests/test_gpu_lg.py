@@ -411,3 +411,30 @@ def test_every_all_s_tile_shape_gives_the_same_jk(chain16_lg):
         assert np.abs(J - J0).max() <= 1e-12 * scale and np.abs(K - K0).max() <= 1e-12 * scale, shape
     for i in alls:
         eng.lg_set_list_form(i, 1)
+
+
+@pytest.mark.parametrize("name,ncell", [("h2_sheet", (2, 2, 1)), ("li_cube", (2, 2, 2))])
+def test_tensor_core_rows_in_2d_and_3d(systems, name, ncell):
+    """The generic kernel's rows on the FP64 tensor cores for two and three
+    periodic directions (one tile pass per direction), set by hand on every
+    generic learned-grid list: J/K equal the CUDA-core rows' to 1e-12 of the
+    density scale."""
+    from william_ci_b200.engine import TCE_METHOD_LEARNED
+    sysm = systems(name, ncell)
+    eng = _lg_engine(sysm)
+    net, _, _ = _trained(eng, sysm, n_train=3000)
+    eng.lg_predict_rules(net)
+    eng.set_method(TCE_METHOD_LEARNED)
+    P = random_density(sysm.nbas, 10) * 0.05
+    scale = np.abs(P).sum()
+    eng.direct_JK(P)                     # the judge's rejects move to the plain list
+    gen = [i for i, w in enumerate(eng.lg_lists()) if w["kind"] == 0]
+    assert gen
+    out = {}
+    for form in (0, 1):
+        for i in gen:
+            eng.lg_set_list_form(i, form)
+        out[form] = eng.direct_JK(P)
+    for a, b in zip(out[0], out[1]):
+        assert np.abs(a - b).max() <= 1e-12 * scale
+    eng.close()

@@ -520,7 +520,9 @@ int lg_rebuild_lists(Handle *h)
 // kernel (the all-s kernel in each of its tile shapes, TCE_TC_SHAPES)
 static int lg_nforms(const Handle *h, const Handle::LgList &w)
 {
-    if (h->ndp != 1 || (w.nq != 32 && w.nq != 64)) return 1;
+    if (w.nq != 32 && w.nq != 64) return 1;
+    if (w.kind == 0) return 2;               // the generic kernel's rows: every ndp
+    if (h->ndp != 1) return 1;
     return w.kind == 1 ? 1 + tce_tc_shapes_s(w.nq) : 2;
 }
 
@@ -529,7 +531,7 @@ static bool lg_tc_available(const Handle *h, const Handle::LgList &w) { return l
 static int lg_tc_default(const Handle *h, const Handle::LgList &w)
 {
     if (!lg_tc_available(h, w) || w.fp32) return 0;
-    if (w.kind == 0) return w.nq == 64 ? 1 : 0;
+    if (w.kind == 0) return (h->ndp == 1 && w.nq == 64) ? 1 : 0;
     if (w.kind == 1) return 1;
     return w.nq == 32 ? 1 : 0;
 }

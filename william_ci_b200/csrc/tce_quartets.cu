@@ -163,10 +163,11 @@ __device__ __forceinline__ void tce_dmma(double &d0, double &d1, double a, doubl
                  : "d"(a), "d"(b));
 }
 
-// The rows of row_dot for a batch, one periodic direction, on the FP64
-// tensor cores: the batch's nb * R rows (primitive quartet x power
+// The rows of row_dot for a batch and periodic direction d on the FP64 tensor
+// cores: the batch's nb * ncomb rows of direction d (primitive quartet x power
 // combination) in chunks of 32 are the A operand (32 x N, F = Re[G_n H_n
-// e^{i n phi}]), the rule's T table the B operand (N x 32 nodes per pass);
+// e^{i n phi}]), the rule's T table of direction d the B operand (N x 32
+// nodes per pass);
 // mma.sync.m8n8k4 per 8 x 8 tile and step of four orders.  Lane l builds the
 // A fragments of rows 8 m + l/4 (m = 0..3) at order 4 s + l%4, cos and sin
 // of n phi by the three-term recurrence in steps of four (re-seeded every 32
@@ -175,15 +176,20 @@ __device__ __forceinline__ void tce_dmma(double &d0, double &d1, double a, doubl
 // as row_dot: rows[r * 33 + x] = sgn I_r(t_{8 g0c + x}).
 template <int NQ>
 __device__ void tc_rows(const DevSys &S, const RuleView &Rv, const QCtx &Q, int nb, const WarpBuf &b, int lane,
-                        int g0c)
+                        int g0c, int d)
 {
     constexpr int RS = 32 + 1;
     const int rq = lane >> 2, cq = lane & 3;
-    const int lsA = Q.lsA, lsB = Q.lsB, lsC = Q.lsC, lsD = Q.lsD, R = Q.R;
+    const int lsA = Q.lsA, lsB = Q.lsB, lsC = Q.lsC, lsD = Q.lsD, R = Q.R, nd = Q.ncomb;
     const int nppb = Q.Ub.npp, nppk = Q.Uk.npp;
-    const int nrows = nb * R;
-    const double *T = Rv.T;
-    const int *gm = Rv.gmax;
+    const int nrows = nb * nd;                 // the batch's rows of direction d
+    const double *T = Rv.T + (size_t)d * Rv.strideD;
+    const int *gm = Rv.gmax + d * TCE_MAXG;
+    // row rr = (primitive quartet p, combination cmb) of direction d -> its place in b.rows
+    auto orow = [&](int rr) {
+        const int p = rr / nd;
+        return p * R + d * nd + (rr - p * nd);
+    };
     for (int r0 = 0; r0 < nrows; r0 += 32) {
         int goff[4], hoff[4], nmr[4];
         double sg[4];
@@ -195,17 +201,17 @@ __device__ void tc_rows(const DevSys &S, const RuleView &Rv, const QCtx &Q, int 
             goff[m] = hoff[m] = 0;
             sg[m] = 0.0;
             if (r < nrows) {
-                const int p = r / R, cmb = r - p * R;
+                const int p = r / nd, cmb = r - p * nd;
                 const int ia = cmb % (lsA + 1), t1 = cmb / (lsA + 1);
                 const int ib = t1 % (lsB + 1), t2 = t1 / (lsB + 1);
                 const int ic = t2 % (lsC + 1), id = t2 / (lsC + 1);
                 const int2 pq = b.qlist[p];
                 const PairPrim &Pb = S.pp[Q.Ub.pp_off + pq.x];
                 const PairPrim &Pk = S.pp[Q.Uk.pp_off + pq.y];
-                nmr[m] = Pb.N[0] < Pk.N[0] ? Pb.N[0] : Pk.N[0];
-                goff[m] = (int)((((long long)ia * (lsB + 1) + ib) * 2 + 0) * Q.Ub.Nlen * nppb + pq.x);
-                hoff[m] = (int)((((long long)ic * (lsD + 1) + id) * 2 + 1) * Q.Uk.Nlen * nppk + pq.y);
-                sg[m] = pow(S.a[0], -(double)(ia + ib + ic + id));
+                nmr[m] = Pb.N[d] < Pk.N[d] ? Pb.N[d] : Pk.N[d];
+                goff[m] = (int)(((((long long)d * (lsA + 1) + ia) * (lsB + 1) + ib) * 2 + 0) * Q.Ub.Nlen * nppb + pq.x);
+                hoff[m] = (int)(((((long long)d * (lsC + 1) + ic) * (lsD + 1) + id) * 2 + 1) * Q.Uk.Nlen * nppk + pq.y);
+                sg[m] = pow(S.a[d], -(double)(ia + ib + ic + id));
                 nmax = nmr[m] > nmax ? nmr[m] : nmax;
             }
         }
@@ -214,8 +220,8 @@ __device__ void tc_rows(const DevSys &S, const RuleView &Rv, const QCtx &Q, int 
         auto phase = [&](int m) {
             const int r = r0 + 8 * m + rq;
             if (r >= nrows) return 0.0;
-            const int2 pq = b.qlist[r / R];
-            return S.a[0] * (S.pp[Q.Ub.pp_off + pq.x].cen[0] - (S.pp[Q.Uk.pp_off + pq.y].cen[0] + Q.Tsh[0]));
+            const int2 pq = b.qlist[r / nd];
+            return S.a[d] * (S.pp[Q.Ub.pp_off + pq.x].cen[d] - (S.pp[Q.Uk.pp_off + pq.y].cen[d] + Q.Tsh[d]));
         };
         const double2 *Gv = S.vec + Q.Ub.vec_off, *Hv = S.vec + Q.Uk.vec_off;
         {
@@ -294,7 +300,8 @@ __device__ void tc_rows(const DevSys &S, const RuleView &Rv, const QCtx &Q, int 
 #pragma unroll
                 for (int t = 0; t < 4; ++t)
 #pragma unroll
-                    for (int i = 0; i < 2; ++i) b.rows[(size_t)r * RS + 8 * t + 2 * cq + i] = acc[8 * m + 2 * t + i] * sg[m];
+                    for (int i = 0; i < 2; ++i)
+                        b.rows[(size_t)orow(r) * RS + 8 * t + 2 * cq + i] = acc[8 * m + 2 * t + i] * sg[m];
             }
         }
     }
@@ -323,8 +330,8 @@ __device__ void process_batch(const DevSys &S, const RuleView &Rv, const QCtx &Q
         bool rows_done = false;
         // tensor-core rows when the launch asks for them (32- and 64-node rules)
         if constexpr (RO && (NQ == 32 || NQ == 64)) {
-            if (tc && ndp == 1) {
-                tc_rows<NQ>(S, Rv, Q, nb, b, lane, g0c);
+            if (tc) {
+                for (int d = 0; d < ndp; ++d) tc_rows<NQ>(S, Rv, Q, nb, b, lane, g0c, d);
                 rows_done = true;
             }
         }
