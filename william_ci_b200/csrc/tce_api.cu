@@ -124,7 +124,9 @@ int route(const Handle *h, const int4 &q)
     }
     if (cls == 0 && sp && (h->nq == 32 || h->nq == 40)) return 1 * 16;
     if (sp && tce_r1_supported(h->ndp, h->nq, cls)) return 2 * 16 + cls;
-    return 0;
+    // generic kernel: one list per number of shells above p, each launched with
+    // its own largest block (buffers sized for the list, not for (dd|dd))
+    return (l[0] > 1) + (l[1] > 1) + (l[2] > 1) + (l[3] > 1);
 }
 
 // split a list of quartets (most expensive first) into per-kernel device lists
@@ -142,6 +144,10 @@ int make_lists(Handle *h, const std::vector<int4> &items)
         w.kind = key / 16;
         w.cls = key % 16;
         w.n = (long long)by[key].size();
+        for (const int4 &q : by[key]) {
+            w.max_ncomb = std::max(w.max_ncomb, ncomb_of(h, q.x, q.y, q.z, q.w));
+            w.max_ncq = std::max(w.max_ncq, h->sh_n[q.x] * h->sh_n[q.y] * h->sh_n[q.z] * h->sh_n[q.w]);
+        }
         int s = upload(h, &w.d, by[key]);
         if (s) return s;
         h->nitems_shard += w.n;
@@ -648,8 +654,8 @@ static int jk_body(Handle *h, const double *dP, double *dJ, double *dK, cudaStre
             a.P = dP;
             a.J = dJ;
             a.K = dK;
-            a.max_ncomb = h->max_ncomb;
-            a.max_ncq = h->max_ncq;
+            a.max_ncomb = w.max_ncomb;
+            a.max_ncq = w.max_ncq;
             a.fixed_gmax = h->d_gmax;
             a.num_sms = h->num_sms;
             a.use_tc = h->use_tc && h->nq == 64;   // tensor-core rows measured faster with 64 nodes only

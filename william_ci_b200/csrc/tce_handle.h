@@ -52,7 +52,8 @@ struct Handle {
     // the J/K work of this shard, one list per kernel: kind 0 generic
     // (k_quartets), 1 all-s (k_quartets_s), 2 one-periodic-direction s/p class
     // `cls` (k_quartets_r1)
-    struct WorkList { int kind, cls; int4 *d = nullptr; long long n = 0; };
+    // (generic lists: cls = shells above p, 0..4; max_ncomb / max_ncq of the list's quartets)
+    struct WorkList { int kind, cls; int4 *d = nullptr; long long n = 0; int max_ncomb = 1, max_ncq = 1; };
     std::vector<WorkList> lists;
     long long nitems_shard = 0;
     int *d_tnmax = nullptr;
@@ -83,7 +84,15 @@ struct Handle {
     // tc: kernel form chosen by tce_lg_autotune (-1: the default rule of
     // lg_tc_default, 0: CUDA cores, 1: FP64 tensor cores); tc_choice keeps the
     // choices per list key across rebuilds
-    struct LgList { int kind, cls, nq, fp32, tc = -1; int4 *d = nullptr; int *rule = nullptr; long long n = 0; };
+    // generic lists (kind 0): cls = shells above p (0..4), and the largest
+    // combination count and block of the list's quartets size its buffers
+    struct LgList {
+        int kind, cls, nq, fp32, tc = -1;
+        int4 *d = nullptr;
+        int *rule = nullptr;
+        long long n = 0;
+        int max_ncomb = 1, max_ncq = 1;
+    };
     std::vector<LgList> lg_lists;
     std::map<int, int> tc_choice;
     long long n_lg = 0, n_fp32 = 0;

@@ -391,6 +391,14 @@ static int lg_route(const Handle *h, const int4 &q)
     return 0;
 }
 
+// the generic kernel's lists by the number of shells above p (0..4): each list
+// launches with its own largest block and combination count, so that quartets
+// without d shells do not carry the per-warp buffers of (dd|dd)
+static int generic_size_class(const Handle *h, const int4 &q)
+{
+    return (h->sh_l[q.x] > 1) + (h->sh_l[q.y] > 1) + (h->sh_l[q.z] > 1) + (h->sh_l[q.w] > 1);
+}
+
 static void fill_common(Handle *h, QuartetHostArgs &a)
 {
     a.max_ncomb = h->max_ncomb;
@@ -449,7 +457,8 @@ int lg_rebuild_lists(Handle *h)
         const int r = h->item_rule[(size_t)i];
         const int4 &q = h->items_host[(size_t)i];
         if (r >= 0 && r < h->lg_nrules) {
-            const int route = lg_route(h, q);
+            int route = lg_route(h, q);
+            if (route == 0) route = generic_size_class(h, q);
             const bool f32 = h->fp32_thr > 0.0 && route >= 16 && h->ndp == 1 && h->d_rule_T32 &&
                              h->Qsh[q.x + (size_t)h->nsh * q.y] * h->Qsh[q.z + (size_t)h->nsh * q.w] < h->fp32_thr;
             const int key = (route * 2 + (h->rules_host[r].nq == 64 ? 1 : 0)) * 2 + (f32 ? 1 : 0);
@@ -496,6 +505,13 @@ int lg_rebuild_lists(Handle *h)
             if (tcit != h->tc_choice.end()) w.tc = tcit->second;
         }
         w.n = (long long)lg[key].size();
+        if (w.kind == 0) {
+            w.max_ncomb = w.max_ncq = 1;
+            for (const int4 &q : lg[key]) {
+                w.max_ncomb = std::max(w.max_ncomb, ncomb_of(h, q.x, q.y, q.z, q.w));
+                w.max_ncq = std::max(w.max_ncq, h->sh_n[q.x] * h->sh_n[q.y] * h->sh_n[q.z] * h->sh_n[q.w]);
+            }
+        }
         if ((s = upload(h, &w.d, lg[key]))) return s;
         if ((s = upload(h, &w.rule, rl[key]))) return s;
         h->lg_lists.push_back(w);
@@ -551,6 +567,8 @@ static int lg_launch_list(Handle *h, const Handle::LgList &w, const QuartetHostA
         QuartetHostArgs b = a;
         b.method = TCE_METHOD_LEARNED;
         b.dict_nq = w.nq;
+        b.max_ncomb = w.max_ncomb;
+        b.max_ncq = w.max_ncq;
         b.items = w.d;
         b.nitems = (int)w.n;
         b.item_rule = w.rule;
