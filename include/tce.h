@@ -153,6 +153,18 @@ int tce_schwarz(void *handle, double *Q);
  * tce_stored_jk. */
 int tce_eri_stored(void *handle, int64_t eri_size, double *eri);
 
+/* The two-electron part of the TREXIO export (trexio_conv_integrals,
+ * trexio_conv.f90:267-359): from the full stored integrals on the device
+ * (tce_eri_stored with sao = 0; the reference reads a full nbas^4 array, so
+ * SAO mode has no export), the entries it writes, in its order: (i, j, k, l)
+ * with i fastest, then j, k, l, kept when i >= j, (i == j => k >= l) and
+ * ERI(i, k, j, l) != 0; index[4e..4e+3] = (i, j, k, l) 1-based, value[e] =
+ * ERI(i, k, j, l).  *count = the stream's length; the first min(count, cap)
+ * entries are written (cap 0: count only).  The caller passes them to
+ * trexio_write_ao_2e_int_eri in chunks, as the reference does with BUFSIZE
+ * 10000.  libtrexio itself is not part of this library. */
+int tce_trexio_eri(void *handle, int64_t cap, int32_t *index, double *value, int64_t *count);
+
 /* J and K from the device-resident stored ERIs (rows < ERI_size filled).
  * Replaces hartree_exchange_potential (hartree_exchange_potential.f90:30). */
 int tce_stored_jk(void *handle, const double *P, double *J, double *K);

@@ -179,3 +179,22 @@ def test_fast_quad_self_check_vs_oracle(systems, name, ncell):
     dref = max(np.abs(o32.shell_block(*q, mode=0) - o128.shell_block(*q, mode=0)).max() for q in sample)
     assert abs(d - dref) <= 1e-12, (d, dref)
     assert keep == (dref <= 1e-10)
+
+
+def test_trexio_stream_from_the_device(systems):
+    """tce_trexio_eri: the entry stream of the TREXIO export computed on the
+    device from the full stored integrals equals the reference loop run on the
+    same array (indices and values exactly), and the array equals the
+    oracle's full integrals to 1e-10."""
+    import pyoracle as po
+    from william_ci_b200 import trexio_out as TX
+    from william_ci_b200.engine import Engine
+    sysm = systems("h_chain64", (4, 1, 1))
+    with Engine(sysm, sao=False) as eng:
+        E = eng.ERI_integral_toroidal()
+        idx, val = eng.trexio_eri()
+    ridx, rval = TX.reference_stream(E)
+    assert np.array_equal(idx, ridx)
+    assert np.array_equal(val, rval)
+    Eo, _ = po.Oracle(sysm, sao=False).eri_stored()
+    assert np.abs(E - Eo).max() < 1e-10

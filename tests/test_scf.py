@@ -51,3 +51,41 @@ def test_direct_and_stored_jk_give_the_same_rhf_energy(which):
     assert r1.converged and r2.converged
     assert abs(r1.energy - r2.energy) < 1e-10
     assert r1.iterations == r2.iterations
+
+
+def test_trexio_chunks_follow_the_reference_writer():
+    """eri_chunks cuts an entry stream into the reference's buffered writes:
+    full buffers at offsets 0, B, 2B, ...; the last partial buffer passed with
+    count B, its tail left from the buffer before (trexio_conv.f90:326-357)."""
+    from william_ci_b200 import trexio_out as TX
+    n, B = 25, 10
+    idx = np.arange(4 * n, dtype=np.int32).reshape(n, 4)
+    val = np.arange(n, dtype=np.float64) + 0.5
+    calls = TX.eri_chunks(idx, val, bufsize=B)
+    assert [c[0] for c in calls] == [0, 10, 20] and all(c[1] == B for c in calls)
+    np.testing.assert_array_equal(calls[1][3], val[10:20])
+    last = calls[2][3]
+    np.testing.assert_array_equal(last[:5], val[20:25])
+    np.testing.assert_array_equal(last[5:], val[15:20])     # stale entries of the previous buffer
+    assert len(TX.eri_chunks(idx[:20], val[:20], bufsize=B)) == 2
+
+
+def test_trexio_reference_stream_on_the_oracle_integrals():
+    """The stream restatement on the oracle's full integrals of the 2-cell ring:
+    the loop's conditions and order."""
+    from william_ci_b200 import trexio_out as TX
+    sysm = make_system("h2_ring")
+    o = po.Oracle(sysm, sao=False)
+    E, _ = o.eri_stored()
+    idx, val = TX.reference_stream(E)
+    n = sysm.nbas
+    expect = []
+    for l in range(n):
+        for k in range(n):
+            for j in range(n):
+                for i in range(n):
+                    if (i == j and k < l) or i < j or E[i, k, j, l] == 0.0:
+                        continue
+                    expect.append((i + 1, j + 1, k + 1, l + 1, E[i, k, j, l]))
+    assert [tuple(r) for r in idx] == [e[:4] for e in expect]
+    np.testing.assert_array_equal(val, [e[4] for e in expect])

@@ -1239,6 +1239,34 @@ int tce_eri_stored(void *handle, int64_t eri_size, double *eri)
     return TCE_OK;
 }
 
+int tce_trexio_eri(void *handle, int64_t cap, int32_t *index, double *value, int64_t *count)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h || !count || cap < 0 || (cap > 0 && (!index || !value))) return fail(h, TCE_ERR_ARG, "bad argument");
+    if (!h->d_eri || h->eri_size != h->nbas)
+        return fail(h, TCE_ERR_STATE, "needs the full stored integrals: tce_eri_stored with sao = 0 first");
+    int32_t *d_idx = nullptr;
+    double *d_val = nullptr;
+    int s;
+    if (cap > 0) {
+        if ((s = dalloc(h, &d_idx, (size_t)cap * 4))) return s;
+        if ((s = dalloc(h, &d_val, (size_t)cap))) return s;
+    }
+    long long cnt = 0;
+    if (tce_trexio_stream(h->d_eri, h->nbas, cap, d_idx, d_val, &cnt, h->st) != TCE_OK)
+        return fail(h, TCE_ERR_CUDA, "integral stream kernels failed");
+    *count = cnt;
+    const long long m = std::min<long long>(cnt, cap);
+    if (m > 0) {
+        CK(h, cudaMemcpyAsync(index, d_idx, sizeof(int32_t) * 4 * (size_t)m, cudaMemcpyDeviceToHost, h->st));
+        CK(h, cudaMemcpyAsync(value, d_val, sizeof(double) * (size_t)m, cudaMemcpyDeviceToHost, h->st));
+        CK(h, cudaStreamSynchronize(h->st));
+    }
+    dfree(h, d_idx);
+    dfree(h, d_val);
+    return TCE_OK;
+}
+
 int tce_stored_jk(void *handle, const double *P, double *J, double *K)
 {
     Handle *h = static_cast<Handle *>(handle);

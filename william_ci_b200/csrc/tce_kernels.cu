@@ -599,3 +599,68 @@ int tce_sort_items(const DevSys &S, const int4 *items, long long n, int4 *sorted
     cudaFree(idx);
     return rc;
 }
+
+// ---------------------------------------------------------------------------
+// The two-electron integral stream of trexio_conv_integrals
+// (trexio_conv.f90:267-359): over (i, j, k, l), i fastest, then j, k, l, the
+// entries with i >= j, (i == j => k >= l) and ERI(i, k, j, l) != 0 of the full
+// nbas^4 array, in that order, as (i, j, k, l) 1-based and the value.
+// ---------------------------------------------------------------------------
+#include <thrust/copy.h>
+#include <thrust/iterator/counting_iterator.h>
+
+struct TrexioKeep {
+    const double *eri;
+    long long n;
+    __host__ __device__ bool operator()(long long t) const
+    {
+        const long long i = t % n, r1 = t / n, j = r1 % n, r2 = r1 / n, k = r2 % n, l = r2 / n;
+        if (i < j) return false;
+        if (i == j && k < l) return false;
+        return eri[i + n * (k + n * (j + n * l))] != 0.0;
+    }
+};
+
+__global__ void k_trexio_pack(const double *__restrict__ eri, long long n, const long long *__restrict__ pos,
+                              long long cnt, int32_t *index, double *value)
+{
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= cnt) return;
+    const long long t = pos[e];
+    const long long i = t % n, r1 = t / n, j = r1 % n, r2 = r1 / n, k = r2 % n, l = r2 / n;
+    index[4 * e] = (int32_t)(i + 1);
+    index[4 * e + 1] = (int32_t)(j + 1);
+    index[4 * e + 2] = (int32_t)(k + 1);
+    index[4 * e + 3] = (int32_t)(l + 1);
+    value[e] = eri[i + n * (k + n * (j + n * l))];
+}
+
+int tce_trexio_stream(const double *d_eri, long long n, long long cap, int32_t *d_index, double *d_value,
+                      long long *count, cudaStream_t st)
+{
+    const long long tot = n * n * n * n;
+    long long *pos = nullptr;
+    if (cudaMalloc(&pos, sizeof(long long) * (size_t)(tot > 0 ? tot / 2 + n * n + 1 : 1)) != cudaSuccess)
+        return TCE_ERR_NOMEM;
+    long long cnt = 0;
+    int rc = TCE_OK;
+    try {
+        auto pol = thrust::cuda::par.on(st);
+        thrust::counting_iterator<long long> first(0);
+        long long *end = thrust::copy_if(pol, first, first + tot, pos, TrexioKeep{d_eri, n});
+        cnt = (long long)(end - pos);
+    } catch (...) {
+        rc = TCE_ERR_CUDA;
+    }
+    if (rc == TCE_OK) {
+        *count = cnt;
+        const long long m = cnt < cap ? cnt : cap;
+        if (m > 0 && d_index && d_value) {
+            k_trexio_pack<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(d_eri, n, pos, m, d_index, d_value);
+            if (cudaGetLastError() != cudaSuccess) rc = TCE_ERR_CUDA;
+        }
+        if (rc == TCE_OK && cudaStreamSynchronize(st) != cudaSuccess) rc = TCE_ERR_CUDA;
+    }
+    cudaFree(pos);
+    return rc;
+}

@@ -115,6 +115,11 @@ int tce_launch_sym_fill(int nf, int fpuc, const int *ncl, double *eri, cudaStrea
 // count among them.
 int tce_sort_items(const DevSys &S, const int4 *items, long long n, int4 *sorted, double *cost_sorted,
                    int *d_max_ncomb, cudaStream_t st);
+// The integral stream of trexio_conv_integrals from the full nbas^4 stored
+// integrals on the device: *count entries; the first min(count, cap) packed as
+// 1-based (i, j, k, l) into d_index[4 e ..] and their values into d_value.
+int tce_trexio_stream(const double *d_eri, long long n, long long cap, int32_t *d_index, double *d_value,
+                      long long *count, cudaStream_t st);
 int tce_launch_count_work(const DevSys &S, const int4 *items, int nitems, int prim_screen, const int *tnmax,
                           unsigned long long *nprim, double *flops, cudaStream_t st, const int *item_rule = nullptr,
                           const RuleDev *rules = nullptr, const int *rule_tnmax = nullptr);

@@ -47,7 +47,8 @@ EXPORTS = ["tce_create", "tce_destroy", "tce_last_error", "tce_get_info", "tce_s
            "tce_lg_autotune", "tce_lg_lists", "tce_dfjk_create", "tce_dfjk", "tce_dfjk_destroy",
            "tce_dfjk_last_error", "tce_ao_to_kmo", "tce_shard_items", "tce_lg_list_profile",
            "tce_df_create", "tce_df_destroy", "tce_df_last_error", "tce_df_integrals", "tce_df_fitted", "tce_dfmp2",
-           "tce_gk_rule", "tce_lg_dictionary", "tce_lg_setup", "tce_lg_set_list_form"]
+           "tce_gk_rule", "tce_lg_dictionary", "tce_lg_setup", "tce_lg_set_list_form",
+           "tce_trexio_eri"]
 
 TCE_METHOD_FIXED, TCE_METHOD_LEARNED, TCE_METHOD_PLAIN = 0, 1, 2
 TCE_NFEAT = 12
@@ -141,6 +142,7 @@ def lib():
         L.tce_lg_lists.argtypes = [C.c_void_p, _ip, _ip]
         L.tce_lg_list_profile.argtypes = [C.c_void_p, C.c_int32, _ip, _dp, _dp]
         L.tce_lg_set_list_form.argtypes = [C.c_void_p, C.c_int32, C.c_int32]
+        L.tce_trexio_eri.argtypes = [C.c_void_p, C.c_int64, _ip, _dp, _lp]
         L.tce_ao_to_kmo.argtypes = [C.c_void_p, _dp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _dp]
         L.tce_dfjk_create.argtypes = [C.c_int32, C.c_int32, C.c_int32, _ip, _dp, _dp, C.POINTER(C.c_void_p)]
         L.tce_dfjk.argtypes = [C.c_void_p, _dp, _dp, _dp]
@@ -282,6 +284,17 @@ class Engine:
         q = np.array([S1, S2, S3, S4], dtype=np.int32)
         _check(lib().tce_shell_block_noalloc(self.h, _i(q), int(mode), _d(blk)), self.h)
         return blk.reshape(n, order="F")
+
+    def trexio_eri(self):
+        """The integral stream of the TREXIO export (tce_trexio_eri) from the full
+        stored integrals (run ERI_integral_toroidal with sao=False first):
+        indices (count, 4) 1-based (i, j, k, l) and values ERI(i, k, j, l)."""
+        n = C.c_int64()
+        _check(lib().tce_trexio_eri(self.h, 0, None, None, C.byref(n)), self.h)
+        idx = np.zeros(4 * max(n.value, 1), dtype=np.int32)
+        val = np.zeros(max(n.value, 1))
+        _check(lib().tce_trexio_eri(self.h, n.value, _i(idx), _d(val), C.byref(n)), self.h)
+        return idx[:4 * n.value].reshape(n.value, 4), val[:n.value]
 
     def ERI_integral_toroidal(self) -> np.ndarray:
         n = self.nbas
