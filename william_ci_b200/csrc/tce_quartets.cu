@@ -1061,6 +1061,10 @@ int tce_launch_quartets(const DevSys &S, const QuartetHostArgs &h, cudaStream_t 
         if (per < 1) per = 1;
         long long grid = (long long)nsm * per;
         if (grid * warps > h.scratch_warps) grid = h.scratch_warps / warps;
+        // a list of known length takes no more warps than it has quartets: the
+        // plain list runs next to the learned-grid kernels, and its idle blocks
+        // would hold the registers and shared memory they need
+        if (!h.nitems_dev && h.nitems > 0) grid = std::min<long long>(grid, (h.nitems + warps - 1) / warps);
         if (grid < 1) return TCE_ERR_NOMEM;
         k_plain<<<(unsigned)grid, 32 * warps, smem, st>>>(S, A);
         e = cudaGetLastError();
