@@ -653,12 +653,12 @@ def main():
     tune = eng.lg_autotune(3) if world == 1 else None
     if tune is not None:
         names = {0: "generic", 1: "all-s", 2: "one-p"}
-        shapes = {1: "16x32", 2: "32x16", 3: "16x16", 4: "8x64"}
+        shapes = {1: {1: "16x32", 2: "32x16", 3: "16x16", 4: "8x64", 5: "8x32"}, 2: {1: "8x32", 2: "16x32", 3: "8x64"}}
 
         def form(w):
             if not w["tc"]:
                 return "CUDA cores"
-            return "tensor cores" + (" %s tiles per pass" % shapes[w["tc"]] if w["kind"] == 1 else "")
+            return "tensor cores" + (" %s tiles per pass" % shapes[w["kind"]][w["tc"]] if w["kind"] in shapes else "")
         tune["lists"] = ["%s cls%d nq%d%s: %s, %d quartets" % (names[w["kind"]], w["cls"], w["nq"],
                                                                 " fp32" if w["fp32"] else "", form(w), w["n"])
                          for w in eng.lg_lists()]

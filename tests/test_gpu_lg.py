@@ -386,7 +386,8 @@ def test_learned_grid_setup_from_the_c_abi(systems):
 
 def test_every_all_s_tile_shape_gives_the_same_jk(chain16_lg):
     """The all-s tensor-core kernel in each tile shape the autotuner can pick
-    (16 x 32, 32 x 16, 16 x 16, 8 x 64 primitive quartets x nodes per pass),
+    (16 x 32, 32 x 16, 16 x 16, 8 x 64, 8 x 32 primitive quartets x nodes per
+    pass),
     set by hand on every all-s list: J/K equal the CUDA-core kernel's to 1e-12
     of the density scale."""
     from william_ci_b200.engine import TCE_METHOD_LEARNED
@@ -404,12 +405,43 @@ def test_every_all_s_tile_shape_gives_the_same_jk(chain16_lg):
     for i in alls:
         eng.lg_set_list_form(i, 0)
     J0, K0 = eng.direct_JK(P)
-    for shape in (1, 2, 3, 4):
+    for shape in (1, 2, 3, 4, 5):
         for i in alls:
             eng.lg_set_list_form(i, shape)
         J, K = eng.direct_JK(P)
         assert np.abs(J - J0).max() <= 1e-12 * scale and np.abs(K - K0).max() <= 1e-12 * scale, shape
     for i in alls:
+        eng.lg_set_list_form(i, 1)
+
+
+def test_every_one_p_tile_shape_gives_the_same_jk(chain16_lg):
+    """The one-p tensor-core kernel (both power combinations per step loop,
+    the real directions by moments) in each tile shape the autotuner can pick
+    (8 x 32, 16 x 32 and, for 64-node rules, 8 x 64 primitive quartets x nodes
+    per pass), set by hand on every one-p list: J/K equal the CUDA-core
+    kernel's to 1e-12 of the density scale, with no more judge rejects."""
+    from william_ci_b200.engine import TCE_METHOD_LEARNED
+    sysm, eng, net = chain16_lg
+    P = random_density(sysm.nbas, 11) * 0.05
+    scale = np.abs(P).sum()
+    eng.set_method(TCE_METHOD_LEARNED)
+    eng.set_fp32_threshold(0.0)
+    eng.set_graph(False)
+    eng.lg_predict_rules(net)
+    eng.direct_JK(P)                     # the judge's rejects move to the plain list
+    lists = eng.lg_lists()
+    onep = [(i, w["nq"]) for i, w in enumerate(lists) if w["kind"] == 2]
+    assert onep and {nq for _, nq in onep} == {32, 64}
+    for i, _ in onep:
+        eng.lg_set_list_form(i, 0)
+    J0, K0 = eng.direct_JK(P)
+    for shape in (1, 2, 3):
+        for i, nq in onep:
+            eng.lg_set_list_form(i, shape if shape <= (3 if nq == 64 else 2) else 1)
+        J, K = eng.direct_JK(P)
+        assert eng.lg_stats()["rejected"] == 0
+        assert np.abs(J - J0).max() <= 1e-12 * scale and np.abs(K - K0).max() <= 1e-12 * scale, shape
+    for i, _ in onep:
         eng.lg_set_list_form(i, 1)
 
 

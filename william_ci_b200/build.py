@@ -13,9 +13,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtce.so")
-SOURCES = ["tce_api.cu", "tce_kernels.cu", "tce_kernels_s.cu", "tce_kernels_slg.cu", "tce_kernels_tc.cu", "tce_quartets.cu", "tce_lg.cu", "tce_mp2.cu", "tce_onee.cu", "tce_dfjk.cu", "tce_kmo.cu", "tce_df.cu", "tce_lgsetup.cu"]
+SOURCES = ["tce_api.cu", "tce_kernels.cu", "tce_kernels_s.cu", "tce_kernels_slg.cu", "tce_kernels_tc.cu", "tce_kernels_sp2.cu", "tce_quartets.cu", "tce_lg.cu", "tce_mp2.cu", "tce_onee.cu", "tce_dfjk.cu", "tce_kmo.cu", "tce_df.cu", "tce_lgsetup.cu"]
 OBJDIR = os.path.join(HERE, "_build")
-HEADERS = ["tce_device.cuh", "tce_kernels.h", "tce_handle.h", "tce_kernels_s.cuh"]
+HEADERS = ["tce_device.cuh", "tce_kernels.h", "tce_handle.h", "tce_kernels_s.cuh", "tce_kernels_tc.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

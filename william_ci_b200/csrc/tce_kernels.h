@@ -92,9 +92,11 @@ int tce_launch_quartets_r1_lg(const DevSys &S, int cls, const SArgsHost &h, int 
 int tce_launch_quartets_s_tc(const DevSys &S, const SArgsHost &h, int nq, int shape, cudaStream_t st);
 // number of tile shapes of the all-s tensor-core kernel for nq-node rules (shapes 1..n)
 int tce_tc_shapes_s(int nq);
-// one-p s/p classes of one periodic direction, learned grid, tensor-core node
-// sums (k_quartets_r1_tc); cls as tce_launch_quartets_r1
-int tce_launch_quartets_r1_tc(const DevSys &S, int cls, const SArgsHost &h, int nq, cudaStream_t st);
+// s/p classes with one or two p shells of one periodic direction, learned
+// grid, tensor-core node sums (k_quartets_sp_tc) in tile shape
+// 1..tce_tc_shapes_sp(nq); cls: bit i set when shell i of (A, B | C, D) is p
+int tce_launch_quartets_sp_tc(const DevSys &S, int cls, const SArgsHost &h, int nq, int shape, cudaStream_t st);
+int tce_tc_shapes_sp(int nq);
 inline bool tce_r1_supported(int ndp, int nq, int cls)
 {
     return ndp == 1 && nq == 32 && cls >= 0 && cls < 16 && __builtin_popcount(cls) == 1;

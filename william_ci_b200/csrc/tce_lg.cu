@@ -366,8 +366,14 @@ static int ensure_plain(Handle *h)
     return TCE_OK;
 }
 
+// s/p lists with two p shells: their CUDA-core form (form 0) is the generic kernel
+static bool lg_generic_cuda_core(const Handle::LgList &w)
+{
+    return w.kind == 2 && __builtin_popcount(w.cls) >= 2;
+}
+
 // which kernel evaluates a learned-grid quartet: kind * 16 + cls (kind 1 all-s,
-// 2 one periodic direction with a single p shell in the reference component
+// 2 one periodic direction with one or two p shells in the reference component
 // order, 0 everything else)
 static int lg_route(const Handle *h, const int4 &q)
 {
@@ -387,7 +393,7 @@ static int lg_route(const Handle *h, const int4 &q)
                     if (h->lxyz[3 * (h->sh_first[S] + c) + d] != (c == d ? 1 : 0)) return 0;
     }
     if (cls == 0) return 16;
-    if (h->ndp == 1 && __builtin_popcount(cls) == 1) return 32 + cls;
+    if (h->ndp == 1 && __builtin_popcount(cls) <= 2) return 32 + cls;
     return 0;
 }
 
@@ -459,7 +465,9 @@ int lg_rebuild_lists(Handle *h)
         if (r >= 0 && r < h->lg_nrules) {
             int route = lg_route(h, q);
             if (route == 0) route = generic_size_class(h, q);
+            // (no FP32 form for two p shells: their CUDA-core form is the generic kernel)
             const bool f32 = h->fp32_thr > 0.0 && route >= 16 && h->ndp == 1 && h->d_rule_T32 &&
+                             __builtin_popcount(route & 15) <= 1 &&
                              h->Qsh[q.x + (size_t)h->nsh * q.y] * h->Qsh[q.z + (size_t)h->nsh * q.w] < h->fp32_thr;
             const int key = (route * 2 + (h->rules_host[r].nq == 64 ? 1 : 0)) * 2 + (f32 ? 1 : 0);
             lg[key].push_back(q);
@@ -505,7 +513,7 @@ int lg_rebuild_lists(Handle *h)
             if (tcit != h->tc_choice.end()) w.tc = tcit->second;
         }
         w.n = (long long)lg[key].size();
-        if (w.kind == 0) {
+        if (w.kind == 0 || lg_generic_cuda_core(w)) {
             w.max_ncomb = w.max_ncq = 1;
             for (const int4 &q : lg[key]) {
                 w.max_ncomb = std::max(w.max_ncomb, ncomb_of(h, q.x, q.y, q.z, q.w));
@@ -528,28 +536,30 @@ int lg_rebuild_lists(Handle *h)
 
 // Whether a learned-grid list has a tensor-core form (one periodic direction:
 // generic rows, all-s and one-p kernels) and which form it runs by default:
-// the all-s kernel on the tensor cores for FP64 quartets, the one-p kernel for
-// FP64 quartets with 32-node rules, the generic rows with 64-node rules (the
-// forms measured faster on the 64-cell chain); FP32-panel lists keep their
-// CUDA-core kernels unless tuned otherwise.
+// the all-s kernel on the tensor cores for FP64 quartets, the one-p kernel on
+// the tensor cores for every list (its FP64 tensor-core form is faster than
+// the FP32-panel CUDA-core kernel too), the generic rows with 64-node rules
+// (the forms measured faster on the 64-cell chain); the other FP32-panel
+// lists keep their CUDA-core kernels unless tuned otherwise.
 // kernel forms of a list: 0 the CUDA-core kernel, 1.. the FP64 tensor-core
-// kernel (the all-s kernel in each of its tile shapes, TCE_TC_SHAPES)
+// kernel (the all-s and one-p kernels in each of their tile shapes)
 static int lg_nforms(const Handle *h, const Handle::LgList &w)
 {
     if (w.nq != 32 && w.nq != 64) return 1;
     if (w.kind == 0) return 2;               // the generic kernel's rows: every ndp
     if (h->ndp != 1) return 1;
-    return w.kind == 1 ? 1 + tce_tc_shapes_s(w.nq) : 2;
+    return 1 + (w.kind == 1 ? tce_tc_shapes_s(w.nq) : tce_tc_shapes_sp(w.nq));
 }
 
 static bool lg_tc_available(const Handle *h, const Handle::LgList &w) { return lg_nforms(h, w) > 1; }
 
 static int lg_tc_default(const Handle *h, const Handle::LgList &w)
 {
-    if (!lg_tc_available(h, w) || w.fp32) return 0;
+    if (!lg_tc_available(h, w)) return 0;
+    if (w.kind == 2) return 1;
+    if (w.fp32) return 0;
     if (w.kind == 0) return (h->ndp == 1 && w.nq == 64) ? 1 : 0;
-    if (w.kind == 1) return 1;
-    return w.nq == 32 ? 1 : 0;
+    return 1;
 }
 
 static int lg_tc(const Handle *h, const Handle::LgList &w)
@@ -563,7 +573,7 @@ static int lg_tc(const Handle *h, const Handle::LgList &w)
 static int lg_launch_list(Handle *h, const Handle::LgList &w, const QuartetHostArgs &a, const double *dP, double *dJ,
                           double *dK, int tc, cudaStream_t st)
 {
-    if (w.kind == 0) {
+    if (w.kind == 0 || (lg_generic_cuda_core(w) && tc == 0)) {
         QuartetHostArgs b = a;
         b.method = TCE_METHOD_LEARNED;
         b.dict_nq = w.nq;
@@ -600,7 +610,7 @@ static int lg_launch_list(Handle *h, const Handle::LgList &w, const QuartetHostA
     if (w.kind == 1)
         return tc ? tce_launch_quartets_s_tc(h->S, b, w.nq, tc, st)
                   : tce_launch_quartets_s_lg(h->S, b, w.nq, w.fp32 != 0, st);
-    return tc ? tce_launch_quartets_r1_tc(h->S, w.cls, b, w.nq, st)
+    return tc ? tce_launch_quartets_sp_tc(h->S, w.cls, b, w.nq, tc, st)
               : tce_launch_quartets_r1_lg(h->S, w.cls, b, w.nq, w.fp32 != 0, st);
 }
 
