@@ -249,6 +249,7 @@ __global__ void __launch_bounds__(256, MINB) k_quartets_sp_tc(DevSys S, SArgs A)
 #pragma unroll
                     for (int t = 0; t < NT; ++t)
                         tN[t] = (0 <= gmb[t] && cq <= S.ncap) ? __ldg(Tg + (size_t)cq * NQ + 8 * (g0 + t) + rq) : 0.0;
+#pragma unroll 2
                     for (int s4 = 0; s4 <= nend; s4 += 4) {
                         const int n = s4 + cq, n1 = n + 4;
                         double F[NCOMB][MT], Tb[NT];
