@@ -682,6 +682,11 @@ def main():
     # kernels of one learned-grid pass: one per work list (kernel class, rule size,
     # FP32 panels), the plain list on the side stream, the judge's fallback launch
     launches_per_step = eng.pass_kernels()
+    # the lists as one chain on one stream against the default two chains (tce_set_list_streams):
+    # what the overlap of one list's tail with the next list's start buys
+    eng.set_list_streams(1)
+    one_chain_ms, _ = run(TCE_METHOD_LEARNED, args.steps, args.warmup)
+    eng.set_list_streams(2)
     # each work list's kernel alone: time and algorithmic work, for per-kernel fractions
     per_list = eng.lg_list_profile(3) if world == 1 else None
     # comparison arms on the same device: the plain adaptive method and the system's 32-node rule
@@ -709,6 +714,34 @@ def main():
     single_err, single_rej = pass_error(eng, ho, np.full(len(ho), single), T_ho, offs_ho)
     single_plain = eng.lg_stats()["plain_direct"]
     eng.lg_set_item_rules(net_rules)
+    # the reference's own rules on the learned grid's kernels (tensor cores, FP32 panels,
+    # autotuned forms; the 40-node rule padded to 64 nodes): a one-rule dictionary whose Gauss
+    # weights are its own weights, so that the judge accepts every block; the blocks are those
+    # of the fixed_rule and rule_40_node arms
+    from william_ci_b200 import learned_grid as LGm
+    from william_ci_b200 import quadrature as Qm
+
+    def reference_rule_on_tc(nodes):
+        e = Engine(sysm)
+        if world > 1:
+            e.set_shard(rank, world)
+        tr, wr = Qm.mapped_gauss_legendre(nodes)
+        e.lg_set_rules([(tr, wr, wr)])
+        e.set_plain_rule(*LGm.plain_rule(), 0.6)
+        e.lg_set_item_rules(np.zeros(len(e.items()), dtype=np.int32))
+        e.set_fp32_threshold(FP32_THRESHOLD)
+        e.set_method(TCE_METHOD_LEARNED)
+        if world == 1:
+            e.lg_autotune(3)
+        e.set_graph(True)
+        ms, _ = run(TCE_METHOD_LEARNED, args.steps, args.warmup, e=e)
+        B, _, _ = e.rule_blocks(0, ho)
+        err = float(np.abs(B - T_ho).max())
+        e.close()
+        return ms, err
+
+    r32tc_ms, err32tc = reference_rule_on_tc(32)
+    r40tc_ms, err40tc = reference_rule_on_tc(40)
     eng.set_method(TCE_METHOD_LEARNED)
     for _ in range(2):               # back to the network's rules (their rejects already routed)
         step()
@@ -813,6 +846,17 @@ def main():
                                    "plain_list": single_plain, "heldout_judge_rejects": single_rej,
                                    "method": "the method without the network: the one dictionary rule most training "
                                              "quartets accept, for every quartet, judge and plain fallback"},
+            "fixed_rule_tensor_cores": {"value": nq_total / (r32tc_ms * 1e-3), "ms_per_step": r32tc_ms,
+                                        "max_err_vs_oracle_table128": err32tc,
+                                        "method": "the reference's default 32-node rule on the learned grid's "
+                                                  "kernels (FP64 tensor cores, FP32 panels, autotuned forms)"},
+            "list_chains": {"two_chains_ms_per_step": ms_step, "one_chain_ms_per_step": one_chain_ms,
+                            "note": "the learned-grid lists split into two cost-balanced chains on two streams "
+                                    "(the default, the headline) or run one after another on one stream"},
+            "rule_40_node_tensor_cores": {"value": nq_total / (r40tc_ms * 1e-3), "ms_per_step": r40tc_ms,
+                                          "max_err_vs_oracle_table128": err40tc,
+                                          "method": "the reference's nquad_128 setting (40-node rule, padded to 64 "
+                                                    "nodes) on the learned grid's kernels"},
             "learned_grid_fp64_only": {"value": nq_total / (lg64_ms * 1e-3), "ms_per_step": lg64_ms},
             "fp32_panels": fp32,
             "cuda_graph": "each J/K pass replayed as one CUDA graph (tce_set_graph)",
@@ -832,12 +876,19 @@ def main():
     # the north-star figures last, so that a reader of the end of the line has them
     summary = {"lg_over_plain": plain_ms / ms_step,
                "lg_over_rule_40_node": r40_ms / ms_step, "lg_over_single_rule_judged": single_ms / ms_step,
+               "lg_over_fixed_rule_tensor_cores": r32tc_ms / ms_step,
+               "lg_over_rule_40_node_tensor_cores": r40tc_ms / ms_step,
                "max_err_vs_oracle_table128": {"learned_grid": lg_err["learned_grid"], "rule_40_node": err40,
                                               "single_rule_judged": single_err,
                                               "fixed_32_node_rule": lg_err["fixed_32_node_rule"],
+                                              "fixed_32_node_rule_tensor_cores": err32tc,
+                                              "rule_40_node_tensor_cores": err40tc,
                                               "plain": lg_err["plain"]},
                "pass_ms": {"learned_grid": ms_step, "rule_40_node": r40_ms, "single_rule_judged": single_ms,
-                           "fixed_32_node_rule": fixed_ms, "plain": plain_ms}}
+                           "learned_grid_one_chain": one_chain_ms,
+                           "fixed_32_node_rule": fixed_ms, "fixed_32_node_rule_tensor_cores": r32tc_ms,
+                           "rule_40_node_tensor_cores": r40tc_ms,
+                           "plain": plain_ms}}
     if "rhf_scf" in line:
         summary["rhf_energy_abs_diff_vs_oracle"] = {k: line["rhf_scf"][k]["abs_diff_vs_oracle"]
                                                     for k in ("learned_grid", "fixed_32_node_rule")}

@@ -204,6 +204,13 @@ int tce_set_graph(void *handle, int32_t on);
  * arithmetic type, different summation order.  No reference counterpart. */
 int tce_set_tensor_cores(void *handle, int32_t on);
 
+/* The learned-grid work lists of a pass as n chains (1 or 2; default 2): the
+ * lists split by their summed cost estimates, longest first, each chain on
+ * its own stream inside the pass (and its CUDA graph), so that the tail of
+ * one list's persistent launch overlaps the start of the next.  Every list
+ * has its own work counter.  No reference counterpart (execution option). */
+int tce_set_list_streams(void *handle, int32_t n);
+
 /* Kernel-form tuning of the learned-grid pass (after tce_lg_predict_rules /
  * tce_lg_set_item_rules): every work list that has both a CUDA-core and an
  * FP64 tensor-core kernel is timed in each of its forms (the CUDA-core

@@ -226,6 +226,36 @@ def test_graph_replay_matches_direct_launches(chain16_lg):
     eng.set_graph(False)
 
 
+def test_one_and_two_list_chains_give_the_same_jk(chain16_lg):
+    """The learned-grid lists as one chain or as two chains on two streams
+    (tce_set_list_streams), with and without the CUDA graph: J/K equal to
+    1e-13 of the density scale (only the order of the atomic sums differs),
+    and the judge rejects nothing more."""
+    from william_ci_b200.engine import TCE_METHOD_LEARNED
+    sysm, eng, net = chain16_lg
+    P = random_density(sysm.nbas, 7) * 0.05
+    scale = np.abs(P).sum()
+    eng.set_method(TCE_METHOD_LEARNED)
+    eng.lg_predict_rules(net)
+    eng.direct_JK(P)                     # the judge's rejects move to the plain list
+    assert len(eng.lg_lists()) > 2
+    eng.set_graph(False)
+    eng.set_list_streams(1)
+    J0, K0 = eng.direct_JK(P)
+    for graph in (False, True):
+        eng.set_graph(graph)
+        eng.set_list_streams(2)
+        for _ in range(2):               # captured, then replayed
+            J, K = eng.direct_JK(P)
+            assert eng.lg_stats()["rejected"] == 0
+            assert np.abs(J - J0).max() <= 1e-13 * scale and np.abs(K - K0).max() <= 1e-13 * scale, graph
+    eng.set_graph(False)
+    from william_ci_b200.engine import TCEError
+    with pytest.raises(TCEError):
+        eng.set_list_streams(3)
+    eng.set_list_streams(2)
+
+
 def test_fp32_panels_error_vs_fp64(chain16_lg):
     """FP32 node sums for quartets with Schwarz product below 1e-6: the J/K
     difference from the all-FP64 pass stays below 1e-10 per unit density."""

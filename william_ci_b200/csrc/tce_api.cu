@@ -354,6 +354,9 @@ int build(Handle *h, const tce_system *sys)
     CK(h, cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
     CK(h, cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
     CK(h, cudaEventCreateWithFlags(&h->ev_fb, cudaEventDisableTiming));
+    CK(h, cudaStreamCreateWithFlags(&h->st3, cudaStreamNonBlocking));
+    CK(h, cudaEventCreateWithFlags(&h->ev_fork3, cudaEventDisableTiming));
+    CK(h, cudaEventCreateWithFlags(&h->ev_join3, cudaEventDisableTiming));
     int s;
     DevSys &S = h->S;
     S.ndp = h->ndp; S.nq = h->nq; S.ncap = h->ncap; S.nbas = nbas; S.nfuc = h->nfuc;
@@ -682,11 +685,13 @@ void release_streams(Handle *h)
 {
     if (h->st) cudaStreamDestroy(h->st);
     if (h->st2) cudaStreamDestroy(h->st2);
-    for (cudaEvent_t e : {h->ev0, h->ev1, h->ev_in, h->ev_out, h->ev_fork, h->ev_join, h->ev_fb})
+    if (h->st3) cudaStreamDestroy(h->st3);
+    for (cudaEvent_t e : {h->ev0, h->ev1, h->ev_in, h->ev_out, h->ev_fork, h->ev_join, h->ev_fb, h->ev_fork3, h->ev_join3})
         if (e) cudaEventDestroy(e);
     if (h->h_fb) cudaFreeHost(h->h_fb);
-    h->st = h->st2 = nullptr;
+    h->st = h->st2 = h->st3 = nullptr;
     h->ev0 = h->ev1 = h->ev_in = h->ev_out = h->ev_fork = h->ev_join = h->ev_fb = nullptr;
+    h->ev_fork3 = h->ev_join3 = nullptr;
     h->h_fb = nullptr;
 }
 
@@ -815,6 +820,7 @@ int tce_destroy(void *handle)
     if (h->st) cudaStreamSynchronize(h->st);
     drop_graph(h);
     if (h->st2) cudaStreamSynchronize(h->st2);
+    if (h->st3) cudaStreamSynchronize(h->st3);
     for (void *p : h->allocs) cudaFree(p);
     release_streams(h);
     delete h;
@@ -928,6 +934,20 @@ int tce_set_tensor_cores(void *handle, int32_t on)
     if (!h) return fail(h, TCE_ERR_ARG, "NULL handle");
     h->use_tc = on ? 1 : 0;
     ++h->work_version;   // a captured pass is re-captured
+    return TCE_OK;
+}
+
+int tce_set_list_streams(void *handle, int32_t n)
+{
+    Handle *h = static_cast<Handle *>(handle);
+    if (!h) return fail(h, TCE_ERR_ARG, "NULL handle");
+    if (n != 1 && n != 2) return fail(h, TCE_ERR_ARG, "list streams: 1 or 2");
+    h->list_streams = n;
+    // a captured pass is re-captured; the lists are unchanged, so rejects
+    // read from the last pass still apply
+    const bool keep_fb = h->fb_version == h->work_version;
+    ++h->work_version;
+    if (keep_fb) h->fb_version = h->work_version;
     return TCE_OK;
 }
 

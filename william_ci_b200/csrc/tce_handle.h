@@ -92,6 +92,7 @@ struct Handle {
         int *rule = nullptr;
         long long n = 0;
         int max_ncomb = 1, max_ncq = 1;
+        double cost = 0.0;               // summed cost estimate of its quartets (chain balance)
     };
     std::vector<LgList> lg_lists;
     std::map<int, int> tc_choice;
@@ -122,6 +123,15 @@ struct Handle {
     unsigned long long *d_node_evals = nullptr;
     unsigned int *d_next2 = nullptr;     // work counter of the second kernel of a pass
     unsigned int *d_next3 = nullptr;
+    // The learned-grid lists of a pass run as list_streams chains (1 or 2): the
+    // second chain on st3, forked from and joined to the pass's stream, so
+    // that one list's tail overlaps the next list's start; every list has its
+    // own work counter (d_list_next[list]).
+    int list_streams = 2;
+    cudaStream_t st3 = nullptr;
+    cudaEvent_t ev_fork3 = nullptr, ev_join3 = nullptr;
+    unsigned int *d_list_next = nullptr;
+    int list_next_cap = 0;
     // CUDA graph of the J/K pass (tce_set_graph); rebuilt when any key changes
     int use_graph = 0;
     int use_tc = 1;                      // FP64 tensor-core node sums where a kernel has them

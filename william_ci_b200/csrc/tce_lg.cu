@@ -357,6 +357,10 @@ static int ensure_plain(Handle *h)
     if (!h->d_node_evals && (s = dalloc(h, &h->d_node_evals, 1))) return s;
     if (!h->d_next2 && (s = dalloc(h, &h->d_next2, 1))) return s;
     if (!h->d_next3 && (s = dalloc(h, &h->d_next3, 1))) return s;
+    if (!h->d_list_next) {   // one work counter per learned-grid list (at most 3 x 16 x 4 lists)
+        if ((s = dalloc(h, &h->d_list_next, 3 * 16 * 4))) return s;
+        h->list_next_cap = 3 * 16 * 4;
+    }
     if (!h->d_plain_scratch) {
         const long long warps = (long long)h->num_sms * 16;
         const long long per = tce_plain_scratch_per_warp(h->S, h->max_ncq);
@@ -458,6 +462,8 @@ int lg_rebuild_lists(Handle *h)
     std::vector<std::vector<int4>> lg(3 * 16 * 4);
     std::vector<std::vector<int>> rl(3 * 16 * 4);
     std::vector<int4> pl;
+    std::vector<double> lcost(3 * 16 * 4, 0.0);
+    const bool have_cost = h->cost_host.size() == h->items_host.size();
     h->n_fp32 = 0;
     for (long long i : h->shard_idx) {
         const int r = h->item_rule[(size_t)i];
@@ -472,6 +478,7 @@ int lg_rebuild_lists(Handle *h)
             const int key = (route * 2 + (h->rules_host[r].nq == 64 ? 1 : 0)) * 2 + (f32 ? 1 : 0);
             lg[key].push_back(q);
             rl[key].push_back(r);
+            lcost[(size_t)key] += have_cost ? h->cost_host[(size_t)i] : 1.0;
         } else {
             pl.push_back(q);
         }
@@ -513,6 +520,7 @@ int lg_rebuild_lists(Handle *h)
             if (tcit != h->tc_choice.end()) w.tc = tcit->second;
         }
         w.n = (long long)lg[key].size();
+        w.cost = lcost[(size_t)key] * (w.nq == 64 ? 2.0 : 1.0);   // per-quartet cost scales with the nodes
         if (w.kind == 0 || lg_generic_cuda_core(w)) {
             w.max_ncomb = w.max_ncq = 1;
             for (const int4 &q : lg[key]) {
@@ -571,7 +579,7 @@ static int lg_tc(const Handle *h, const Handle::LgList &w)
 // one learned-grid list with kernel form tc (0 CUDA cores, >= 1 FP64 tensor
 // cores; for the all-s kernel the tile shape)
 static int lg_launch_list(Handle *h, const Handle::LgList &w, const QuartetHostArgs &a, const double *dP, double *dJ,
-                          double *dK, int tc, cudaStream_t st)
+                          double *dK, int tc, cudaStream_t st, unsigned int *next)
 {
     if (w.kind == 0 || (lg_generic_cuda_core(w) && tc == 0)) {
         QuartetHostArgs b = a;
@@ -584,7 +592,7 @@ static int lg_launch_list(Handle *h, const Handle::LgList &w, const QuartetHostA
         b.item_rule = w.rule;
         b.fb_items = h->d_fb_items;
         b.fb_count = h->d_fb_count;
-        b.next = h->d_next;
+        b.next = next;
         b.use_tc = tc;
         return tce_launch_quartets(h->S, b, st);
     }
@@ -592,7 +600,7 @@ static int lg_launch_list(Handle *h, const Handle::LgList &w, const QuartetHostA
     b.items = w.d;
     b.nitems = (int)w.n;
     b.prim_screen = h->prim_screen;
-    b.next = h->d_next;
+    b.next = next;
     b.P = dP;
     b.J = dJ;
     b.K = dK;
@@ -700,7 +708,36 @@ int lg_jk_passes(Handle *h, const double *dP, double *dJ, double *dK, cudaStream
         CKS(h, tce_launch_quartets(h->S, b, h->st2));
         CK(h, cudaEventRecord(h->ev_join, h->st2));
     }
-    for (const auto &w : h->lg_lists) CKS(h, lg_launch_list(h, w, a, dP, dJ, dK, lg_tc(h, w), st));
+    // the lists as one or two chains: longest-processing-time split by their cost
+    // estimates, each chain in list order; the second chain on st3
+    const int nl = (int)h->lg_lists.size();
+    std::vector<int> chain((size_t)nl, 0);
+    if (h->list_streams > 1 && nl > 1 && h->d_list_next && nl <= h->list_next_cap) {
+        std::vector<int> order((size_t)nl);
+        std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int x, int y) { return h->lg_lists[(size_t)x].cost > h->lg_lists[(size_t)y].cost; });
+        double load[2] = {0.0, 0.0};
+        for (int i : order) {
+            const int c = load[0] <= load[1] ? 0 : 1;
+            chain[(size_t)i] = c;
+            load[c] += h->lg_lists[(size_t)i].cost;
+        }
+    }
+    const bool two = std::find(chain.begin(), chain.end(), 1) != chain.end();
+    if (two) {
+        CK(h, cudaEventRecord(h->ev_fork3, st));
+        CK(h, cudaStreamWaitEvent(h->st3, h->ev_fork3, 0));
+    }
+    for (int i = 0; i < nl; ++i) {
+        const auto &w = h->lg_lists[(size_t)i];
+        unsigned int *next = (h->d_list_next && i < h->list_next_cap) ? h->d_list_next + i : h->d_next;
+        CKS(h, lg_launch_list(h, w, a, dP, dJ, dK, lg_tc(h, w), chain[(size_t)i] ? h->st3 : st, next));
+    }
+    if (two) {
+        CK(h, cudaEventRecord(h->ev_join3, h->st3));
+        CK(h, cudaStreamWaitEvent(st, h->ev_join3, 0));
+    }
     // join before the judge's fallback: both plain launches use the same per-warp scratch
     if (side) CK(h, cudaStreamWaitEvent(st, h->ev_join, 0));
     if (h->n_lg > 0) {   // the judge's rejects, count read on the device
@@ -1360,7 +1397,7 @@ int tce_lg_autotune(void *handle, int32_t reps, int32_t *ntuned, int32_t *nswitc
             for (int r = 0; r < reps && s == TCE_OK; ++r) {
                 cudaMemsetAsync(h->d_fb_count, 0, sizeof(unsigned int), h->st);
                 cudaEventRecord(e0, h->st);
-                s = lg_launch_list(h, w, a, h->d_P, h->d_J, h->d_K, tc, h->st);
+                s = lg_launch_list(h, w, a, h->d_P, h->d_J, h->d_K, tc, h->st, h->d_next);
                 cudaEventRecord(e1, h->st);
                 if (s == TCE_OK && cudaEventSynchronize(e1) != cudaSuccess) s = TCE_ERR_CUDA;
                 float ms = 0.f;
@@ -1435,7 +1472,7 @@ int tce_lg_list_profile(void *handle, int32_t reps, int32_t *n, double *ms, doub
         for (int r = 0; r < reps && s == TCE_OK; ++r) {
             cudaMemsetAsync(h->d_fb_count, 0, sizeof(unsigned int), h->st);
             cudaEventRecord(e0, h->st);
-            s = lg_launch_list(h, w, a, h->d_P, h->d_J, h->d_K, lg_tc(h, w), h->st);
+            s = lg_launch_list(h, w, a, h->d_P, h->d_J, h->d_K, lg_tc(h, w), h->st, h->d_next);
             cudaEventRecord(e1, h->st);
             if (s == TCE_OK && cudaEventSynchronize(e1) != cudaSuccess) s = TCE_ERR_CUDA;
             float t = 0.f;

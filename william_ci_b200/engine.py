@@ -43,7 +43,7 @@ EXPORTS = ["tce_create", "tce_destroy", "tce_last_error", "tce_get_info", "tce_s
            "tce_mlp_get_params", "tce_mlp_set_params", "tce_mlp_loss_grad", "tce_mlp_train", "tce_mlp_predict",
            "tce_lg_predict_rules", "tce_lg_work", "tce_quad_self_check", "tce_set_graph",
            "tce_set_fp32_threshold", "tce_dfmp2_energy", "tce_mp2_last_error", "tce_create_blocks",
-           "tce_pass_kernels", "tce_set_tensor_cores", "tce_nuclear_attraction", "tce_quad_self_check_nuc",
+           "tce_pass_kernels", "tce_set_tensor_cores", "tce_set_list_streams", "tce_nuclear_attraction", "tce_quad_self_check_nuc",
            "tce_lg_autotune", "tce_lg_lists", "tce_dfjk_create", "tce_dfjk", "tce_dfjk_destroy",
            "tce_dfjk_last_error", "tce_ao_to_kmo", "tce_shard_items", "tce_lg_list_profile",
            "tce_df_create", "tce_df_destroy", "tce_df_last_error", "tce_df_integrals", "tce_df_fitted", "tce_dfmp2",
@@ -137,6 +137,7 @@ def lib():
         L.tce_set_graph.argtypes = [C.c_void_p, C.c_int32]
         L.tce_pass_kernels.argtypes = [C.c_void_p, _ip]
         L.tce_set_tensor_cores.argtypes = [C.c_void_p, C.c_int32]
+        L.tce_set_list_streams.argtypes = [C.c_void_p, C.c_int32]
         L.tce_nuclear_attraction.argtypes = [C.c_void_p, C.c_int32, _dp, _ip, _dp]
         L.tce_lg_autotune.argtypes = [C.c_void_p, C.c_int32, _ip, _ip, _dp]
         L.tce_lg_lists.argtypes = [C.c_void_p, _ip, _ip]
@@ -483,6 +484,10 @@ class Engine:
     def set_tensor_cores(self, on: bool = True):
         """FP64 tensor-core node sums where a kernel has them (tce_set_tensor_cores)."""
         _check(lib().tce_set_tensor_cores(self.h, int(bool(on))), self.h)
+
+    def set_list_streams(self, n: int = 2):
+        """The learned-grid lists of a pass as n chains on their own streams (tce_set_list_streams)."""
+        _check(lib().tce_set_list_streams(self.h, int(n)), self.h)
 
     def set_graph(self, on: bool = True):
         """Capture each J/K pass into a CUDA graph and replay it (tce_set_graph)."""
