@@ -801,18 +801,24 @@ def main():
             traffic = None
     kernels = None
     if per_list:
-        names = {0: "k_quartets<%d>", 1: "k_quartets_s%s<%d>", 2: "k_quartets_r1%s<%d>"}
         kernels = []
         for w in per_list:
-            nm = names[w["kind"]] % ((w["nq"],) if w["kind"] == 0 else ("_tc" if w["tc"] else "", w["nq"]))
-            if w["kind"] == 1 and w["tc"]:
+            # kind 1 all-s, 2 one or two p shells (their CUDA-core forms: k_quartets_r1 for one
+            # p shell, the generic kernel for two), 0 generic
+            if w["kind"] == 0 or (w["kind"] == 2 and not w["tc"] and bin(w["cls"]).count("1") >= 2):
+                nm = "k_quartets<%d>" % w["nq"]
+            elif w["kind"] == 1:
+                nm = "k_quartets_s%s<%d>" % ("_tc" if w["tc"] else "", w["nq"])
+            else:
+                nm = ("k_quartets_sp_tc<%d>" if w["tc"] else "k_quartets_r1<%d>") % w["nq"]
+            if w["kind"] in (1, 2) and w["tc"]:
                 nm += " tile shape %d" % w["tc"]
             kernels.append({"kernel": nm + (" fp32" if w["fp32"] else ""), "cls": w["cls"], "quartets": w["n"],
                             "ms": w["ms"], "flops": w["flops"],
                             "tflops": w["flops"] / (w["ms"] * 1e-3) / 1e12 if w["ms"] > 0 else None,
                             "frac": w["flops"] / (w["ms"] * 1e-3) / 1e12 / peak if w["ms"] > 0 else None})
     roofline = {"bound": "fp64", "kernel": "the learned-grid J/K pass, one CUDA graph: k_quartets<32|64>, "
-                                           "k_quartets_s[_tc], k_quartets_r1[_tc] (per-quartet rule, judge, fused "
+                                           "k_quartets_s[_tc], k_quartets_sp_tc, k_quartets_r1 (per-quartet rule, judge, fused "
                                            "J/K scatter) and the plain launches",
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if (achieved and peak) else None, "traffic": traffic,
