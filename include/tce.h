@@ -197,11 +197,11 @@ int tce_set_graph(void *handle, int32_t on);
 
 /* Node sums of the learned-grid pass on the FP64 tensor cores (mma.sync
  * m8n8k4, FP64 in and out) where a kernel has that form: the all-s quartets
- * of one periodic direction, and the one-p s/p classes of one periodic
- * direction with 32-node rules, and the rows (primitive quartet x power
- * combination) of the generic kernel of one periodic direction with 64-node
- * rules (FP64 quartets; the FP32-panel quartets keep their kernel).  Default on; off gives the FP64 CUDA-core kernels.  Same
- * arithmetic type, different summation order.  No reference counterpart. */
+ * and the s/p classes with one or two p shells of one periodic direction
+ * (32- and 64-node rules, tile shapes from tce_lg_autotune), and the rows
+ * (primitive quartet x power combination) of the generic kernel.  Default
+ * on; off gives the FP64 CUDA-core kernels.  Same arithmetic type, different
+ * summation order.  No reference counterpart. */
 int tce_set_tensor_cores(void *handle, int32_t on);
 
 /* The learned-grid work lists of a pass as n chains (1 or 2; default 2): the
