@@ -55,3 +55,12 @@ def test_bad_arguments_are_rejected_before_the_device():
     with pytest.raises(E.TCEError) as ei:
         E.Engine(s, nquad=33)
     assert ei.value.code in (E.TCE_ERR_UNSUPPORTED, E.TCE_ERR_ARG)
+
+
+def test_execution_options_reject_a_null_handle():
+    """The pass's execution options (graph, tensor cores, list chains) check
+    their handle before touching anything: a NULL handle is an argument error."""
+    lib = E.lib()
+    assert lib.tce_set_graph(None, 1) == E.TCE_ERR_ARG
+    assert lib.tce_set_tensor_cores(None, 1) == E.TCE_ERR_ARG
+    assert lib.tce_set_list_streams(None, 2) == E.TCE_ERR_ARG
