@@ -879,7 +879,8 @@ def main():
         line["named_shapes"] = {nm: named_shape_stage(nm, flush) for nm in NAMED}
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(sysm, stride=1)
-    # the north-star figures last, so that a reader of the end of the line has them
+    # the headline figures last (speed-ups, held-out errors, pass times, energies), so that a
+    # reader of the end of the line has them
     summary = {"lg_over_plain": plain_ms / ms_step,
                "lg_over_rule_40_node": r40_ms / ms_step, "lg_over_single_rule_judged": single_ms / ms_step,
                "lg_over_fixed_rule_tensor_cores": r32tc_ms / ms_step,
